@@ -1,0 +1,201 @@
+"""ctypes binding of libgdp.so for tests and benchmarks.
+
+The library itself is C/CUDA (include/gdp.h); this module only mirrors its
+structs as numpy dtypes and loads the shared object.  It never computes an
+alignment: every score, direction and traceback comes from the CUDA kernels
+inside libgdp.so, and loading fails loudly when the library is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgdp.so")
+
+FULL, UPPER, LOWER = 0, 1, 2
+FLAG_JUMP_LATE, FLAG_REVP, FLAG_TRACEBACK, FLAG_RERUN16 = 1, 2, 4, 8
+HIGHQ, MEDQ, LOWQ, ENDQ = 0, 1, 2, 3
+STATUS = {0: "GDP_OK", 1: "GDP_ERR_LEN", 2: "GDP_ERR_BAND", 3: "GDP_ERR_PARAM",
+          4: "GDP_ERR_BUDGET", 5: "GDP_ERR_TIMEOUT", 6: "GDP_ERR_CUDA",
+          7: "GDP_ERR_RECS", 8: "GDP_ERR_NOGENOME"}
+
+# struct gdp_pair (include/gdp.h), 88 bytes
+PAIR_DTYPE = np.dtype([
+    ("rseq", "<i8"), ("rseq_uc", "<i8"), ("gseq", "<i8"), ("gseq_alt", "<i8"),
+    ("rlength", "<i4"), ("glength", "<i4"), ("lband", "<i4"), ("uband", "<i4"),
+    ("variant", "i1"), ("precision", "i1"), ("mismatchtype", "i1"), ("flags", "i1"),
+    ("open", "<i2"), ("extend", "<i2"),
+    ("tb_r", "<i4"), ("tb_c", "<i4"),
+    ("queryoffset", "<i4"), ("genomeoffset", "<i4"),
+    ("chroffset", "<u4"), ("chrhigh", "<u4"),
+    ("watsonp", "i1"), ("genestrand", "i1"), ("reserved", "<i2"),
+    ("dynprogindex", "<i4"),
+])
+assert PAIR_DTYPE.itemsize == 88
+
+# struct gdp_rec, 16 bytes
+REC_DTYPE = np.dtype([
+    ("querypos", "<i4"), ("genomepos", "<i4"), ("genomejump", "<i4"),
+    ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1"),
+])
+assert REC_DTYPE.itemsize == 16
+
+# struct gdp_result, 48 bytes
+RESULT_DTYPE = np.dtype([
+    ("status", "<i4"), ("score", "<i4"), ("precision", "<i4"), ("rerun", "<i4"),
+    ("tb_score", "<i4"), ("nmatches", "<i4"), ("nmismatches", "<i4"),
+    ("nopens", "<i4"), ("nindels", "<i4"), ("nrecs", "<i4"),
+    ("rec_offset", "<i8"),
+])
+assert RESULT_DTYPE.itemsize == 48
+
+WL_FIXED, WL_SHORT, WL_CDNA, WL_MIX, WL_LONG = 1, 2, 3, 4, 5
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def load(path=LIB_PATH):
+    """Loads libgdp.so and declares its entry points."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"libgdp.so not built at {path}: run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    lib.gdp_version.restype = ctypes.c_char_p
+    lib.gdp_ctx_create.argtypes = [ctypes.POINTER(vp), i32, i32, i64]
+    lib.gdp_ctx_destroy.argtypes = [vp]
+    lib.gdp_set_genome.argtypes = [vp, vp, vp, ctypes.c_uint64]
+    lib.gdp_align_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_align_batch_device.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+    lib.gdp_fill_dump.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, vp, vp, vp]
+    lib.gdp_launch_count.argtypes = [vp]
+    lib.gdp_launch_count.restype = i64
+    lib.gdp_last_error.argtypes = [vp]
+    lib.gdp_last_error.restype = ctypes.c_char_p
+    lib.gdp_workload_genome.argtypes = [ctypes.c_uint64, vp, i64]
+    lib.gdp_workload_genomecomp.argtypes = [vp, i64, vp]
+    lib.gdp_workload_pairs.argtypes = [i32, ctypes.c_uint64, vp, i64, i64, vp, vp, i64,
+                                       ctypes.POINTER(i64)]
+    lib.gdp_workload_pairs.restype = i64
+    lib.gdp_pair_cells.argtypes = [vp]
+    lib.gdp_pair_cells.restype = i64
+    return lib
+
+
+def make_genome(lib, seed, length):
+    """Returns (char genome as uint8 array, genomecomp blocks as uint32 array)."""
+    g = np.zeros(length, dtype=np.uint8)
+    lib.gdp_workload_genome(seed, _ptr(g), length)
+    nwords = (length + 31) // 32
+    blocks = np.zeros(3 * nwords, dtype=np.uint32)
+    lib.gdp_workload_genomecomp(_ptr(g), length, _ptr(blocks))
+    return g, blocks
+
+
+def make_pairs(lib, kind, seed, genome, npairs, arena_bytes=None):
+    """Generates a seeded synthetic batch; returns (pairs, arena)."""
+    if arena_bytes is None:
+        per = {WL_FIXED: 600, WL_SHORT: 1200, WL_CDNA: 16000, WL_MIX: 12000, WL_LONG: 36000}[kind]
+        arena_bytes = npairs * per + (1 << 16)
+    pairs = np.zeros(npairs, dtype=PAIR_DTYPE)
+    arena = np.zeros(arena_bytes, dtype=np.uint8)
+    used = ctypes.c_int64(0)
+    n = lib.gdp_workload_pairs(kind, seed, _ptr(genome), genome.size, npairs, _ptr(pairs),
+                               _ptr(arena), arena_bytes, ctypes.byref(used))
+    if n != npairs:
+        raise RuntimeError(f"arena too small: generated {n} of {npairs} pairs")
+    return pairs, arena[:max(used.value, 1)].copy()
+
+
+def pair_cells(lib, pairs):
+    """In-band cells per pair over the reference's compare domain."""
+    out = np.zeros(pairs.size, dtype=np.int64)
+    base = pairs.ctypes.data
+    for i in range(pairs.size):
+        out[i] = lib.gdp_pair_cells(ctypes.c_void_p(base + i * PAIR_DTYPE.itemsize))
+    return out
+
+
+def band_cells(pairs):
+    """Vectorised in-band cell count (same domain as pair_cells)."""
+    r = pairs["rlength"].astype(np.int64)
+    g = pairs["glength"].astype(np.int64)
+    var = pairs["variant"]
+    lb = np.where(var == UPPER, 0, pairs["lband"]).astype(np.int64)
+    ub = np.where(var == LOWER, 0, pairs["uband"]).astype(np.int64)
+    total = np.zeros(pairs.size, dtype=np.int64)
+    # sum over diagonals d = r - c in [-ub, lb] of the cells with 1<=c<=g, 1<=r<=rl
+    for i in range(pairs.size):
+        d = np.arange(-ub[i], lb[i] + 1)
+        cmin = np.maximum(1, 1 - d)
+        cmax = np.minimum(g[i], r[i] - d)
+        total[i] = np.maximum(0, cmax - cmin + 1).sum()
+    return total
+
+
+class Context:
+    """One libgdp context (device, tables, resident genome)."""
+
+    def __init__(self, lib, device=0, mode=0, budget=0):
+        self.lib = lib
+        h = ctypes.c_void_p()
+        rc = lib.gdp_ctx_create(ctypes.byref(h), device, mode, budget)
+        if rc != 0:
+            raise RuntimeError(f"gdp_ctx_create failed: {STATUS.get(rc, rc)}")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.gdp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def error(self):
+        return self.lib.gdp_last_error(self.h).decode()
+
+    def launches(self):
+        return int(self.lib.gdp_launch_count(self.h))
+
+    def set_genome(self, blocks, altblocks=None, length=None):
+        if length is None:
+            length = blocks.size // 3 * 32
+        rc = self.lib.gdp_set_genome(self.h, _ptr(blocks), _ptr(altblocks), length)
+        if rc != 0:
+            raise RuntimeError(f"gdp_set_genome: {STATUS.get(rc, rc)} {self.error()}")
+
+    def align(self, pairs, arena, max_recs=None):
+        n = pairs.size
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        if max_recs is None:
+            max_recs = int((pairs["rlength"].astype(np.int64) + pairs["glength"] + 2).sum())
+        recs = np.zeros(max(max_recs, 1), dtype=REC_DTYPE)
+        used = ctypes.c_int64(0)
+        rc = self.lib.gdp_align_batch(self.h, _ptr(pairs), n, _ptr(arena), arena.size,
+                                      _ptr(results), _ptr(recs), max_recs, ctypes.byref(used))
+        if rc != 0:
+            raise RuntimeError(f"gdp_align_batch: {STATUS.get(rc, rc)} {self.error()}")
+        return results, recs[:used.value]
+
+    def fill_dump(self, pairs, arena):
+        n = pairs.size
+        sizes = (pairs["glength"].astype(np.int64) + 1) * (pairs["rlength"].astype(np.int64) + 1)
+        offs = np.zeros(n, dtype=np.int64)
+        offs[1:] = np.cumsum(sizes)[:-1]
+        total = int(sizes.sum())
+        H = np.zeros(total, dtype=np.int16)
+        dN = np.zeros(total, dtype=np.int8)
+        dE = np.zeros(total, dtype=np.int8)
+        dF = np.zeros(total, dtype=np.int8)
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        rc = self.lib.gdp_fill_dump(self.h, _ptr(pairs), n, _ptr(arena), arena.size, _ptr(offs),
+                                    _ptr(H), _ptr(dN), _ptr(dE), _ptr(dF), _ptr(results))
+        if rc != 0:
+            raise RuntimeError(f"gdp_fill_dump: {STATUS.get(rc, rc)} {self.error()}")
+        return offs, H, dN, dE, dF, results

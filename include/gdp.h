@@ -1,0 +1,191 @@
+/*
+ * gdp.h -- C ABI of the B200 banded affine-gap dynamic-programming library
+ * (libgdp.so), a drop-in for the fills and tracebacks of GMAP's
+ * src/dynprog_simd.c.
+ *
+ * Two layers are exported:
+ *
+ *  1. The batch API below (gdp_*): plain pointers and sizes, one call per
+ *     batch of independent alignment pairs.  Each pair carries exactly the
+ *     arguments of the reference entry point it replaces:
+ *       Dynprog_simd_8 / Dynprog_simd_16           (src/dynprog_simd.h:16-26, :46-55)
+ *       Dynprog_simd_8_upper / _16_upper           (src/dynprog_simd.h:27-35, :56-64)
+ *       Dynprog_simd_8_lower / _16_lower           (src/dynprog_simd.h:37-45, :66-74)
+ *       Dynprog_traceback_8 / _16                  (src/dynprog_simd.h:76-83, :102-109)
+ *       Dynprog_traceback_8_upper / _16_upper      (src/dynprog_simd.h:85-92, :111-118)
+ *       Dynprog_traceback_8_lower / _16_lower      (src/dynprog_simd.h:94-100, :120-125)
+ *     rsequence/gsequence/gsequence_alt, rlength/glength, lband/uband,
+ *     mismatchtype, open/extend, jump_late_p, revp, and for the traceback
+ *     (r, c), rsequenceuc, queryoffset, genomeoffset, chroffset, chrhigh,
+ *     watsonp, genestrand, dynprogindex keep the reference's meaning.
+ *
+ *  2. The twelve reference-signature entry points themselves, declared in
+ *     gdp_dynprog_simd.h, implemented on top of the batch API.
+ *
+ * All arithmetic is integer and bit-exact with the reference's AVX2 build:
+ * the final score, every in-band score and E/F/nogap direction, and the
+ * traceback Pair list.
+ */
+#ifndef GDP_H
+#define GDP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Variants: which reference fill a pair runs. */
+enum {
+  GDP_FULL = 0,   /* Dynprog_simd_{8,16}: band lband below, uband above the diagonal */
+  GDP_UPPER = 1,  /* Dynprog_simd_{8,16}_upper: r <= c <= r + uband, horizontal gaps only */
+  GDP_LOWER = 2   /* Dynprog_simd_{8,16}_lower: c <= r <= c + lband, vertical gaps only */
+};
+
+/* gdp_pair_t.flags */
+enum {
+  GDP_FLAG_JUMP_LATE = 1,   /* jump_late_p */
+  GDP_FLAG_REVP = 2,        /* revp: sequences are read backwards from their last character */
+  GDP_FLAG_TRACEBACK = 4,   /* run Dynprog_traceback_* from (tb_r, tb_c) */
+  GDP_FLAG_RERUN16 = 8      /* precision 8: rerun in 16-bit when the 8-bit fill overflows */
+};
+
+/* Mismatch types (src/dynprog.h:53) */
+enum { GDP_HIGHQ = 0, GDP_MEDQ = 1, GDP_LOWQ = 2, GDP_ENDQ = 3 };
+
+/* Per-pair and per-call status codes */
+enum {
+  GDP_OK = 0,
+  GDP_ERR_LEN = 1,       /* rlength/glength <= 0 or above the library maximum */
+  GDP_ERR_BAND = 2,      /* negative band, or the traceback start lies outside the filled band */
+  GDP_ERR_PARAM = 3,     /* bad variant / precision / mismatchtype / open / extend */
+  GDP_ERR_BUDGET = 4,    /* the pair's direction storage exceeds the context budget */
+  GDP_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+  GDP_ERR_CUDA = 6,      /* a CUDA call failed */
+  GDP_ERR_RECS = 7,      /* traceback record buffer too small */
+  GDP_ERR_NOGENOME = 8   /* a traceback needs genome characters but no genome is loaded */
+};
+
+/*
+ * One alignment pair.  Sequence fields are byte offsets into the caller's
+ * sequence arena.  Every sequence is stored forward in memory; with
+ * GDP_FLAG_REVP the reference's convention (a pointer to the last character,
+ * indexed seq[1-r]) is applied by the library.
+ */
+typedef struct gdp_pair {
+  int64_t rseq;          /* rsequence, rlength bytes */
+  int64_t rseq_uc;       /* rsequenceuc (upper-case query), used by the traceback */
+  int64_t gseq;          /* gsequence, glength bytes */
+  int64_t gseq_alt;      /* gsequence_alt, glength bytes (may equal gseq) */
+  int32_t rlength, glength;
+  int32_t lband, uband;  /* FULL uses both; UPPER uses uband; LOWER uses lband */
+  int8_t variant;        /* GDP_FULL / GDP_UPPER / GDP_LOWER */
+  int8_t precision;      /* 8 or 16 */
+  int8_t mismatchtype;   /* GDP_HIGHQ.. */
+  int8_t flags;          /* GDP_FLAG_* */
+  int16_t open, extend;  /* gap penalties, each in [-127, 0] */
+  int32_t tb_r, tb_c;    /* traceback start (normally rlength, glength) */
+  int32_t queryoffset, genomeoffset;
+  uint32_t chroffset, chrhigh;
+  int8_t watsonp, genestrand;
+  int16_t reserved;
+  int32_t dynprogindex;
+} gdp_pair_t;
+
+/*
+ * One traceback Pair record (the fields of the reference's struct Pair_T,
+ * src/pairdef.h:10-50, that Dynprog_traceback_* sets).  Records of a pair
+ * are stored in push order: the first record is the one the reference
+ * pushes first (nearest the traceback start).  A gap holder
+ * (Pairpool_push_gapholder, src/pairpool.c:374) has querypos = genomepos =
+ * -1 and genomejump = the skipped genome length; all other records have
+ * genomejump = 0 and dynprogindex = the pair's dynprogindex.
+ */
+typedef struct gdp_rec {
+  int32_t querypos;
+  int32_t genomepos;
+  int32_t genomejump;
+  char cdna, comp, genome, genomealt;
+} gdp_rec_t;
+
+/* Per-pair result. */
+typedef struct gdp_result {
+  int32_t status;        /* GDP_OK or GDP_ERR_* */
+  int32_t score;         /* matrix[glength][rlength] (lower: matrix[rlength][glength]) */
+  int32_t precision;     /* 8 or 16: the precision whose outputs were kept */
+  int32_t rerun;         /* 1 if an 8-bit fill overflowed and was rerun in 16 bits */
+  int32_t tb_score, nmatches, nmismatches, nopens, nindels;  /* traceback totals */
+  int32_t nrecs;         /* number of Pair records */
+  int64_t rec_offset;    /* index of the first record in the record buffer */
+} gdp_result_t;
+
+typedef struct gdp_ctx gdp_ctx;
+
+/* Library version string. */
+const char *gdp_version(void);
+
+/*
+ * Creates a context on CUDA device `device`.  `mode` is the reference's
+ * Mode_T (src/mode.h:4; 0 = STANDARD) and selects the substitution and
+ * consistency tables built as Dynprog_init does (src/dynprog.c:1007-1196).
+ * `dir_budget_bytes` bounds the device memory used for direction matrices
+ * per submitted wave (0 = library default).
+ */
+int gdp_ctx_create(gdp_ctx **ctx, int device, int mode, int64_t dir_budget_bytes);
+void gdp_ctx_destroy(gdp_ctx *ctx);
+
+/*
+ * Makes a genome resident on the device, in the reference's genomecomp
+ * format (three uint32 per 32 nt: high, low, N-flags; src/genome.c:9723).
+ * `altblocks` may be NULL (then the alternate genome equals the genome).
+ * Tracebacks read genome characters for short genome skips from it, as
+ * Pairpool_add_genomeskip does through Genome_get_char.
+ */
+int gdp_set_genome(gdp_ctx *ctx, const uint32_t *blocks, const uint32_t *altblocks,
+                   uint64_t genomelength);
+
+/*
+ * Aligns a batch end to end: host arena and pairs in, host results and
+ * traceback records out.  Returns GDP_OK when every pair was processed
+ * (per-pair failures are reported in results[i].status).  `recs` may be
+ * NULL when no pair asks for a traceback.
+ */
+int gdp_align_batch(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
+                    const char *arena, int64_t arena_bytes,
+                    gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                    int64_t *nrecs_used);
+
+/*
+ * Same as gdp_align_batch, but every pointer is a device pointer already
+ * resident in HBM (pairs, arena, results, recs), and the work is enqueued
+ * on the context's stream without a host synchronisation.  `rec_offsets`
+ * (device, npairs entries) gives each pair's first record slot; pairs with
+ * a traceback may write at most rlength + glength + 2 records.
+ */
+int gdp_align_batch_device(gdp_ctx *ctx, const gdp_pair_t *d_pairs, int64_t npairs,
+                           const char *d_arena, gdp_result_t *d_results,
+                           gdp_rec_t *d_recs, const int64_t *d_rec_offsets);
+
+/*
+ * Parity/debug entry: fills every pair and expands its in-band scores and
+ * directions into dense (glength+1) x (rlength+1) arrays in (c, r) order
+ * (out[c * (rlength+1) + r], lower variants transposed), covering the
+ * reference's compare domain (src/dynprog_simd.c:1044-1051, :1089-1096,
+ * :1134-1141).  Directions use the reference's codes: DIAG 0, HORIZ -1,
+ * VERT -2.  dense_offsets[i] is pair i's first element in the dense arrays.
+ */
+int gdp_fill_dump(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
+                  const char *arena, int64_t arena_bytes, const int64_t *dense_offsets,
+                  int16_t *H, int8_t *dN, int8_t *dE, int8_t *dF, gdp_result_t *results);
+
+/* Kernel launches issued by the context since creation (one per kernel). */
+int64_t gdp_launch_count(gdp_ctx *ctx);
+
+/* Last error message of the context (empty when none). */
+const char *gdp_last_error(gdp_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

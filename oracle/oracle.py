@@ -1,0 +1,120 @@
+"""Oracle loaders -- TEST INFRASTRUCTURE ONLY.
+
+Two CPU oracles with one interface:
+  * Reference: the reference's own AVX2 functions compiled from its sources
+    into oracle/_ref/libgdpref.so (see oracle/Makefile).
+  * Restatement: oracle/liboracle.so, this repository's plain-C restatement
+    of the same algorithm (oracle/gdp_oracle.c), pinned against the first.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline / reference
+arm import this module, and only as the checker or the timed CPU baseline.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libgdpref.so")
+REF_LIB_NOFLUSH = os.path.join(HERE, "_ref", "libgdpref_noflush.so")
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+class CpuOracle:
+    """Wraps libgdpref.so (prefix 'ref_') or liboracle.so (prefix 'orc_')."""
+
+    def __init__(self, path, prefix):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        self._init = getattr(self.lib, prefix + "init")
+        self._init.argtypes = [i32]
+        self._set_genome = getattr(self.lib, prefix + "set_genome")
+        self._set_genome.argtypes = [vp, vp, ctypes.c_uint64]
+        self._align = getattr(self.lib, prefix + "align")
+        self._align.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
+        self._align.restype = i32
+        self._bench = getattr(self.lib, prefix + "bench")
+        self._bench.argtypes = [vp, vp, i64, i32, ctypes.POINTER(i64)]
+        self._bench.restype = ctypes.c_double
+        self._pd = getattr(self.lib, prefix + "pairdistance")
+        self._pd.argtypes = [i32, i32, i32]
+        self._cons = getattr(self.lib, prefix + "consistent")
+        self._cons.argtypes = [i32, i32, i32]
+        self._genome_keep = None
+
+    def init(self, mode=0):
+        self._init(mode)
+
+    def pairdistance(self, mt, c1, c2):
+        return self._pd(mt, c1, c2)
+
+    def consistent(self, gs, c1, c2):
+        return self._cons(gs, c1, c2)
+
+    def set_genome(self, blocks, altblocks=None, length=None):
+        if length is None:
+            length = blocks.size // 3 * 32
+        self._genome_keep = (blocks, altblocks)
+        self._set_genome(_ptr(blocks), _ptr(altblocks), length)
+
+    def align(self, pair_arr, i, arena, want_matrix=True, max_recs=None):
+        """Fills pair i (and traces back if its flags ask).  Returns a dict."""
+        p = pair_arr[i:i + 1]
+        rl, gl = int(p["rlength"][0]), int(p["glength"][0])
+        n = (rl + 1) * (gl + 1)
+        H = np.zeros(n, np.int16) if want_matrix else None
+        dN = np.zeros(n, np.int8) if want_matrix else None
+        dE = np.zeros(n, np.int8) if want_matrix else None
+        dF = np.zeros(n, np.int8) if want_matrix else None
+        final = np.zeros(1, np.int32)
+        stats = np.zeros(6, np.int32)
+        if max_recs is None:
+            max_recs = rl + gl + 8
+        recs = np.zeros(max_recs, dtype=_rec_dtype())
+        nrec = self._align(_ptr(p), _ptr(arena), _ptr(H), _ptr(dN), _ptr(dE), _ptr(dF),
+                           _ptr(final), _ptr(stats), _ptr(recs), max_recs)
+        return {"score": int(final[0]), "H": H, "dN": dN, "dE": dE, "dF": dF,
+                "stats": stats, "recs": recs[:min(nrec, max_recs)], "nrecs": nrec}
+
+    def bench(self, pairs, arena, nthreads):
+        cs = ctypes.c_int64(0)
+        secs = self._bench(_ptr(pairs), _ptr(arena), pairs.size, nthreads, ctypes.byref(cs))
+        return secs, cs.value
+
+
+def _rec_dtype():
+    return np.dtype([("querypos", "<i4"), ("genomepos", "<i4"), ("genomejump", "<i4"),
+                     ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1")])
+
+
+def reference(noflush=False):
+    return CpuOracle(REF_LIB_NOFLUSH if noflush else REF_LIB, "ref_")
+
+
+def restatement():
+    return CpuOracle(ORACLE_LIB, "orc_")
+
+
+def reference_available():
+    return os.path.exists(REF_LIB)
+
+
+def domain_mask(variant, rlength, glength, lband, uband):
+    """Boolean (glength+1, rlength+1) mask of the reference's compare domain."""
+    c = np.arange(glength + 1)[:, None]
+    r = np.arange(rlength + 1)[None, :]
+    if variant == 0:
+        lo, hi = c - uband, c + lband
+    elif variant == 1:
+        lo, hi = c - uband, c
+    else:
+        lo, hi = c, c + lband
+    m = (r >= np.maximum(lo, 1)) & (r <= np.minimum(hi, rlength)) & (c >= 1)
+    return m
