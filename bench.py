@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the batched banded affine-gap DP path (fills + tracebacks).
+
+Default workload (one step = one batch): 1,000,000 short-read pairs,
+rlength U{75..300}, lband/uband U{3..30}, 3% substitutions, 1% indels, 5%
+random non-matching windows, 8-bit fills with the 16-bit rerun on overflow,
+traceback of every pair.  Synthetic, seeded.  Metric: GCUPS over the
+in-band cells of the reference's compare domain, whole job, fill +
+traceback.  `value` is measured with pairs and sequences resident in HBM;
+`e2e` goes through the host-buffer C-ABI call gdp_align_batch (host->device
+copies, planning, kernels, device->host copies of results and Pair records
+all inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gdp|reference]
+
+For N > 1 launch with torchrun; each rank aligns its own shard of the same
+size (weak scaling, no data-path collective: pairs are independent).
+`--impl reference` times the reference's own CPU code (oracle/_ref, built
+from the reference sources) on the host cores over a bounded sample.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gmap-gsnap_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import gdp  # noqa: E402
+
+WORKLOADS = {
+    "short": (gdp.WL_SHORT, 1_000_000, "short reads r U{75..300}, bands U{3..30}, 8-bit + 16-bit rerun"),
+    "fixed": (gdp.WL_FIXED, 10_000, "fixed 150x160, lband=uband=10, 16-bit"),
+    "mix": (gdp.WL_MIX, 20_000, "70/25/5 short/long/cdna mix"),
+    "cdna": (gdp.WL_CDNA, 2_000, "cDNA upper fill, r log-U[200,5000]"),
+    "long": (gdp.WL_LONG, 2_000, "long reads r U{1000..10000}, bands U{50..200}, 16-bit"),
+}
+OPS_PER_CELL = 9          # E: 2 add + 1 max, F: 2 add + 1 max, H: 1 add + 2 max
+DIR_BYTES_PER_CELL = 0.5  # 4 direction bits per cell
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "gdp" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_workload(lib, name, npairs, seed, genome_len=1 << 24):
+    kind = WORKLOADS[name][0]
+    genome, blocks = gdp.make_genome(lib, 777, genome_len)
+    pairs, arena = gdp.make_pairs(lib, kind, seed, genome, npairs)
+    return genome, blocks, pairs, arena
+
+
+def cpu_baseline(lib, name, seed, target_seconds, threads=None):
+    """The reference's own code (oracle/_ref) on a bounded sample of the same
+    workload, all host threads (or the port when the reference is absent)."""
+    import oracle
+    kind = "reference" if oracle.reference_available() else "port"
+    ref = oracle.reference() if kind == "reference" else oracle.restatement()
+    ref.init(0)
+    threads = threads or os.cpu_count() or 1
+    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+    ref.set_genome(blocks, None, genome.size)
+    n = 200
+    while True:
+        pairs, arena = gdp.make_pairs(lib, WORKLOADS[name][0], seed + 99, genome, n)
+        secs, _ = ref.bench(pairs, arena, threads)
+        if secs >= target_seconds / 4 or n >= 2_000_000:
+            break
+        n = int(min(2_000_000, n * max(2.0, target_seconds / max(secs, 1e-3))))
+    cells = int(gdp.band_cells(pairs).sum())
+    return {"value": round(cells / secs / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+            "sample": f"{n} pairs of the '{name}' workload ({cells} in-band cells), fill + traceback, "
+                      f"{secs:.2f} s wall on {threads} threads", "seconds": secs, "pairs": n, "cells": cells}
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        barrier(world)
+        return
+    lib = gdp.load()
+    name = args.workload
+    import oracle
+    kind = "reference" if oracle.reference_available() else "port"
+    ref = oracle.reference() if kind == "reference" else oracle.restatement()
+    ref.init(0)
+    threads = os.cpu_count() or 1
+    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+    ref.set_genome(blocks, None, genome.size)
+    cal = cpu_baseline(lib, name, args.seed, args.cpu_seconds / max(args.steps, 1), threads)
+    pairs, arena = gdp.make_pairs(lib, WORKLOADS[name][0], args.seed + 99, genome, cal["pairs"])
+    cells = int(gdp.band_cells(pairs).sum())
+    for _ in range(args.warmup):
+        ref.bench(pairs[:max(1, pairs.size // 20)], arena, threads)
+    times = []
+    for _ in range(args.steps):
+        secs, _ = ref.bench(pairs, arena, threads)
+        times.append(secs)
+    t = sum(times)
+    value = cells * args.steps / t / 1e9
+    line = {"metric": "GCUPS (in-band cells, fill + traceback), batched", "value": round(value, 4),
+            "unit": "GCUPS", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16/int8",
+            "data": "synthetic", "config": {"workload": name, "pairs_per_step": int(pairs.size),
+                                            "description": WORKLOADS[name][2]},
+            "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+                             "sample": f"{pairs.size} pairs of '{name}' per step on {threads} threads"},
+            "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "alignments_per_s": round(pairs.size * args.steps / t, 1)}
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def run_gdp(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    lib = gdp.load()
+    name = args.workload
+    npairs = args.npairs or WORKLOADS[name][1]
+    genome, blocks, pairs, arena = make_workload(lib, name, npairs, args.seed + 1000 * rank)
+    cells = int(gdp.band_cells(pairs).sum())
+    ctx = gdp.Context(lib, device=local)
+    ctx.set_genome(blocks, None, genome.size)
+
+    # resident inputs and outputs
+    plan = ctypes.c_void_p()
+    rc = lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan))
+    assert rc == 0, ctx.error()
+    total_recs = int(lib.gdp_plan_total_recs(plan))
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    d_arena = torch.from_numpy(arena).cuda()
+    d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    d_recs = torch.empty(max(total_recs, 1) * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+
+    def step():
+        rc = lib.gdp_plan_execute(ctx.h, plan, ctypes.c_void_p(d_pairs.data_ptr()),
+                                  ctypes.c_void_p(d_arena.data_ptr()), ctypes.c_void_p(d_res.data_ptr()),
+                                  ctypes.c_void_p(d_recs.data_ptr()))
+        assert rc == 0, ctx.error()
+
+    for _ in range(args.warmup):
+        step()
+    lib.gdp_sync(ctx.h)
+    res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+    bad = int((res["status"] != 0).sum())
+
+    sampler = ClockSampler(local)
+    ctx.profile(True)
+    ctx.profile_reset()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    sampler.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+    t1.record(stream)
+    t1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = ctx.launches() - launches0
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ms_max = max_over_ranks(world, ms)
+    total_cells = sum_over_ranks(world, float(cells))
+    total_pairs = sum_over_ranks(world, float(pairs.size))
+    value = total_cells * args.steps / (ms_max * 1e-3) / 1e9
+
+    # dominant kernel and its roofline (integer issue bound)
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    top_name, (top_ms, top_n) = top
+    avg_launch_ms = top_ms / top_n
+    int_peak = ctx.int_peak()
+    achieved_ops = cells * OPS_PER_CELL / (avg_launch_ms * 1e-3)
+    dir_bytes = int(lib.gdp_plan_dir_bytes(plan))
+
+    # end to end through the host-buffer C ABI call
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    results = np.zeros(pairs.size, dtype=gdp.RESULT_DTYPE)
+    recs = np.zeros(max(total_recs, 1), dtype=gdp.REC_DTYPE)
+    used = ctypes.c_int64(0)
+    rc = lib.gdp_align_batch(ctx.h, gdp._ptr(pairs), pairs.size, gdp._ptr(arena), arena.size,
+                             gdp._ptr(results), gdp._ptr(recs), recs.size, ctypes.byref(used))
+    assert rc == 0, ctx.error()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        rc = lib.gdp_align_batch(ctx.h, gdp._ptr(pairs), pairs.size, gdp._ptr(arena), arena.size,
+                                 gdp._ptr(results), gdp._ptr(recs), recs.size, ctypes.byref(used))
+        assert rc == 0, ctx.error()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / e2e_steps)
+    e2e_value = total_cells / (e2e_ms * 1e-3) / 1e9
+    h2d = pairs.nbytes + arena.nbytes
+    d2h = results.nbytes + int(used.value) * gdp.REC_DTYPE.itemsize
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(lib, name, args.seed, args.cpu_seconds)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    lib.gdp_plan_destroy(plan)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm = None
+    if os.path.exists(peaks_path):
+        hbm = json.load(open(peaks_path)).get("hbm_gbs")
+    if rank == 0:
+        line = {
+            "metric": "GCUPS (in-band cells, fill + traceback), batched",
+            "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16/int8", "data": "synthetic",
+            "config": {"workload": name, "pairs_per_gpu": int(pairs.size), "description": WORKLOADS[name][2],
+                       "cells_per_gpu": cells, "l2": "inputs larger than L2 (sequence arena %.0f MB, "
+                       "direction words %.0f MB per step)" % (arena.nbytes / 1e6, dir_bytes / 1e6),
+                       "parallelism": f"pairs sharded, {world} independent rank(s)"},
+            "alignments_per_s": round(total_pairs * args.steps / (ms_max * 1e-3), 1),
+            "e2e": {"value": round(e2e_value, 3), "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
+            "roofline": {"bound": "int", "kernel": top_name,
+                         "achieved": round(achieved_ops / 1e12, 3), "peak": round(int_peak / 1e12, 3),
+                         "unit": "Tops/s (int32 lane-ops)", "frac": round(achieved_ops / int_peak, 4),
+                         "peak_source": "measured int32 issue probe (gdp_measure_int_peak)",
+                         "ops_per_cell": OPS_PER_CELL, "avg_launch_ms": round(avg_launch_ms, 3),
+                         "traffic": None,
+                         "dir_write_gbs": round(dir_bytes / (avg_launch_ms * 1e-3) / 1e9, 1),
+                         "hbm_peak_gbs": hbm},
+            "kernels": {k: {"ms_total": round(v[0], 3), "launches": v[1]} for k, v in prof.items()},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "bad_status_pairs": bad,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gdp", "reference"], default="gdp")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="short")
+    ap.add_argument("--npairs", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=1002)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gdp(args)
+
+
+if __name__ == "__main__":
+    main()

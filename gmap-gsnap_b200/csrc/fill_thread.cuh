@@ -1,0 +1,285 @@
+/*
+ * fill_thread.cuh -- one-thread-per-pair fill kernels for sm_100a.
+ *
+ * Each thread runs one alignment pair through exactly the block sweep of
+ * the reference (src/dynprog_simd.c): blocks of W lanes (W = 16 for the
+ * 16-bit fills, 32 for the 8-bit fills), each block swept over its column
+ * range, every lane of a block computed for every swept column (including
+ * the lanes outside the band, whose values reach the in-band E values),
+ * then for the full band the scalar F loop over the in-band lanes.  A
+ * block's W lane states (H, E) and their query profiles live in registers;
+ * the only state that crosses blocks -- the last lane's final H and the F
+ * carry FF (src/dynprog_simd.c:6999) -- goes through a per-thread scratch
+ * column in global memory, interleaved across threads so a warp's accesses
+ * coalesce.
+ *
+ * Saturating int8/int16 lane arithmetic is done in int32 with explicit
+ * clamps (the F chain is plain int, as in the reference).  Directions are
+ * packed to 4 bits per cell (see gdp_internal.h) and written as W/8 words
+ * per block column.
+ */
+#pragma once
+#include "gdp_internal.h"
+
+#define GDP_SEL(k) ((uint32_t) (k) | ((uint32_t) ((k) | 8) << 4) | ((uint32_t) ((k) | 8) << 8) | ((uint32_t) ((k) | 8) << 12))
+
+/* Sign-extended byte `sel` of {hi:lo} (PTX prmt, default mode). */
+__device__ __forceinline__ int
+prof_byte (uint32_t lo, uint32_t hi, uint32_t sel) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi), "r"(sel));
+  return (int) r;
+}
+
+/* Signed byte-wise max of two packed profiles (lower fill folds g, g_alt). */
+__device__ __forceinline__ uint32_t
+bytemax (uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int x = (int) (int8_t) (a >> (8 * k)), y = (int) (int8_t) (b >> (8 * k));
+    r |= (uint32_t) (uint8_t) (x > y ? x : y) << (8 * k);
+  }
+  return r;
+}
+
+/* Character at 1-based position i of a sequence, honouring revp. */
+__device__ __forceinline__ int
+seqch (const char *base, int len, int i, bool revp) {
+  return (int) (uint8_t) __ldg(base + (revp ? len - i : i - 1)) & 127;
+}
+
+struct FillParams {
+  const gdp_pair_t *pairs;
+  const char *arena;
+  const int32_t *list;     /* pair indices of this group */
+  const int32_t *count;    /* device: number of entries in list */
+  uint32_t *dirs;          /* direction words */
+  int16_t *hdump;          /* debug (may be NULL): score of every swept cell, 8 per direction word */
+  gdp_meta_t *meta;
+  gdp_result_t *res;
+  int2 *scratch;           /* [y * nslots + slot] = (H of the block's last lane, FF) */
+  int64_t nslots;
+  int scratch_rows;        /* columns available per slot */
+  const gdp_tables_t *tab;
+};
+
+/* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records the largest
+   in-band score), 2 = 8-bit pass of a rerun pair (skipped when the 16-bit
+   pass proved an overflow; stops at the first in-band 127). */
+template <int W, int VARIANT, bool LATE, int MODE>
+__global__ void __launch_bounds__(128)
+fill_thread_kernel (FillParams P) {
+  constexpr int LO = (W == 32) ? -128 : -32768;
+  constexpr int HI = (W == 32) ? 127 : 32767;
+  constexpr int WORDS = W / 8;
+  __shared__ int8_t s_nt2int[128];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
+  __syncthreads();
+
+  const int64_t slot = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *P.count;
+  for (int64_t li = slot; li < n; li += P.nslots) {
+    const int pi = __ldg(P.list + li);
+    const gdp_pair_t p = P.pairs[pi];
+    gdp_meta_t *mp = P.meta + pi;
+    if (MODE == 2 && mp->maxh16 >= 127) {
+      mp->status8 = 1;   /* the 16-bit scores reach 127, so the 8-bit fill overflows */
+      continue;
+    }
+    gdp_geom_t g;
+    gdp_geom_of(&p, W, &g);
+    const bool revp = (p.flags & GDP_FLAG_REVP) != 0;
+    const int open = p.open, ext = p.extend, oe = p.open + p.extend;
+    const int mt = p.mismatchtype;
+    const int lband = p.lband, uband = p.uband;
+    const char *lseq = P.arena + (VARIANT == GDP_LOWER ? p.gseq : p.rseq);
+    const char *lalt = P.arena + (VARIANT == GDP_LOWER ? p.gseq_alt : p.rseq);
+    const int llen = (VARIANT == GDP_LOWER) ? p.glength : p.rlength;
+    const char *sseq = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq);
+    const char *salt = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq_alt);
+    const int slen = (VARIANT == GDP_LOWER) ? p.rlength : p.glength;
+    uint32_t *dir = P.dirs + ((W == 16) ? mp->dir16 : mp->dir8);
+    int2 *sc = P.scratch + slot;
+    const int64_t scs = P.nslots;
+    int final_score = LO, maxh = LO;
+    bool aborted = false;
+
+    for (int xlo = 0; xlo <= g.X; xlo += W) {
+      const int xhi = min(xlo + W - 1, g.X);
+      int y0, y1;
+      gdp_block_sweep(&g, xlo, &y0, &y1);
+      if (y1 < y0) continue;
+
+      /* lane profiles: 5 signed bytes per lane */
+      uint32_t plo[W], phi[W];
+#pragma unroll
+      for (int i = 0; i < W; i++) {
+        const int x = xlo + i;
+        if (VARIANT != GDP_LOWER) {
+          const int q = (x == 0) ? 'N' : (x <= llen ? seqch(lseq, llen, x, revp) : 'N');
+          plo[i] = __ldg(&P.tab->profq_lo[mt][q]);
+          phi[i] = __ldg(&P.tab->profq_hi[mt][q]);
+        } else {
+          if (x == 0) {
+            /* 16-bit: column 0 scores against 'N' (:8689); 8-bit: against code 4 (:5459) */
+            const int c0 = (W == 32) ? 4 : 'N';
+            plo[i] = __ldg(&P.tab->profg_lo[mt][c0]);
+            phi[i] = __ldg(&P.tab->profg_hi[mt][c0]);
+          } else if (x <= llen) {
+            const int a = seqch(lseq, llen, x, revp), b = seqch(lalt, llen, x, revp);
+            plo[i] = bytemax(__ldg(&P.tab->profg_lo[mt][a]), __ldg(&P.tab->profg_lo[mt][b]));
+            phi[i] = bytemax(__ldg(&P.tab->profg_hi[mt][a]), __ldg(&P.tab->profg_hi[mt][b]));
+          } else {
+            plo[i] = 0; phi[i] = 0;
+          }
+        }
+      }
+      int H[W], E[W];
+#pragma unroll
+      for (int i = 0; i < W; i++) { H[i] = LO - open; E[i] = LATE ? LO : LO + 1; }
+      int bot_prev = LO;   /* H[y-1][xlo-1] from the block above */
+      if (xlo > 0 && y0 > 0) bot_prev = sc[(int64_t) (y0 - 1) * scs].x;
+      uint32_t *dcol = dir;
+
+      for (int y = y0; y <= y1; y++) {
+        /* swept-column classes */
+        uint32_t selA, selB;
+        bool col0 = false;
+        if (VARIANT == GDP_LOWER) {
+          const int k = (y == 0) ? 4 : s_nt2int[seqch(sseq, slen, y, revp)];
+          selA = selB = GDP_SEL(k);
+        } else if (y == 0) {
+          selA = selB = GDP_SEL(4);
+          col0 = (VARIANT == GDP_FULL);
+        } else {
+          selA = GDP_SEL(s_nt2int[seqch(sseq, slen, y, revp)]);
+          selB = GDP_SEL(s_nt2int[seqch(salt, slen, y, revp)]);
+        }
+        int2 above = make_int2(LO, GDP_NEGINT);
+        if (xlo > 0) above = sc[(int64_t) y * scs];
+        int diag;
+        if (y == 0) diag = (VARIANT == GDP_FULL) ? (xlo == 0 ? 0 : LO) : 0;
+        else diag = (xlo == 0) ? LO : bot_prev;
+        bot_prev = above.x;
+
+        uint32_t bH = 0, bV = 0, bE = 0, bF = 0;
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+          const int x = xlo + i;
+          const int Hold = H[i];
+          int Eold = E[i];
+          const bool masked = (VARIANT != GDP_FULL) && (x >= y);
+          if (masked) Eold = LO;
+          const int T1 = max(Hold + open, LO);
+          bool pE = LATE ? (Eold >= T1) : (Eold > T1);
+          int Ee = max(max(Eold, T1) + ext, LO);
+          if (masked) Ee = LO;
+          int ps;
+          if (VARIANT == GDP_FULL && col0) {
+            ps = (x == 0) ? 0 : LO;
+          } else if (VARIANT == GDP_LOWER) {
+            ps = prof_byte(plo[i], phi[i], selA);
+          } else {
+            ps = max(prof_byte(plo[i], phi[i], selA), prof_byte(plo[i], phi[i], selB));
+          }
+          const int Hv = min(max(diag + ps, LO), HI);
+          diag = Hold;
+          bool pN = LATE ? (Ee >= Hv) : (Ee > Hv);
+          int Hn = max(Hv, Ee);
+          if (VARIANT == GDP_FULL) {
+            if (x == y + lband && y > 0 && x <= xhi) { Hn = Hv; pE = false; pN = false; }
+          } else {
+            if (x == y && x <= xhi) { pE = false; pN = false; }   /* diagonal fix (:7966-7969) */
+          }
+          H[i] = Hn;
+          E[i] = Ee;
+          bE |= (uint32_t) pE << i;
+          bH |= (uint32_t) pN << i;
+        }
+        if (VARIANT == GDP_FULL) {
+          /* F loop over the in-band lanes (:6916-7000) */
+          int Fp, Hp;
+          if (xlo == 0 || y >= xlo + uband) { Fp = GDP_NEGINT; Hp = GDP_NEGINT; }
+          else { Fp = above.y; Hp = above.x; }
+#pragma unroll
+          for (int i = 0; i < W; i++) {
+            const int d = xlo + i - y;
+            if (d == -uband) {
+              Fp = GDP_NEGINT + oe;
+              Hp = H[i];
+            } else if (d > -uband && d <= lband && xlo + i <= xhi) {
+              const int s = Hp + open;
+              const bool pF = LATE ? (Fp >= s) : (Fp > s);
+              const int F = (pF ? Fp : s) + ext;
+              const bool pV = LATE ? (F >= H[i]) : (F > H[i]);
+              if (pV) H[i] = F;
+              Hp = H[i];
+              Fp = F;
+              bF |= (uint32_t) pF << i;
+              bV |= (uint32_t) pV << i;
+            }
+          }
+          sc[(int64_t) y * scs] = make_int2(H[W - 1], Fp);
+        } else {
+          sc[(int64_t) y * scs] = make_int2(H[W - 1], 0);
+        }
+        if (MODE != 0) {
+#pragma unroll
+          for (int i = 0; i < W; i++) {
+            const int x = xlo + i;
+            bool dom;
+            if (VARIANT == GDP_FULL) dom = (x - y >= -uband) && (x - y <= lband);
+            else if (VARIANT == GDP_UPPER) dom = (x <= y) && (x >= y - uband);
+            else dom = (x >= y - lband) && (x <= y);
+            dom = dom && x >= 1 && y >= 1 && x <= g.X;
+            if (dom) maxh = max(maxh, H[i]);
+          }
+        }
+        if (y == g.Y) {
+#pragma unroll
+          for (int i = 0; i < W; i++) if (xlo + i == g.X) final_score = H[i];
+        }
+        if (P.hdump != nullptr) {
+          int16_t *hd = P.hdump + (dcol - P.dirs) * 8;
+#pragma unroll
+          for (int i = 0; i < W; i++) hd[i] = (int16_t) H[i];
+        }
+        /* direction words */
+#pragma unroll
+        for (int j = 0; j < WORDS; j++) {
+          const uint32_t w = ((bH >> (8 * j)) & 0xFFu) | (((bV >> (8 * j)) & 0xFFu) << 8) |
+                             (((bE >> (8 * j)) & 0xFFu) << 16) | (((bF >> (8 * j)) & 0xFFu) << 24);
+          dcol[j] = w;
+        }
+        dcol += WORDS;
+      }
+      dir = dcol;
+      if (MODE == 2 && maxh >= HI) { aborted = true; break; }
+    }
+
+    /* the final cell must have been swept */
+    int y0l, y1l;
+    gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
+    const bool swept = (g.Y >= y0l && g.Y <= y1l);
+    if (MODE == 1) {
+      mp->maxh16 = maxh;
+    }
+    if (MODE == 2) {
+      const bool overflow = aborted || maxh >= HI || final_score <= -128 + 30;
+      mp->status8 = overflow ? 1 : 0;
+      mp->final8 = final_score;
+      if (!overflow) {
+        P.res[pi].score = final_score;
+        P.res[pi].precision = 8;
+        P.res[pi].rerun = 0;
+      }
+    } else {
+      gdp_result_t *r = P.res + pi;
+      r->score = final_score;
+      r->precision = W == 16 ? 16 : 8;
+      r->rerun = (MODE == 1) ? 1 : 0;
+      if (!swept) r->status = GDP_ERR_BAND;
+    }
+  }
+}

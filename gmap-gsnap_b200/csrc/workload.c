@@ -248,9 +248,14 @@ make_pair (rng_t *r, int kind, const char *genome, int64_t glen_total,
     } else {
       n = mutate(r, q, rlength, tmp, rlength * 2 + 64, &m);
     }
-    if (n < rlength - lband) n = rlength - lband;
-    if (n > rlength + uband) n = rlength + uband;
-    if (n < 1) n = 1;
+    {
+      int want = n;
+      if (want < rlength - lband) want = rlength - lband;
+      if (want > rlength + uband) want = rlength + uband;
+      if (want < 1) want = 1;
+      if (want > n) memcpy(tmp + n, genome + pos + rlength, want - n);   /* pad from the flank */
+      n = want;
+    }
     glength = n;
     memcpy(w, tmp, glength);
     free(tmp);

@@ -68,7 +68,25 @@ def load(path=LIB_PATH):
     lib.gdp_ctx_destroy.argtypes = [vp]
     lib.gdp_set_genome.argtypes = [vp, vp, vp, ctypes.c_uint64]
     lib.gdp_align_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
-    lib.gdp_align_batch_device.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+    lib.gdp_plan_create.argtypes = [vp, vp, i64, ctypes.POINTER(vp)]
+    lib.gdp_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
+    lib.gdp_plan_total_recs.argtypes = [vp]
+    lib.gdp_plan_total_recs.restype = i64
+    lib.gdp_plan_rec_offset.argtypes = [vp, i64]
+    lib.gdp_plan_rec_offset.restype = i64
+    lib.gdp_plan_dir_bytes.argtypes = [vp]
+    lib.gdp_plan_dir_bytes.restype = i64
+    lib.gdp_plan_destroy.argtypes = [vp]
+    lib.gdp_sync.argtypes = [vp]
+    lib.gdp_debug_tables.argtypes = [i32, vp, vp, vp]
+    lib.gdp_ctx_stream.argtypes = [vp]
+    lib.gdp_ctx_stream.restype = vp
+    lib.gdp_profile_enable.argtypes = [vp, i32]
+    lib.gdp_profile_read.argtypes = [vp, i32, ctypes.c_char_p, i32, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(i64)]
+    lib.gdp_profile_reset.argtypes = [vp]
+    lib.gdp_measure_int_peak.argtypes = [vp]
+    lib.gdp_measure_int_peak.restype = ctypes.c_double
     lib.gdp_fill_dump.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, vp, vp, vp]
     lib.gdp_launch_count.argtypes = [vp]
     lib.gdp_launch_count.restype = i64
@@ -82,6 +100,17 @@ def load(path=LIB_PATH):
     lib.gdp_pair_cells.argtypes = [vp]
     lib.gdp_pair_cells.restype = i64
     return lib
+
+
+def tables(lib, mode=0):
+    """The substitution / consistency tables libgdp builds (host only)."""
+    pd = np.zeros((4, 128, 128), np.int16)
+    cons = np.zeros((3, 128, 128), np.uint8)
+    nt = np.zeros(128, np.int8)
+    rc = lib.gdp_debug_tables(mode, _ptr(pd), _ptr(cons), _ptr(nt))
+    if rc != 0:
+        raise RuntimeError(f"gdp_debug_tables: {STATUS.get(rc, rc)}")
+    return pd, cons, nt
 
 
 def make_genome(lib, seed, length):
@@ -119,19 +148,21 @@ def pair_cells(lib, pairs):
 
 
 def band_cells(pairs):
-    """Vectorised in-band cell count (same domain as pair_cells)."""
+    """In-band cells per pair over the reference's compare domain (same as
+    pair_cells), vectorised over the band's diagonals d = r - c."""
     r = pairs["rlength"].astype(np.int64)
     g = pairs["glength"].astype(np.int64)
     var = pairs["variant"]
     lb = np.where(var == UPPER, 0, pairs["lband"]).astype(np.int64)
     ub = np.where(var == LOWER, 0, pairs["uband"]).astype(np.int64)
     total = np.zeros(pairs.size, dtype=np.int64)
-    # sum over diagonals d = r - c in [-ub, lb] of the cells with 1<=c<=g, 1<=r<=rl
-    for i in range(pairs.size):
-        d = np.arange(-ub[i], lb[i] + 1)
+    if pairs.size == 0:
+        return total
+    for d in range(-int(ub.max()), int(lb.max()) + 1):
+        on = (d >= -ub) & (d <= lb)
         cmin = np.maximum(1, 1 - d)
-        cmax = np.minimum(g[i], r[i] - d)
-        total[i] = np.maximum(0, cmax - cmin + 1).sum()
+        cmax = np.minimum(g, r - d)
+        total += np.where(on, np.maximum(0, cmax - cmin + 1), 0)
     return total
 
 
@@ -162,6 +193,29 @@ class Context:
 
     def launches(self):
         return int(self.lib.gdp_launch_count(self.h))
+
+    def stream_handle(self):
+        return int(self.lib.gdp_ctx_stream(self.h) or 0)
+
+    def profile(self, on=True):
+        self.lib.gdp_profile_enable(self.h, 1 if on else 0)
+
+    def profile_reset(self):
+        self.lib.gdp_profile_reset(self.h)
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} since the last reset."""
+        out = {}
+        name = ctypes.create_string_buffer(64)
+        for k in range(27):
+            ms, n = ctypes.c_double(0), ctypes.c_int64(0)
+            self.lib.gdp_profile_read(self.h, k, name, 64, ctypes.byref(ms), ctypes.byref(n))
+            if n.value:
+                out[name.value.decode()] = (ms.value, n.value)
+        return out
+
+    def int_peak(self):
+        return float(self.lib.gdp_measure_int_peak(self.h))
 
     def set_genome(self, blocks, altblocks=None, length=None):
         if length is None:

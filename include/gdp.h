@@ -157,15 +157,26 @@ int gdp_align_batch(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
                     int64_t *nrecs_used);
 
 /*
- * Same as gdp_align_batch, but every pointer is a device pointer already
- * resident in HBM (pairs, arena, results, recs), and the work is enqueued
- * on the context's stream without a host synchronisation.  `rec_offsets`
- * (device, npairs entries) gives each pair's first record slot; pairs with
- * a traceback may write at most rlength + glength + 2 records.
+ * Plans for device-resident batches.  gdp_plan_create inspects the pairs
+ * (host copy) once: it validates them, bins them by fill kind and work,
+ * and lays out the device direction storage and the traceback record
+ * slots.  gdp_plan_execute then enqueues the fills and tracebacks on the
+ * context's stream for device-resident pairs / arena / results / records
+ * (device pointers, same contents as planned) without synchronising the
+ * host.  Record slots: pair i may write up to rlength + glength + 2
+ * records starting at gdp_plan_rec_offset(plan, i).
  */
-int gdp_align_batch_device(gdp_ctx *ctx, const gdp_pair_t *d_pairs, int64_t npairs,
-                           const char *d_arena, gdp_result_t *d_results,
-                           gdp_rec_t *d_recs, const int64_t *d_rec_offsets);
+typedef struct gdp_plan gdp_plan;
+int gdp_plan_create(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, gdp_plan **plan);
+int gdp_plan_execute(gdp_ctx *ctx, gdp_plan *plan, const gdp_pair_t *d_pairs, const char *d_arena,
+                     gdp_result_t *d_results, gdp_rec_t *d_recs);
+int64_t gdp_plan_total_recs(const gdp_plan *plan);
+int64_t gdp_plan_rec_offset(const gdp_plan *plan, int64_t i);
+int64_t gdp_plan_dir_bytes(const gdp_plan *plan);
+void gdp_plan_destroy(gdp_plan *plan);
+
+/* Waits for the context's stream. */
+int gdp_sync(gdp_ctx *ctx);
 
 /*
  * Parity/debug entry: fills every pair and expands its in-band scores and
@@ -178,6 +189,32 @@ int gdp_align_batch_device(gdp_ctx *ctx, const gdp_pair_t *d_pairs, int64_t npai
 int gdp_fill_dump(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
                   const char *arena, int64_t arena_bytes, const int64_t *dense_offsets,
                   int16_t *H, int8_t *dN, int8_t *dE, int8_t *dF, gdp_result_t *results);
+
+/*
+ * Host-only: fills caller arrays with the tables a context built for
+ * `mode`: pd[4][128][128] (pairdistance_array), cons[3][128][128]
+ * (consistent_array), nt2int[128] (nt_to_int_array).  Any may be NULL.
+ */
+int gdp_debug_tables(int mode, int16_t *pd, uint8_t *cons, int8_t *nt2int);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+   order work against it. */
+void *gdp_ctx_stream(gdp_ctx *ctx);
+
+/*
+ * Per-kernel timing.  While enabled, every kernel launch of the context is
+ * bracketed by CUDA events on its stream.  gdp_profile_read(ctx, id, ...)
+ * returns, for kernel id 0..26 (0..23 fill kinds, 24 traceback, 25 result
+ * initialisation, 26 integer-rate probe), its name, total device
+ * milliseconds and launch count since the last reset.
+ */
+int gdp_profile_enable(gdp_ctx *ctx, int on);
+int gdp_profile_read(gdp_ctx *ctx, int id, char *name, int name_cap, double *ms, int64_t *launches);
+int gdp_profile_reset(gdp_ctx *ctx);
+
+/* Integer issue rate of the device (32-bit lane-ops per second), measured
+   with an ALU/FMA-pipe probe kernel: the denominator of the fill roofline. */
+double gdp_measure_int_peak(gdp_ctx *ctx);
 
 /* Kernel launches issued by the context since creation (one per kernel). */
 int64_t gdp_launch_count(gdp_ctx *ctx);

@@ -473,6 +473,10 @@ tbread (const gdp_pair_t *p, const grid_t *G, const int8_t *plane, int c, int r)
   }
   at = gidx(G, c, r);
   if (plane != G->dF && !G->wr[at]) tb_stale++;
+  /* Full band: a cell above the band was computed from the previous block's
+     row at a column that block never swept (the reference's X_prev read of
+     matrix[c-1][rlo-1], src/dynprog_simd.c:6838), i.e. from stale scratch. */
+  if (p->variant == GDP_FULL && r < c - p->uband) tb_stale++;
   return plane[at];
 }
 #define TBREAD(plane, c, r) tbread(p, G, G->plane, (c), (r))

@@ -1,0 +1,164 @@
+"""Bit-exact parity of the CUDA fills and tracebacks (called through
+libgdp.so's C ABI) with the reference's AVX2 functions.
+
+The oracle is the reference itself compiled from its sources
+(oracle/_ref/libgdpref.so) when that library is present, else the C
+restatement (oracle/liboracle.so) that tests/test_oracle.py pins against
+it.  Bar: identical integers -- every in-band score and E/F/nogap
+direction over the reference's compare domain, the final score, the
+traceback score and counts, and every Pair record.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import gdp
+import oracle as orc
+import parity
+
+pytestmark = pytest.mark.gpu
+
+GENOME = {}
+
+
+@pytest.fixture(scope="module")
+def env(gdplib, restatement):
+    ref = orc.reference() if orc.reference_available() else restatement
+    ref.init(0)
+    g, blocks, altb = cases.genome(5, length=1 << 17)
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, altb, g.size)
+    ref.set_genome(blocks, altb, g.size)
+    restatement.set_genome(blocks, altb, g.size)
+    GENOME['g'] = g
+    yield ctx, ref, restatement
+    ctx.close()
+
+
+@pytest.mark.parametrize("seed,variants,precs", [
+    (101, (0,), (16,)), (102, (0,), (8,)), (103, (1,), (16,)), (104, (1,), (8,)),
+    (105, (2,), (16,)), (106, (2,), (8,)), (107, (0, 1, 2), (8, 16)),
+])
+def test_fill_random(env, seed, variants, precs):
+    ctx, ref, _ = env
+    pairs, arena = cases.random_cases(seed, 300, variants=variants, precisions=precs)
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+
+
+@pytest.mark.parametrize("seed", [201, 202, 203])
+def test_traceback_random(env, seed):
+    ctx, ref, rest = env
+    pairs, arena = cases.random_cases(seed, 400)
+    fails, nundef = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+
+
+def test_rerun_contract(env, gdplib):
+    """8-bit pairs with the 16-bit rerun: the kept precision follows the
+    overflow rule, and the kept outputs are bit-exact with that precision."""
+    ctx, ref, rest = env
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 31, GENOME['g'], 200)
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+    res, _ = ctx.align(pairs, arena)
+    assert (res["status"] == 0).all()
+    assert (res["precision"] == 16).sum() > 0
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+
+
+@pytest.mark.parametrize("kind,n", [(gdp.WL_FIXED, 300), (gdp.WL_CDNA, 12), (gdp.WL_LONG, 4)])
+def test_workload_shapes(env, gdplib, kind, n):
+    ctx, ref, rest = env
+    pairs, arena = gdp.make_pairs(gdplib, kind, 40 + kind, GENOME['g'], n)
+    if kind != gdp.WL_FIXED:
+        fails = parity.check_fill(ctx, ref, pairs[:3], arena)
+        assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+
+
+def test_edge_shapes(env):
+    """Lengths 1, block boundaries (15/16/17, 31/32/33), zero bands, bands
+    wider than the matrix."""
+    ctx, ref, rest = env
+    rng = np.random.default_rng(7)
+    rows = []
+    for rl in (1, 2, 15, 16, 17, 31, 32, 33, 47, 48, 64, 65):
+        for dg in (0, 1, -1, 5):
+            gl = max(1, rl + dg)
+            for variant in (0, 1, 2):
+                if variant == 1 and gl < rl:
+                    continue
+                if variant == 2 and gl > rl:
+                    continue
+                for lb_extra, ub_extra in ((0, 0), (1, 2), (40, 40)):
+                    rows.append((rl, gl, variant, lb_extra, ub_extra))
+    pairs, arena = cases.random_cases(0, 1)
+    out = np.zeros(len(rows) * 2, dtype=gdp.PAIR_DTYPE)
+    chunks, off = [], 0
+    for j, (rl, gl, variant, le, ue) in enumerate(rows):
+        for prec_i, prec in enumerate((8, 16)):
+            q = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=rl)
+            gq = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=gl)
+            gq[:min(rl, gl)] = q[:min(rl, gl)]
+            p = out[2 * j + prec_i]
+            chunks += [q, q, gq, gq]
+            p["rseq"], p["rseq_uc"], p["gseq"], p["gseq_alt"] = off, off + rl, off + 2 * rl, off + 2 * rl + gl
+            off += 2 * rl + 2 * gl
+            p["rlength"], p["glength"], p["variant"], p["precision"] = rl, gl, variant, prec
+            if variant == 0:
+                p["lband"], p["uband"] = max(0, rl - gl) + le, max(0, gl - rl) + ue
+            elif variant == 1:
+                p["uband"] = gl - rl + ue
+            else:
+                p["lband"] = rl - gl + le
+            p["open"], p["extend"], p["mismatchtype"] = -8, -3, 0
+            p["flags"] = gdp.FLAG_TRACEBACK | (gdp.FLAG_JUMP_LATE if j % 2 else 0)
+            p["tb_r"], p["tb_c"] = rl, gl
+            p["genomeoffset"], p["chrhigh"], p["watsonp"], p["dynprogindex"] = 100, 60000, 1, 1
+    arena = np.concatenate(chunks).astype(np.uint8)
+    fails = parity.check_fill(ctx, ref, out, arena)
+    assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, out, arena)
+    assert not fails, "\n".join(fails)
+
+
+def test_golden_vectors(env, gdplib):
+    """The committed golden vectors (recorded from the reference's compiled
+    functions) reproduce on the GPU: final scores, traceback stats, and a
+    digest of every record."""
+    ctx, _, _ = env
+    path = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+    z = np.load(path)
+    pairs, arena = z["pairs"], z["arena"]
+    gctx = gdp.Context(gdplib)
+    gctx.set_genome(z["genome_blocks"], z["genome_alt"], int(z["genome_length"]))
+    res, recs = gctx.align(pairs, arena)
+    defined = z["defined"].astype(bool)
+    assert np.array_equal(res["score"], z["score"])
+    assert (res["status"][defined] == 0).all()
+    stats = np.stack([res[k] for k in ("tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs")], 1)
+    assert np.array_equal(stats[defined], z["stats"][defined])
+    offs = np.concatenate([[0], np.cumsum(z["stats"][:, 5])])
+    for i in np.nonzero(defined)[0]:
+        r0 = int(res["rec_offset"][i])
+        g = recs[r0:r0 + int(res["nrecs"][i])]
+        assert g.tobytes() == z["recs"][offs[i]:offs[i + 1]].tobytes(), f"pair {i}"
+    gctx.close()
+
+
+def test_batch_determinism_and_launches(env, gdplib):
+    """Two runs of the same batch give identical bytes, and every run launches
+    this library's kernels (no host fallback exists)."""
+    ctx, _, _ = env
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 77, GENOME['g'], 2000)
+    before = ctx.launches()
+    r1, c1 = ctx.align(pairs, arena)
+    mid = ctx.launches()
+    r2, c2 = ctx.align(pairs, arena)
+    assert mid > before
+    assert r1.tobytes() == r2.tobytes() and c1.tobytes() == c2.tobytes()

@@ -1,0 +1,116 @@
+"""The oracle is pinned before it is trusted (CPU only).
+
+* The restatement (oracle/gdp_oracle.c) reproduces the committed golden
+  vectors, which were recorded from the reference's own compiled functions
+  (tests/golden/make_golden.py): final scores, traceback scores and counts,
+  every Pair record, and a digest of the in-band scores and directions.
+* Where the reference library (oracle/_ref, built from the reference
+  sources) is present, the restatement also matches it live on fresh
+  seeded cases, and both build identical substitution tables.
+* libgdp's own host-built tables equal the reference's for every mode.
+"""
+import ctypes
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import gdp
+import oracle as orc
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+
+
+def _digest(out, p):
+    m = orc.domain_mask(int(p["variant"]), int(p["rlength"]), int(p["glength"]),
+                        int(p["lband"]), int(p["uband"])).ravel()
+    h = hashlib.sha1()
+    for k in ("H", "dN", "dE", "dF"):
+        h.update(np.ascontiguousarray(out[k][m]).tobytes())
+    return np.frombuffer(h.digest(), np.uint8)
+
+
+def _golden_precision(pairs, i, o8, restatement, arena):
+    p = pairs[i]
+    if not (p["flags"] & gdp.FLAG_RERUN16):
+        return int(p["precision"])
+    m = orc.domain_mask(int(p["variant"]), int(p["rlength"]), int(p["glength"]),
+                        int(p["lband"]), int(p["uband"])).ravel()
+    return 16 if ((o8["H"][m] >= 127).any() or o8["score"] <= -98) else 8
+
+
+def test_restatement_matches_golden(restatement):
+    z = np.load(GOLDEN)
+    pairs, arena = z["pairs"], z["arena"]
+    restatement.set_genome(z["genome_blocks"], z["genome_alt"], int(z["genome_length"]))
+    offs = np.concatenate([[0], np.cumsum(z["stats"][:, 5])])
+    for i in range(pairs.size):
+        q = pairs[i:i + 1].copy()
+        if q["flags"][0] & gdp.FLAG_RERUN16:
+            q["precision"] = _golden_precision(pairs, i, restatement.align(q.copy(), 0, arena),
+                                               restatement, arena)
+        out = restatement.align(q, 0, arena)
+        assert out["score"] == z["score"][i], i
+        assert np.array_equal(_digest(out, q[0]), z["fill_digest"][i]), i
+        if z["defined"][i]:
+            assert np.array_equal(out["stats"], z["stats"][i]), i
+            assert out["recs"].tobytes() == z["recs"][offs[i]:offs[i + 1]].tobytes(), i
+
+
+@pytest.mark.parametrize("seed", [31, 32])
+def test_restatement_matches_reference_live(reference, restatement, seed):
+    restatement.lib.orc_last_tb_stale.restype = ctypes.c_int
+    g, blocks, altb = cases.genome(seed, length=1 << 17)
+    reference.set_genome(blocks, altb, g.size)
+    restatement.set_genome(blocks, altb, g.size)
+    pairs, arena = cases.random_cases(seed, 300)
+    for i in range(pairs.size):
+        a = reference.align(pairs, i, arena)
+        b = restatement.align(pairs, i, arena)
+        p = pairs[i]
+        m = orc.domain_mask(int(p["variant"]), int(p["rlength"]), int(p["glength"]),
+                            int(p["lband"]), int(p["uband"])).ravel()
+        for k in ("H", "dN", "dE", "dF"):
+            assert np.array_equal(a[k][m], b[k][m]), (i, k)
+        assert a["score"] == b["score"], i
+        if not restatement.lib.orc_last_tb_stale():
+            assert np.array_equal(a["stats"], b["stats"]), i
+            assert a["recs"].tobytes() == b["recs"].tobytes(), i
+
+
+@pytest.mark.parametrize("mode", range(7))
+def test_tables_match_reference(reference, restatement, gdplib, mode):
+    reference.init(mode)
+    restatement.init(mode)
+    pd, cons, nt = gdp.tables(gdplib, mode)
+    probe = list(range(128))
+    rng = np.random.default_rng(mode)
+    for mt in range(4):
+        for c1 in probe:
+            for c2 in rng.choice(128, 24, replace=False).tolist() + [ord("A"), ord("N"), ord("z"), 4]:
+                v = reference.pairdistance(mt, c1, c2)
+                assert pd[mt, c1, c2] == v, (mode, mt, c1, c2)
+                assert restatement.pairdistance(mt, c1, c2) == v
+    strands = [0] if mode in (0, 1, 3, 5) else [1, 2]
+    for gs in strands:
+        for c1 in probe:
+            for c2 in probe:
+                v = reference.consistent(gs, c1, c2)
+                assert cons[gs, c1, c2] == v, (mode, gs, c1, c2)
+    reference.init(0)
+    restatement.init(0)
+
+
+def test_product_tables_standard_shape(gdplib):
+    """Spot values of Dynprog_init's tables (src/dynprog.c:1069-1140) in
+    libgdp's own tables, checkable without the reference sources."""
+    pd, cons, nt = gdp.tables(gdplib, 0)
+    A, C, G, T, N = (ord(c) for c in "ACGTN")
+    assert pd[0, A, A] == 3 and pd[0, A, C] == -3 and pd[1, A, C] == -2
+    assert pd[2, A, C] == -1 and pd[3, A, C] == -5
+    assert pd[0, ord("R"), A] == 1 and pd[0, N, N] == 3 and pd[0, ord("a"), A] == 3
+    assert pd[0, A, ord("z")] == 0 and pd[0, ord("*"), A] == 0
+    assert nt[A] == 0 and nt[ord("t")] == 3 and nt[N] == 4 and nt[ord("*")] == 4
+    assert cons[0, ord("R"), G] == 1 and cons[0, A, C] == 0
