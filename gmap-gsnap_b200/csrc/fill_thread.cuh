@@ -264,6 +264,7 @@ fill_thread_kernel (FillParams P) {
     const bool swept = (g.Y >= y0l && g.Y <= y1l);
     if (MODE == 1) {
       mp->maxh16 = maxh;
+      mp->final16 = final_score;
     }
     if (MODE == 2) {
       const bool overflow = aborted || maxh >= HI || final_score <= -128 + 30;
@@ -281,5 +282,24 @@ fill_thread_kernel (FillParams P) {
       r->rerun = (MODE == 1) ? 1 : 0;
       if (!swept) r->status = GDP_ERR_BAND;
     }
+  }
+}
+
+/* Keeps the rerun pairs whose 16-bit in-band maximum stays below 127: only
+   those need the 8-bit pass (the others provably overflow in 8 bits). */
+__global__ void
+compact_rerun_kernel (const int32_t *list, const int32_t *count, const gdp_meta_t *meta,
+                      int32_t *out, int32_t *out_count) {
+  const int n = *count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int pi = list[i];
+    const bool need = meta[pi].maxh16 < 127;
+    const unsigned mask = __ballot_sync(__activemask(), need);
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    const int leader = __ffs(mask) - 1;
+    if (mask && lane == leader) base = atomicAdd(out_count, __popc(mask));
+    base = __shfl_sync(__activemask(), base, leader < 0 ? 0 : leader);
+    if (need) out[base + __popc(mask & ((1u << lane) - 1))] = pi;
   }
 }

@@ -113,7 +113,7 @@ typedef struct gdp_meta {
   int32_t maxh16;     /* largest in-band 16-bit score (rerun pairs) */
   int32_t status8;    /* 8-bit pass: 0 = kept, 1 = overflowed (use 16-bit) */
   int32_t final8;     /* 8-bit final score */
-  int32_t pad;
+  int32_t final16;    /* 16-bit final score (rerun pairs) */
 } gdp_meta_t;
 
 #endif

@@ -1,23 +1,33 @@
 /*
  * runtime.cu -- host runtime and C ABI of libgdp (include/gdp.h).
  *
- * A context owns a CUDA stream, the device copy of the substitution tables
- * (built as Dynprog_init builds them), an optional resident genome, and
- * growable device buffers.  A batch is planned on the host: pairs are
- * validated, binned by fill kind (lane width W, variant, tie rule, pass)
- * and sorted by work within each bin so that the threads of a warp run
- * pairs of similar size; direction storage and traceback record slots are
- * laid out by prefix sums.  Execution enqueues one fill kernel per
- * non-empty bin and one traceback kernel, all on the context stream.
+ * A context owns a compute stream and two copy streams, the device copy of
+ * the substitution tables (built as Dynprog_init builds them), an optional
+ * resident genome, and grow-only device and pinned-host pools.
+ *
+ * Planning (host, O(n)): pairs are validated, binned by fill kind (lane
+ * width W, variant, tie rule, pass) and ordered by work inside each bin
+ * (bucketed), so that the threads of a warp run pairs of similar size;
+ * direction storage and traceback record slots are laid out by prefix sums.
+ * Execution enqueues one fill kernel per non-empty bin, the 8-bit pass of
+ * rerun pairs over a device-compacted list, one traceback kernel, and a
+ * device compaction of the Pair records (CUB scan + warp-per-pair gather).
+ *
+ * gdp_align_batch (host buffers) processes the batch in waves of at most
+ * `wave` pairs with two in-flight slots: while the GPU fills wave i, the host
+ * plans wave i+1, the copy streams move wave i+1's pairs in and wave i-1's
+ * results and records out.
  *
  * 8-bit pairs flagged GDP_FLAG_RERUN16 follow the overflow contract: the
  * 16-bit fill runs first and records the largest in-band score; when that
  * reaches 127 the 8-bit fill would overflow too (its in-band scores are
  * never below the 16-bit ones unless it saturates at the top), so the
  * 16-bit outputs are kept.  Otherwise the 8-bit fill runs and its outputs
- * are kept unless it reaches 127 in the band or ends at or below -98.
+ * are kept unless it reaches 127 in the band, ends at or below -98, or its
+ * traceback would read cells the 8-bit fill never wrote.
  */
 #include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -31,7 +41,7 @@
 #include "fill_thread.cuh"
 #include "traceback.cuh"
 
-#define GDP_VERSION "gdp-b200 0.1"
+#define GDP_VERSION "gdp-b200 0.2"
 
 namespace {
 
@@ -49,9 +59,28 @@ struct DevBuf {
     return e;
   }
   void release () { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+  template <class T> T *as () const { return (T *) p; }
+};
+
+struct HostBuf {   /* pinned host memory */
+  void *p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure (size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t grow = want + want / 4 + 4096;
+    cudaError_t e = cudaHostAlloc(&p, grow, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = grow;
+    return e;
+  }
+  void release () { if (p) cudaFreeHost(p); p = nullptr; bytes = 0; }
+  template <class T> T *as () const { return (T *) p; }
 };
 
 constexpr int NKINDS = 24;   /* (W32, variant, late, pass) */
+constexpr int NBUCKETS = 64; /* work buckets for ordering inside a bin */
 
 inline int kind_id (int w32, int variant, int late, int pass) {
   return (((w32 * 3 + variant) * 2 + late) * 2) + pass;
@@ -59,16 +88,61 @@ inline int kind_id (int w32, int variant, int late, int pass) {
 
 }  // namespace
 
+/* Host side of a plan (pinned so its upload is asynchronous). */
+struct PlanHost {
+  int64_t n = 0;
+  int64_t nlists = 0;
+  HostBuf lists, meta, status, rec_off;
+  int64_t start[NKINDS + 2] = {0};
+  int32_t counts[NKINDS + 1] = {0};
+  int maxY[NKINDS] = {0};
+  int64_t dir_words = 0, total_recs = 0;
+  void release () { lists.release(); meta.release(); status.release(); rec_off.release(); }
+};
+
+/* Device side of a plan. */
+struct PlanDev {
+  DevBuf lists, work, counts, work_counts, status, meta0, meta, rec_off, dirs, hdump;
+  DevBuf slots;        /* records, rlength + glength + 2 per traceback pair */
+  DevBuf nrec_scan;    /* int64 exclusive scan of records per pair */
+  DevBuf total;        /* int64 record total of the plan */
+  DevBuf cub_tmp;
+  void release () {
+    lists.release(); work.release(); counts.release(); work_counts.release(); status.release();
+    meta0.release(); meta.release(); rec_off.release(); dirs.release(); hdump.release();
+    slots.release(); nrec_scan.release(); total.release(); cub_tmp.release();
+  }
+};
+
+struct gdp_plan {
+  PlanHost h;
+  PlanDev d;
+};
+
+/* One in-flight wave of gdp_align_batch. */
+struct Slot {
+  PlanHost h;
+  PlanDev d;
+  DevBuf pairs, results, recs;
+  HostBuf total;           /* pinned int64: records of the wave */
+  cudaEvent_t h2d_done = nullptr, comp_done = nullptr, out_done = nullptr, total_ready = nullptr;
+  int64_t first = 0, count = 0, rec_base = 0;
+  bool busy = false;
+};
+
 struct gdp_ctx {
   int device = 0;
   int nsm = 148;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;        /* compute */
+  cudaStream_t h2d = nullptr, d2h = nullptr;
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
-  DevBuf pairs, arena, results, recs, scratch;
+  int64_t wave = 131072;
+  DevBuf arena, scratch;
+  Slot slot[2];
   std::atomic<int64_t> launches{0};
   std::string err;
   std::mutex mu;
@@ -80,13 +154,17 @@ struct gdp_ctx {
   int64_t prof_n[32] = {0};
 };
 
-/* kernel ids for profiling: 0..23 fill kinds, 24 traceback, 25 init */
+/* kernel ids for profiling: 0..23 fill kinds, 24 traceback, 25 init,
+   26 integer probe, 27 rerun compaction, 28 record compaction */
+#define NPROF 29
 static const char *
 kernel_name (int id) {
   static char buf[32][48];
   if (id == 24) return "traceback_kernel";
   if (id == 25) return "init_results_kernel";
   if (id == 26) return "int_peak_kernel";
+  if (id == 27) return "compact_rerun_kernel";
+  if (id == 28) return "compact_records_kernel";
   const int pass = id & 1, late = (id >> 1) & 1, vw = id >> 2, variant = vw % 3, w32 = vw / 3;
   snprintf(buf[id], sizeof(buf[id]), "fill_thread<W%d,%s,%s,%s>", w32 ? 32 : 16,
            variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early",
@@ -95,8 +173,7 @@ kernel_name (int id) {
 }
 
 static void
-prof_begin (gdp_ctx *ctx, int id, cudaEvent_t *a) {
-  (void) id;
+prof_begin (gdp_ctx *ctx, cudaEvent_t *a) {
   if (!ctx->profiling) return;
   cudaEventCreate(a);
   cudaEventRecord(*a, ctx->stream);
@@ -110,24 +187,6 @@ prof_end (gdp_ctx *ctx, int id, cudaEvent_t a) {
   cudaEventRecord(b, ctx->stream);
   ctx->timed.push_back({id, a, b});
 }
-
-struct gdp_plan {
-  int64_t n = 0;
-  std::vector<int32_t> lists;          /* kinds' lists, then the traceback list */
-  int64_t start[NKINDS + 2] = {0};
-  int32_t counts[NKINDS + 1] = {0};
-  int maxY[NKINDS] = {0};
-  std::vector<gdp_meta_t> meta;
-  std::vector<int64_t> rec_off;
-  std::vector<int32_t> status;
-  int64_t dir_words = 0, total_recs = 0;
-  /* device copies */
-  int32_t *d_lists = nullptr, *d_counts = nullptr, *d_status = nullptr;
-  gdp_meta_t *d_meta0 = nullptr, *d_meta = nullptr;
-  int64_t *d_rec_off = nullptr;
-  uint32_t *d_dirs = nullptr;
-  int16_t *d_hdump = nullptr;          /* debug: scores of every swept cell */
-};
 
 static int
 set_err (gdp_ctx *ctx, const char *what, cudaError_t e) {
@@ -144,26 +203,16 @@ gdp_version (void) {
   return GDP_VERSION;
 }
 
-extern "C" int
-gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
-  *out = nullptr;
-  if (mode < 0 || mode > 6) return GDP_ERR_PARAM;
-  gdp_ctx *ctx = new gdp_ctx();
-  ctx->device = device;
-  ctx->budget = budget > 0 ? budget : (int64_t) 40 << 30;
-  cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) { delete ctx; return GDP_ERR_CUDA; }
-  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GDP_ERR_CUDA; }
-  ctx->h_tab = (gdp_tables_t *) malloc(sizeof(gdp_tables_t));
-  gdp_build_tables(ctx->h_tab, mode);
-  if (cudaMalloc(&ctx->d_tab, sizeof(gdp_tables_t)) != cudaSuccess ||
-      cudaMemcpy(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice) != cudaSuccess) {
-    gdp_ctx_destroy(ctx);
-    return GDP_ERR_CUDA;
-  }
-  *out = ctx;
-  return GDP_OK;
+static void
+slot_release (Slot &sl) {
+  sl.d.release();
+  sl.h.release();
+  sl.pairs.release(); sl.results.release(); sl.recs.release(); sl.total.release();
+  if (sl.h2d_done) cudaEventDestroy(sl.h2d_done);
+  if (sl.comp_done) cudaEventDestroy(sl.comp_done);
+  if (sl.out_done) cudaEventDestroy(sl.out_done);
+  if (sl.total_ready) cudaEventDestroy(sl.total_ready);
+  sl.h2d_done = sl.comp_done = sl.out_done = sl.total_ready = nullptr;
 }
 
 extern "C" void
@@ -171,14 +220,54 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  ctx->pairs.release(); ctx->arena.release(); ctx->results.release();
-  ctx->recs.release(); ctx->scratch.release();
+  if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
+  if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
+  for (auto &t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+  for (int s = 0; s < 2; s++) slot_release(ctx->slot[s]);
+  ctx->arena.release(); ctx->scratch.release();
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
   if (ctx->d_genomealt) cudaFree(ctx->d_genomealt);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+  if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
   free(ctx->h_tab);
   delete ctx;
+}
+
+extern "C" int
+gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
+  *out = nullptr;
+  if (mode < 0 || mode > 6) return GDP_ERR_PARAM;
+  gdp_ctx *ctx = new gdp_ctx();
+  ctx->device = device;
+  ctx->budget = budget > 0 ? budget : (int64_t) 40 << 30;
+  if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return GDP_ERR_CUDA; }
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) != cudaSuccess) {
+    gdp_ctx_destroy(ctx);
+    return GDP_ERR_CUDA;
+  }
+  for (int s = 0; s < 2; s++) {
+    Slot &sl = ctx->slot[s];
+    cudaEventCreateWithFlags(&sl.h2d_done, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&sl.comp_done, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&sl.out_done, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&sl.total_ready, cudaEventDisableTiming);
+  }
+  ctx->h_tab = (gdp_tables_t *) malloc(sizeof(gdp_tables_t));
+  gdp_build_tables(ctx->h_tab, mode);
+  if (cudaMalloc(&ctx->d_tab, sizeof(gdp_tables_t)) != cudaSuccess ||
+      cudaMemcpy(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    gdp_ctx_destroy(ctx);
+    return GDP_ERR_CUDA;
+  }
+  const char *w = getenv("GDP_WAVE_PAIRS");
+  if (w && atol(w) > 0) ctx->wave = atol(w);
+  *out = ctx;
+  return GDP_OK;
 }
 
 extern "C" int
@@ -216,22 +305,26 @@ gdp_profile_enable (gdp_ctx *ctx, int on) {
   return GDP_OK;
 }
 
+static void
+prof_collect (gdp_ctx *ctx) {
+  if (ctx->timed.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &t : ctx->timed) {
+    float f = 0.f;
+    cudaEventElapsedTime(&f, t.a, t.b);
+    ctx->prof_ms[t.id] += f;
+    ctx->prof_n[t.id] += 1;
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  ctx->timed.clear();
+}
+
 extern "C" int
 gdp_profile_read (gdp_ctx *ctx, int id, char *name, int name_cap, double *ms, int64_t *launches) {
   std::lock_guard<std::mutex> lk(ctx->mu);
-  if (id < 0 || id >= 27) return GDP_ERR_PARAM;
-  if (!ctx->timed.empty()) {
-    cudaStreamSynchronize(ctx->stream);
-    for (auto &t : ctx->timed) {
-      float f = 0.f;
-      cudaEventElapsedTime(&f, t.a, t.b);
-      ctx->prof_ms[t.id] += f;
-      ctx->prof_n[t.id] += 1;
-      cudaEventDestroy(t.a);
-      cudaEventDestroy(t.b);
-    }
-    ctx->timed.clear();
-  }
+  if (id < 0 || id >= NPROF) return GDP_ERR_PARAM;
+  prof_collect(ctx);
   if (name && name_cap > 0) snprintf(name, name_cap, "%s", kernel_name(id));
   if (ms) *ms = ctx->prof_ms[id];
   if (launches) *launches = ctx->prof_n[id];
@@ -240,9 +333,8 @@ gdp_profile_read (gdp_ctx *ctx, int id, char *name, int name_cap, double *ms, in
 
 extern "C" int
 gdp_profile_reset (gdp_ctx *ctx) {
-  double dummy;
-  gdp_profile_read(ctx, 0, nullptr, 0, &dummy, nullptr);
   std::lock_guard<std::mutex> lk(ctx->mu);
+  prof_collect(ctx);
   for (int i = 0; i < 32; i++) { ctx->prof_ms[i] = 0; ctx->prof_n[i] = 0; }
   return GDP_OK;
 }
@@ -251,8 +343,8 @@ gdp_profile_reset (gdp_ctx *ctx) {
  * Integer issue-rate probe: every thread runs 16 independent dependency
  * chains of 32-bit add / min-max / multiply-add, so the SMs issue integer
  * lane-ops as fast as their pipes allow.  Used as the roofline denominator
- * of the integer-bound fill.  kind 0: IADD3 + IMNMX (ALU pipe), kind 1:
- * IMAD (FMA pipe), kind 2: both interleaved.
+ * of the integer-bound fill.  kind 0: add + min/max, kind 1: multiply-add,
+ * kind 2: both interleaved.  Each chain step counts as 2 lane-ops.
  */
 __global__ void __launch_bounds__(256)
 int_peak_kernel (int *out, int iters, int kind, int seed) {
@@ -264,9 +356,9 @@ int_peak_kernel (int *out, int iters, int kind, int seed) {
 #pragma unroll
     for (int k = 0; k < 16; k++) {
       if (kind == 0) {
-        a[k] = max(a[k] + b, c - k);          /* 2 ops */
+        a[k] = max(a[k] + b, c - k);
       } else if (kind == 1) {
-        a[k] = a[k] * b + c;                  /* 1 op (IMAD) */
+        a[k] = a[k] * b + c;
         a[k] = a[k] * c + b;
       } else {
         if (k & 1) a[k] = max(a[k] + b, c - k);
@@ -298,6 +390,7 @@ gdp_measure_int_peak (gdp_ctx *ctx) {
       int_peak_kernel<<<blocks, threads, 0, ctx->stream>>>(d, iters, kind, 12345 + rep);
       cudaEventRecord(b, ctx->stream);
       cudaEventSynchronize(b);
+      ctx->launches++;
       float ms = 0.f;
       cudaEventElapsedTime(&ms, a, b);
       const double ops = (double) blocks * threads * iters * 16 * 2;
@@ -318,11 +411,14 @@ gdp_sync (gdp_ctx *ctx) {
 
 extern "C" int
 gdp_set_genome (gdp_ctx *ctx, const uint32_t *blocks, const uint32_t *altblocks, uint64_t len) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
   size_t words = (size_t) ((len + 31) / 32) * 3;
   cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
   if (ctx->d_genomealt) cudaFree(ctx->d_genomealt);
   ctx->d_genome = ctx->d_genomealt = nullptr;
+  ctx->genome_len = 0;
   CK(ctx, cudaMalloc(&ctx->d_genome, words * 4));
   CK(ctx, cudaMemcpy(ctx->d_genome, blocks, words * 4, cudaMemcpyHostToDevice));
   if (altblocks) {
@@ -338,7 +434,7 @@ gdp_set_genome (gdp_ctx *ctx, const uint32_t *blocks, const uint32_t *altblocks,
 /* ------------------------------------------------------------------ */
 
 static int
-validate (const gdp_pair_t &p) {
+validate (const gdp_pair_t &p, int64_t arena_bytes) {
   if (p.variant < GDP_FULL || p.variant > GDP_LOWER) return GDP_ERR_PARAM;
   if (p.precision != 8 && p.precision != 16) return GDP_ERR_PARAM;
   if (p.mismatchtype < 0 || p.mismatchtype > 3) return GDP_ERR_PARAM;
@@ -346,132 +442,167 @@ validate (const gdp_pair_t &p) {
   if (p.genestrand < 0 || p.genestrand > 2) return GDP_ERR_PARAM;
   if (p.rlength <= 0 || p.glength <= 0 || p.rlength > (1 << 20) || p.glength > (1 << 20)) return GDP_ERR_LEN;
   if (p.lband < 0 || p.uband < 0) return GDP_ERR_BAND;
+  if (arena_bytes >= 0) {
+    if (p.rseq < 0 || p.rseq + p.rlength > arena_bytes || p.rseq_uc < 0 || p.rseq_uc + p.rlength > arena_bytes ||
+        p.gseq < 0 || p.gseq + p.glength > arena_bytes || p.gseq_alt < 0 || p.gseq_alt + p.glength > arena_bytes)
+      return GDP_ERR_LEN;
+  }
   if (p.flags & GDP_FLAG_TRACEBACK) {
     if (p.tb_r < 0 || p.tb_c < 0 || p.tb_r > p.rlength || p.tb_c > p.glength) return GDP_ERR_BAND;
   }
   return GDP_OK;
 }
 
-static int64_t
-work_of (const gdp_pair_t &p, int W) {
-  return gdp_pair_words(&p, W);
+static inline int
+bucket_of (int64_t work) {
+  int b = 0;
+  while (work > 1 && b < NBUCKETS - 1) { work >>= 1; b++; }
+  return b;
 }
 
-static void
-plan_free_device (gdp_plan *pl) {
-  cudaFree(pl->d_lists); cudaFree(pl->d_counts); cudaFree(pl->d_status);
-  cudaFree(pl->d_meta0); cudaFree(pl->d_meta); cudaFree(pl->d_rec_off);
-  cudaFree(pl->d_dirs); cudaFree(pl->d_hdump);
-  pl->d_lists = pl->d_counts = pl->d_status = nullptr;
-  pl->d_meta0 = pl->d_meta = nullptr;
-  pl->d_rec_off = nullptr; pl->d_dirs = nullptr; pl->d_hdump = nullptr;
-}
-
+/* Fills ph for pairs[0..n) (pinned host buffers).  arena_bytes < 0 skips the
+   arena bound checks (device-resident callers). */
 static int
-plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, bool hdump, gdp_plan **out) {
-  gdp_plan *pl = new gdp_plan();
-  pl->n = n;
-  pl->meta.resize(n);
-  pl->rec_off.assign(n, 0);
-  pl->status.assign(n, GDP_OK);
-  std::vector<std::vector<std::pair<int64_t, int32_t>>> bins(NKINDS);
-  std::vector<int32_t> tb;
-  int64_t words = 0, recs = 0;
+plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_bytes, PlanHost &ph) {
+  ph.n = n;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = ph.meta.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_meta_t));
+  if (e == cudaSuccess) e = ph.status.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
+  if (e == cudaSuccess) e = ph.rec_off.ensure(std::max<int64_t>(n, 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = ph.lists.ensure(std::max<int64_t>(3 * n, 1) * sizeof(int32_t));
+  if (e != cudaSuccess) return set_err(ctx, "pinned plan buffers", e);
+  gdp_meta_t *meta = ph.meta.as<gdp_meta_t>();
+  int32_t *status = ph.status.as<int32_t>();
+  int64_t *rec_off = ph.rec_off.as<int64_t>();
+  /* counting sort by (kind, work bucket) */
+  std::vector<int64_t> cnt((size_t) NKINDS * NBUCKETS, 0);
+  std::vector<uint16_t> key1(n, 0xffff), key2(n, 0xffff);
+  int64_t words = 0, recs = 0, ntb = 0;
+  int maxY[NKINDS] = {0};
   for (int64_t i = 0; i < n; i++) {
     const gdp_pair_t &p = pairs[i];
-    gdp_meta_t &m = pl->meta[i];
+    gdp_meta_t &m = meta[i];
     m.dir16 = m.dir8 = -1;
-    m.maxh16 = -32768; m.status8 = 0; m.final8 = 0; m.pad = 0;
-    int st = validate(p);
-    pl->status[i] = st;
+    m.maxh16 = -32768; m.status8 = 0; m.final8 = 0; m.final16 = 0;
+    rec_off[i] = 0;
+    const int st = validate(p, arena_bytes);
+    status[i] = st;
     if (st != GDP_OK) continue;
     const int late = (p.flags & GDP_FLAG_JUMP_LATE) ? 1 : 0;
     const bool rerun = p.precision == 8 && (p.flags & GDP_FLAG_RERUN16);
-    gdp_geom_t g16, g8;
-    gdp_geom_of(&p, 16, &g16);
-    gdp_geom_of(&p, 32, &g8);
+    const int Y = (p.variant == GDP_LOWER) ? p.rlength : p.glength;
     if (p.precision == 16 || rerun) {
+      const int64_t w = gdp_pair_words(&p, 16);
+      const int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
       m.dir16 = words;
-      words += (gdp_pair_words(&p, 16) + 3) & ~(int64_t) 3;   /* keep blocks 16-byte aligned */
-      bins[kind_id(0, p.variant, late, rerun ? 1 : 0)].push_back({work_of(p, 16), (int32_t) i});
+      words += (w + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
+      key1[i] = (uint16_t) (k * NBUCKETS + bucket_of(w));
+      cnt[key1[i]]++;
+      maxY[k] = std::max(maxY[k], Y);
     }
     if (p.precision == 8) {
+      const int64_t w = gdp_pair_words(&p, 32);
+      const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
       m.dir8 = words;
-      words += (gdp_pair_words(&p, 32) + 3) & ~(int64_t) 3;
-      bins[kind_id(1, p.variant, late, rerun ? 1 : 0)].push_back({work_of(p, 32), (int32_t) i});
+      words += (w + 3) & ~(int64_t) 3;
+      key2[i] = (uint16_t) (k * NBUCKETS + bucket_of(w));
+      cnt[key2[i]]++;
+      maxY[k] = std::max(maxY[k], Y);
     }
     if (p.flags & GDP_FLAG_TRACEBACK) {
-      pl->rec_off[i] = recs;
+      rec_off[i] = recs;
       recs += (int64_t) p.rlength + p.glength + 2;
-      tb.push_back((int32_t) i);
+      ntb++;
     }
   }
-  pl->dir_words = words;
-  pl->total_recs = recs;
-  int64_t at = 0;
+  /* offsets: kinds in order, heaviest bucket first inside a kind */
+  std::vector<int64_t> at((size_t) NKINDS * NBUCKETS, 0);
+  int64_t pos = 0;
   for (int k = 0; k < NKINDS; k++) {
-    auto &b = bins[k];
-    std::stable_sort(b.begin(), b.end(), [](const std::pair<int64_t, int32_t> &a,
-                                            const std::pair<int64_t, int32_t> &c) { return a.first > c.first; });
-    pl->start[k] = at;
-    pl->counts[k] = (int32_t) b.size();
-    int maxY = 0;
-    for (auto &e : b) {
-      pl->lists.push_back(e.second);
-      const gdp_pair_t &p = pairs[e.second];
-      maxY = std::max(maxY, p.variant == GDP_LOWER ? p.rlength : p.glength);
+    ph.start[k] = pos;
+    int64_t c = 0;
+    for (int b = NBUCKETS - 1; b >= 0; b--) {
+      at[(size_t) k * NBUCKETS + b] = pos;
+      pos += cnt[(size_t) k * NBUCKETS + b];
+      c += cnt[(size_t) k * NBUCKETS + b];
     }
-    pl->maxY[k] = maxY;
-    at += (int64_t) b.size();
+    ph.counts[k] = (int32_t) c;
+    ph.maxY[k] = maxY[k];
   }
-  pl->start[NKINDS] = at;
-  pl->counts[NKINDS] = (int32_t) tb.size();
-  for (int32_t i : tb) pl->lists.push_back(i);
-  pl->start[NKINDS + 1] = at + (int64_t) tb.size();
-
-  cudaSetDevice(ctx->device);
-  const size_t nl = std::max<size_t>(pl->lists.size(), 1);
-  cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_lists, nl * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_counts, (NKINDS + 1) * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_status, std::max<int64_t>(n, 1) * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_meta0, std::max<int64_t>(n, 1) * sizeof(gdp_meta_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_meta, std::max<int64_t>(n, 1) * sizeof(gdp_meta_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_rec_off, std::max<int64_t>(n, 1) * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&pl->d_dirs, std::max<int64_t>(words, 4) * sizeof(uint32_t));
-  if (e == cudaSuccess && hdump) e = cudaMalloc(&pl->d_hdump, std::max<int64_t>(words, 4) * 8 * sizeof(int16_t));
-  if (e == cudaSuccess && !pl->lists.empty())
-    e = cudaMemcpy(pl->d_lists, pl->lists.data(), pl->lists.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(pl->d_counts, pl->counts, (NKINDS + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && n > 0) {
-    e = cudaMemcpy(pl->d_status, pl->status.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(pl->d_meta0, pl->meta.data(), n * sizeof(gdp_meta_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(pl->d_rec_off, pl->rec_off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice);
+  ph.start[NKINDS] = pos;
+  ph.counts[NKINDS] = (int32_t) ntb;
+  int64_t tbpos = pos;
+  pos += ntb;
+  ph.start[NKINDS + 1] = pos;
+  ph.nlists = pos;
+  int32_t *lists = ph.lists.as<int32_t>();
+  for (int64_t i = 0; i < n; i++) {
+    if (key1[i] != 0xffff) lists[at[key1[i]]++] = (int32_t) i;
+    if (key2[i] != 0xffff) lists[at[key2[i]]++] = (int32_t) i;
+    if (status[i] == GDP_OK && (pairs[i].flags & GDP_FLAG_TRACEBACK)) lists[tbpos++] = (int32_t) i;
   }
-  if (e != cudaSuccess) {
-    plan_free_device(pl);
-    delete pl;
-    return set_err(ctx, "plan allocation", e);
-  }
-  *out = pl;
+  ph.dir_words = words;
+  ph.total_recs = recs;
   return GDP_OK;
 }
 
-extern "C" int
-gdp_plan_create (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, gdp_plan **plan) {
-  return plan_build(ctx, pairs, npairs, false, plan);
+/* Device buffers for ph and the async upload of the plan on stream s. */
+static int
+plan_upload (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, bool hdump, cudaStream_t s) {
+  const int64_t n = std::max<int64_t>(ph.n, 1);
+  const size_t nl = (size_t) std::max<int64_t>(ph.nlists, 1);
+  CK(ctx, pd.lists.ensure(nl * sizeof(int32_t)));
+  CK(ctx, pd.work.ensure(nl * sizeof(int32_t)));
+  CK(ctx, pd.counts.ensure((NKINDS + 1) * sizeof(int32_t)));
+  CK(ctx, pd.work_counts.ensure(NKINDS * sizeof(int32_t)));
+  CK(ctx, pd.status.ensure(n * sizeof(int32_t)));
+  CK(ctx, pd.meta0.ensure(n * sizeof(gdp_meta_t)));
+  CK(ctx, pd.meta.ensure(n * sizeof(gdp_meta_t)));
+  CK(ctx, pd.rec_off.ensure(n * sizeof(int64_t)));
+  CK(ctx, pd.dirs.ensure(std::max<int64_t>(ph.dir_words, 4) * sizeof(uint32_t)));
+  CK(ctx, pd.total.ensure(sizeof(int64_t)));
+  if (hdump) CK(ctx, pd.hdump.ensure(std::max<int64_t>(ph.dir_words, 4) * 8 * sizeof(int16_t)));
+  if (ph.nlists > 0)
+    CK(ctx, cudaMemcpyAsync(pd.lists.p, ph.lists.p, ph.nlists * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(pd.counts.p, ph.counts, (NKINDS + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (ph.n > 0) {
+    CK(ctx, cudaMemcpyAsync(pd.status.p, ph.status.p, ph.n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CK(ctx, cudaMemcpyAsync(pd.meta0.p, ph.meta.p, ph.n * sizeof(gdp_meta_t), cudaMemcpyHostToDevice, s));
+    CK(ctx, cudaMemcpyAsync(pd.rec_off.p, ph.rec_off.p, ph.n * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  }
+  return GDP_OK;
 }
 
 extern "C" void
 gdp_plan_destroy (gdp_plan *pl) {
   if (!pl) return;
-  plan_free_device(pl);
+  pl->d.release();
+  pl->h.release();
   delete pl;
 }
 
-extern "C" int64_t gdp_plan_total_recs (const gdp_plan *pl) { return pl->total_recs; }
-extern "C" int64_t gdp_plan_rec_offset (const gdp_plan *pl, int64_t i) { return pl->rec_off[i]; }
-extern "C" int64_t gdp_plan_dir_bytes (const gdp_plan *pl) { return pl->dir_words * 4; }
+extern "C" int
+gdp_plan_create (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, gdp_plan **plan) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  gdp_plan *pl = new gdp_plan();
+  int rc = plan_build(ctx, pairs, npairs, -1, pl->h);
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl->h, pl->d, false, ctx->stream);
+  if (rc == GDP_OK) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = set_err(ctx, "plan upload", e);
+  }
+  if (rc != GDP_OK) {
+    gdp_plan_destroy(pl);
+    return rc;
+  }
+  *plan = pl;
+  return GDP_OK;
+}
+
+extern "C" int64_t gdp_plan_total_recs (const gdp_plan *pl) { return pl->h.total_recs; }
+extern "C" int64_t gdp_plan_rec_offset (const gdp_plan *pl, int64_t i) { return pl->h.rec_off.as<int64_t>()[i]; }
+extern "C" int64_t gdp_plan_dir_bytes (const gdp_plan *pl) { return pl->h.dir_words * 4; }
 
 /* ------------------------------------------------------------------ */
 /* Execution                                                           */
@@ -492,7 +623,32 @@ init_results_kernel (gdp_result_t *res, const int32_t *status, const gdp_pair_t 
   }
 }
 
-typedef void (*fill_fn)(FillParams);
+__global__ void
+gather_nrecs_kernel (const gdp_result_t *res, int64_t n, int64_t *out) {
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+    out[i] = res[i].nrecs;
+}
+
+/* Copies each pair's records from its slot range to the dense position
+   given by the exclusive scan (one warp per pair), points the pair's
+   result at it (offset relative to the batch), and writes the total. */
+__global__ void
+compact_records_kernel (gdp_result_t *res, const int64_t *slot_off, const gdp_rec_t *slots,
+                        const int64_t *scan, int64_t n, gdp_rec_t *out, int64_t *total) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = warp; i < n; i += nwarps) {
+    const int nr = res[i].nrecs;
+    const int64_t dst = scan[i];
+    const gdp_rec_t *src = slots + slot_off[i];
+    for (int k = lane; k < nr; k += 32) out[dst + k] = src[k];
+    if (lane == 0) {
+      res[i].rec_offset = dst;
+      if (i == n - 1) *total = dst + nr;
+    }
+  }
+}
 
 template <int W, int V, bool L, int M>
 static void launch_fill (FillParams P, int grid, cudaStream_t s) {
@@ -514,24 +670,31 @@ launch_kind (int k, FillParams P, int grid, cudaStream_t s) {
 #undef GDP_CASE
 }
 
+static inline int
+fill_grid (gdp_ctx *ctx, int64_t count) {
+  return (int) std::max<int64_t>(1, std::min<int64_t>((count + 127) / 128, (int64_t) ctx->nsm * 16));
+}
+
+/* Enqueues fills and tracebacks of a planned batch on the compute stream.
+   d_slots receives records at the plan's slot offsets. */
 static int
-plan_run (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *d_pairs, const char *d_arena,
-          gdp_result_t *d_res, gdp_rec_t *d_recs) {
+plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
+          gdp_result_t *d_res, gdp_rec_t *d_slots) {
   cudaStream_t s = ctx->stream;
-  const int64_t n = pl->n;
+  const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
   cudaEvent_t ev0 = nullptr;
-  prof_begin(ctx, 25, &ev0);
-  init_results_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(d_res, pl->d_status, d_pairs, n);
+  prof_begin(ctx, &ev0);
+  init_results_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
+      d_res, pd.status.as<int32_t>(), d_pairs, n);
   prof_end(ctx, 25, ev0);
   ctx->launches++;
-  CK(ctx, cudaMemcpyAsync(pl->d_meta, pl->d_meta0, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToDevice, s));
-  /* scratch for the largest kind */
+  CK(ctx, cudaGetLastError());
+  CK(ctx, cudaMemcpyAsync(pd.meta.p, pd.meta0.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToDevice, s));
   size_t need = 0;
   for (int k = 0; k < NKINDS; k++) {
-    if (!pl->counts[k]) continue;
-    const int64_t grid = std::min<int64_t>((pl->counts[k] + 127) / 128, (int64_t) ctx->nsm * 16);
-    need = std::max(need, (size_t) (pl->maxY[k] + 1) * (size_t) grid * 128 * sizeof(int2));
+    if (!ph.counts[k]) continue;
+    need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
   CK(ctx, ctx->scratch.ensure(std::max<size_t>(need, 64)));
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs */
@@ -539,46 +702,88 @@ plan_run (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *d_pairs, const char *d_a
     for (int k = 0; k < NKINDS; k++) {
       const int w32 = (k >> 2) / 3, pass = k & 1;
       const bool second = (w32 == 1 && pass == 1);
-      if ((round == 0) == second || !pl->counts[k]) continue;
-      const int grid = (int) std::min<int64_t>((pl->counts[k] + 127) / 128, (int64_t) ctx->nsm * 16);
+      if ((round == 0) == second || !ph.counts[k]) continue;
+      const int grid = fill_grid(ctx, ph.counts[k]);
       FillParams P;
       P.pairs = d_pairs; P.arena = d_arena;
-      P.list = pl->d_lists + pl->start[k];
-      P.count = pl->d_counts + k;
-      P.dirs = pl->d_dirs;
-      P.hdump = pl->d_hdump;
-      P.meta = pl->d_meta;
+      P.list = pd.lists.as<int32_t>() + ph.start[k];
+      P.count = pd.counts.as<int32_t>() + k;
+      if (second) {
+        /* only the pairs whose 16-bit maximum stayed below 127 run the 8-bit pass */
+        CK(ctx, cudaMemsetAsync(pd.work_counts.as<int32_t>() + k, 0, sizeof(int32_t), s));
+        const int cg = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
+        cudaEvent_t evc = nullptr;
+        prof_begin(ctx, &evc);
+        compact_rerun_kernel<<<cg, 256, 0, s>>>(P.list, P.count, pd.meta.as<gdp_meta_t>(),
+                                                pd.work.as<int32_t>() + ph.start[k],
+                                                pd.work_counts.as<int32_t>() + k);
+        prof_end(ctx, 27, evc);
+        ctx->launches++;
+        CK(ctx, cudaGetLastError());
+        P.list = pd.work.as<int32_t>() + ph.start[k];
+        P.count = pd.work_counts.as<int32_t>() + k;
+      }
+      P.dirs = pd.dirs.as<uint32_t>();
+      P.hdump = pd.hdump.as<int16_t>();
+      P.meta = pd.meta.as<gdp_meta_t>();
       P.res = d_res;
-      P.scratch = (int2 *) ctx->scratch.p;
+      P.scratch = ctx->scratch.as<int2>();
       P.nslots = (int64_t) grid * 128;
-      P.scratch_rows = pl->maxY[k] + 1;
+      P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
       cudaEvent_t ev = nullptr;
-      prof_begin(ctx, k, &ev);
+      prof_begin(ctx, &ev);
       launch_kind(k, P, grid, s);
       prof_end(ctx, k, ev);
       ctx->launches++;
       CK(ctx, cudaGetLastError());
     }
   }
-  if (pl->counts[NKINDS] > 0) {
+  if (ph.counts[NKINDS] > 0) {
     TbParams T;
     T.pairs = d_pairs; T.arena = d_arena;
-    T.list = pl->d_lists + pl->start[NKINDS];
-    T.count = pl->d_counts + NKINDS;
-    T.dirs = pl->d_dirs; T.meta = pl->d_meta; T.res = d_res; T.recs = d_recs;
-    T.rec_off = pl->d_rec_off;
+    T.list = pd.lists.as<int32_t>() + ph.start[NKINDS];
+    T.count = pd.counts.as<int32_t>() + NKINDS;
+    T.dirs = pd.dirs.as<uint32_t>(); T.meta = pd.meta.as<gdp_meta_t>(); T.res = d_res; T.recs = d_slots;
+    T.rec_off = pd.rec_off.as<int64_t>();
     T.genome = ctx->d_genome; T.genomealt = ctx->d_genomealt;
     T.genome_len = ctx->genome_len;
     T.tab = ctx->d_tab;
-    const int grid = (int) std::min<int64_t>((pl->counts[NKINDS] + 127) / 128, (int64_t) ctx->nsm * 16);
     cudaEvent_t ev = nullptr;
-    prof_begin(ctx, 24, &ev);
-    traceback_kernel<<<grid, 128, 0, s>>>(T);
+    prof_begin(ctx, &ev);
+    traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, s>>>(T);
     prof_end(ctx, 24, ev);
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
+  return GDP_OK;
+}
+
+/* Dense records after plan_run: scan of nrecs, gather into `out`, total in
+   pd.total. */
+static int
+compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_res, const gdp_rec_t *d_slots,
+                 gdp_rec_t *out) {
+  cudaStream_t s = ctx->stream;
+  const int64_t n = ph.n;
+  if (n == 0) return GDP_OK;
+  CK(ctx, pd.nrec_scan.ensure((2 * n + 1) * sizeof(int64_t)));
+  int64_t *counts = pd.nrec_scan.as<int64_t>() + n;
+  gather_nrecs_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(d_res, n, counts);
+  ctx->launches++;
+  size_t tmp = 0;
+  CK(ctx, cub::DeviceScan::ExclusiveSum(nullptr, tmp, counts, pd.nrec_scan.as<int64_t>(), (int) n, s));
+  CK(ctx, pd.cub_tmp.ensure(std::max<size_t>(tmp, 16)));
+  CK(ctx, cub::DeviceScan::ExclusiveSum(pd.cub_tmp.p, tmp, counts, pd.nrec_scan.as<int64_t>(), (int) n, s));
+  ctx->launches++;
+  cudaEvent_t ev = nullptr;
+  prof_begin(ctx, &ev);
+  const int grid = (int) std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t) ctx->nsm * 16));
+  compact_records_kernel<<<grid, 256, 0, s>>>(d_res, pd.rec_off.as<int64_t>(), d_slots,
+                                              pd.nrec_scan.as<int64_t>(), n, out, pd.total.as<int64_t>());
+  prof_end(ctx, 28, ev);
+  ctx->launches++;
+  CK(ctx, cudaGetLastError());
   return GDP_OK;
 }
 
@@ -587,22 +792,68 @@ gdp_plan_execute (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *d_pairs, const c
                   gdp_result_t *d_results, gdp_rec_t *d_recs) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  return plan_run(ctx, pl, d_pairs, d_arena, d_results, d_recs);
+  return plan_run(ctx, pl->h, pl->d, d_pairs, d_arena, d_results, d_recs);
 }
 
-/* Uploads pairs/arena, runs, and leaves results on the device. */
+/* ------------------------------------------------------------------ */
+/* Host-buffer path: waves with overlapped planning and copies         */
+/* ------------------------------------------------------------------ */
+
+/* Enqueues wave (first, count) in slot sl: copy-in on the h2d stream, work
+   on the compute stream, results out on the d2h stream.  Records leave once
+   the host knows their count (slot_finish). */
 static int
-stage_and_run (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *pairs, int64_t n,
-               const char *arena, int64_t arena_bytes) {
-  cudaStream_t s = ctx->stream;
-  CK(ctx, ctx->pairs.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_pair_t)));
-  CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
-  CK(ctx, ctx->results.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_result_t)));
-  CK(ctx, ctx->recs.ensure(std::max<int64_t>(pl->total_recs, 1) * sizeof(gdp_rec_t)));
-  CK(ctx, cudaMemcpyAsync(ctx->pairs.p, pairs, n * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s));
-  CK(ctx, cudaMemcpyAsync(ctx->arena.p, arena, arena_bytes, cudaMemcpyHostToDevice, s));
-  return plan_run(ctx, pl, (const gdp_pair_t *) ctx->pairs.p, (const char *) ctx->arena.p,
-                  (gdp_result_t *) ctx->results.p, (gdp_rec_t *) ctx->recs.p);
+slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int64_t count,
+             int64_t arena_bytes, gdp_result_t *results, cudaEvent_t arena_ready) {
+  int rc = plan_build(ctx, pairs + first, count, arena_bytes, sl.h);
+  if (rc != GDP_OK) return rc;
+  sl.first = first;
+  sl.count = count;
+  CK(ctx, sl.pairs.ensure(std::max<int64_t>(count, 1) * sizeof(gdp_pair_t)));
+  CK(ctx, sl.results.ensure(std::max<int64_t>(count, 1) * sizeof(gdp_result_t)));
+  CK(ctx, sl.d.slots.ensure(std::max<int64_t>(sl.h.total_recs, 1) * sizeof(gdp_rec_t)));
+  CK(ctx, sl.recs.ensure(std::max<int64_t>(sl.h.total_recs, 1) * sizeof(gdp_rec_t)));
+  CK(ctx, sl.total.ensure(sizeof(int64_t)));
+  CK(ctx, cudaMemcpyAsync(sl.pairs.p, pairs + first, count * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, ctx->h2d));
+  rc = plan_upload(ctx, sl.h, sl.d, false, ctx->h2d);
+  if (rc != GDP_OK) return rc;
+  CK(ctx, cudaEventRecord(sl.h2d_done, ctx->h2d));
+  CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.h2d_done, 0));
+  if (arena_ready) CK(ctx, cudaStreamWaitEvent(ctx->stream, arena_ready, 0));
+  rc = plan_run(ctx, sl.h, sl.d, sl.pairs.as<gdp_pair_t>(), ctx->arena.as<char>(), sl.results.as<gdp_result_t>(),
+                sl.d.slots.as<gdp_rec_t>());
+  if (rc != GDP_OK) return rc;
+  rc = compact_records(ctx, sl.h, sl.d, sl.results.as<gdp_result_t>(), sl.d.slots.as<gdp_rec_t>(),
+                       sl.recs.as<gdp_rec_t>());
+  if (rc != GDP_OK) return rc;
+  CK(ctx, cudaMemcpyAsync(sl.total.p, sl.d.total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaEventRecord(sl.total_ready, ctx->stream));
+  CK(ctx, cudaEventRecord(sl.comp_done, ctx->stream));
+  CK(ctx, cudaStreamWaitEvent(ctx->d2h, sl.comp_done, 0));
+  CK(ctx, cudaMemcpyAsync(results + first, sl.results.p, count * sizeof(gdp_result_t), cudaMemcpyDeviceToHost,
+                          ctx->d2h));
+  sl.busy = true;
+  return GDP_OK;
+}
+
+/* Waits for the wave's record count and queues its records out at *base. */
+static int
+slot_finish (gdp_ctx *ctx, Slot &sl, gdp_rec_t *recs, int64_t max_recs, int64_t *base, bool *overflow) {
+  if (!sl.busy) return GDP_OK;
+  CK(ctx, cudaEventSynchronize(sl.total_ready));
+  const int64_t total = sl.h.n > 0 ? *sl.total.as<int64_t>() : 0;
+  if (total > 0) {
+    if (recs == nullptr || *base + total > max_recs) {
+      *overflow = true;
+    } else {
+      CK(ctx, cudaMemcpyAsync(recs + *base, sl.recs.p, total * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, ctx->d2h));
+    }
+  }
+  CK(ctx, cudaEventRecord(sl.out_done, ctx->d2h));
+  sl.rec_base = *base;
+  *base += total;
+  sl.busy = false;
+  return GDP_OK;
 }
 
 extern "C" int
@@ -610,42 +861,64 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
                  gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs, int64_t *nrecs_used) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  gdp_plan *pl = nullptr;
-  int rc = plan_build(ctx, pairs, n, false, &pl);
-  if (rc != GDP_OK) return rc;
-  cudaStream_t s = ctx->stream;
-  rc = stage_and_run(ctx, pl, pairs, n, arena, arena_bytes);
-  if (rc == GDP_OK) {
-    cudaError_t e = cudaMemcpyAsync(results, ctx->results.p, n * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) rc = set_err(ctx, "results", e);
-  }
-  if (rc == GDP_OK) {
-    /* compact the records in push order per pair */
-    int64_t used = 0;
-    for (int64_t i = 0; i < n; i++) used += results[i].nrecs;
-    if (recs == nullptr || used > max_recs) {
-      rc = (used == 0) ? GDP_OK : GDP_ERR_RECS;
-    } else if (used > 0) {
-      std::vector<gdp_rec_t> all(pl->total_recs);
-      cudaError_t e = cudaMemcpyAsync(all.data(), ctx->recs.p, pl->total_recs * sizeof(gdp_rec_t),
-                                      cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-      if (e != cudaSuccess) {
-        rc = set_err(ctx, "records", e);
-      } else {
-        int64_t at = 0;
-        for (int64_t i = 0; i < n; i++) {
-          const int nr = results[i].nrecs;
-          if (nr > 0) memcpy(recs + at, all.data() + pl->rec_off[i], nr * sizeof(gdp_rec_t));
-          results[i].rec_offset = at;
-          at += nr;
-        }
-      }
+  if (nrecs_used) *nrecs_used = 0;
+  if (n <= 0) return GDP_OK;
+  CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
+  cudaEvent_t arena_ready;
+  CK(ctx, cudaEventCreateWithFlags(&arena_ready, cudaEventDisableTiming));
+  /* the previous batch may still be reading the arena */
+  for (int s = 0; s < 2; s++) CK(ctx, cudaEventSynchronize(ctx->slot[s].out_done));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  CK(ctx, cudaMemcpyAsync(ctx->arena.p, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->h2d));
+  CK(ctx, cudaEventRecord(arena_ready, ctx->h2d));
+  const int64_t wave = std::max<int64_t>(1, ctx->wave);
+  std::vector<std::pair<int64_t, int64_t>> bases;   /* (first pair, record base) per wave */
+  int64_t base = 0;
+  bool overflow = false;
+  int rc = GDP_OK;
+  int cur = 0;
+  for (int64_t first = 0; first < n && rc == GDP_OK; first += wave) {
+    Slot &sl = ctx->slot[cur];
+    if (sl.busy) {
+      rc = slot_finish(ctx, sl, recs, max_recs, &base, &overflow);
+      bases.push_back({sl.first, sl.rec_base});
+      if (rc != GDP_OK) break;
     }
-    if (nrecs_used) *nrecs_used = used;
+    cudaEventSynchronize(sl.out_done);   /* the slot's buffers are free again */
+    const int64_t count = std::min(wave, n - first);
+    rc = slot_launch(ctx, sl, pairs, first, count, arena_bytes, results, first == 0 ? arena_ready : nullptr);
+    cur ^= 1;
+    /* while this wave runs, queue the previous wave's records out */
+    Slot &prev = ctx->slot[cur];
+    if (rc == GDP_OK && prev.busy) {
+      rc = slot_finish(ctx, prev, recs, max_recs, &base, &overflow);
+      bases.push_back({prev.first, prev.rec_base});
+    }
   }
-  gdp_plan_destroy(pl);
+  for (int s = 0; s < 2 && rc == GDP_OK; s++) {
+    Slot &sl = ctx->slot[cur];
+    if (sl.busy) {
+      rc = slot_finish(ctx, sl, recs, max_recs, &base, &overflow);
+      bases.push_back({sl.first, sl.rec_base});
+    }
+    cur ^= 1;
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->d2h);
+  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  cudaEventDestroy(arena_ready);
+  if (rc == GDP_OK && e != cudaSuccess) rc = set_err(ctx, "batch copies", e);
+  if (rc == GDP_OK && e2 != cudaSuccess) rc = set_err(ctx, "batch kernels", e2);
+  if (rc == GDP_OK) {
+    std::sort(bases.begin(), bases.end());
+    for (size_t w = 0; w < bases.size(); w++) {
+      const int64_t f = bases[w].first, b = bases[w].second;
+      const int64_t end = std::min(n, f + wave);
+      if (b != 0)
+        for (int64_t i = f; i < end; i++) results[i].rec_offset += b;
+    }
+    if (overflow) rc = GDP_ERR_RECS;
+  }
+  if (nrecs_used) *nrecs_used = base;
   return rc;
 }
 
@@ -661,19 +934,30 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
   cudaSetDevice(ctx->device);
   std::vector<gdp_pair_t> pp(pairs, pairs + n);
   for (auto &p : pp) p.flags &= ~GDP_FLAG_TRACEBACK;
-  gdp_plan *pl = nullptr;
-  int rc = plan_build(ctx, pp.data(), n, true, &pl);
-  if (rc != GDP_OK) return rc;
+  gdp_plan pl;
+  int rc = plan_build(ctx, pp.data(), n, arena_bytes, pl.h);
   cudaStream_t s = ctx->stream;
-  rc = stage_and_run(ctx, pl, pp.data(), n, arena, arena_bytes);
-  std::vector<uint32_t> words(std::max<int64_t>(pl->dir_words, 1));
-  std::vector<int16_t> hs(std::max<int64_t>(pl->dir_words, 1) * 8);
+  DevBuf dpairs, dres;
+  for (int k = 0; k < 2; k++) cudaEventSynchronize(ctx->slot[k].out_done);
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl.h, pl.d, true, s);
+  if (rc == GDP_OK) {
+    cudaError_t e = ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16));
+    if (e == cudaSuccess) e = dpairs.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_pair_t));
+    if (e == cudaSuccess) e = dres.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_result_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->arena.p, arena, arena_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dpairs.p, pp.data(), n * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) rc = set_err(ctx, "dump staging", e);
+  }
+  if (rc == GDP_OK)
+    rc = plan_run(ctx, pl.h, pl.d, dpairs.as<gdp_pair_t>(), ctx->arena.as<char>(), dres.as<gdp_result_t>(), nullptr);
+  std::vector<uint32_t> words(std::max<int64_t>(pl.h.dir_words, 1));
+  std::vector<int16_t> hs(std::max<int64_t>(pl.h.dir_words, 1) * 8);
   std::vector<gdp_meta_t> meta(std::max<int64_t>(n, 1));
   if (rc == GDP_OK) {
-    cudaError_t e = cudaMemcpyAsync(results, ctx->results.p, n * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(words.data(), pl->d_dirs, pl->dir_words * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), pl->d_hdump, pl->dir_words * 16, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(meta.data(), pl->d_meta, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaMemcpyAsync(results, dres.p, n * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(words.data(), pl.d.dirs.p, pl.h.dir_words * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), pl.d.hdump.p, pl.h.dir_words * 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(meta.data(), pl.d.meta.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = set_err(ctx, "dump copy", e);
   }
@@ -701,11 +985,11 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
           gdp_block_sweep(&g, b * W, &y0, &y1);
           const int64_t at = dense_offsets[i] + (int64_t) c * R + r;
           if (y < y0 || y > y1) continue;
-          const int64_t widx = base + boff[b] + (int64_t) (y - y0) * (W / 8) + (lane >> 3);
-          const uint32_t w = words[widx];
+          const int64_t col = base + boff[b] + (int64_t) (y - y0) * (W / 8);
+          const uint32_t w = words[col + (lane >> 3)];
           const int sh = lane & 7;
           const int nh = (w >> sh) & 1, nv = (w >> (8 + sh)) & 1, ee = (w >> (16 + sh)) & 1, ff = (w >> (24 + sh)) & 1;
-          if (H) H[at] = hs[(base + boff[b] + (int64_t) (y - y0) * (W / 8)) * 8 + lane];
+          if (H) H[at] = hs[col * 8 + lane];
           if (dN) dN[at] = (int8_t) (nv ? -2 : nh ? -1 : 0);
           if (dE) dE[at] = (int8_t) (ee ? -1 : 0);
           if (dF) dF[at] = (int8_t) (ff ? -2 : 0);
@@ -713,6 +997,9 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
       }
     }
   }
-  gdp_plan_destroy(pl);
+  pl.d.release();
+  pl.h.release();
+  dpairs.release();
+  dres.release();
   return rc;
 }

@@ -190,6 +190,102 @@ struct TbState {
   }
 };
 
+/* One traceback walk over the direction words behind `dc`. */
+__device__ void
+tb_walk (const gdp_pair_t &p, DirCursor &dc, TbState &T) {
+  int r = p.tb_r, c = p.tb_c;
+  const bool lower = (p.variant == GDP_LOWER);
+  /* (x, y) of cell (c, r): lanes are rows except in the lower fill */
+#define CELL(cc, rr) (lower ? dc.cell((cc), (rr)) : dc.cell((rr), (cc)))
+  /* a full-band cell above the band derives from stale scratch in the reference */
+#define ABOVE(cc, rr) (p.variant == GDP_FULL && (rr) < (cc) - p.uband)
+  if (p.variant == GDP_FULL) {
+    while (r > 0 && c > 0 && !T.err) {
+      const int code = CELL(c, r);
+      if (code < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
+      const int dir = (code & 2) ? -2 : (code & 1) ? -1 : 0;
+      if (dir == -1) {
+        int dist = 1;
+        while (c > 0) {
+          const int e = CELL(c, r);
+          if (e < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
+          c--;
+          if (!(e & 4)) break;
+          dist++;
+        }
+        if (T.err) break;
+        T.genomeskip(r, c + dist, dist);
+      } else if (dir == -2) {
+        int dist = 1;
+        while (r > 0) {
+          const int f = CELL(c, r);
+          if (f < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
+          r--;
+          if (!(f & 8)) break;
+          dist++;
+        }
+        if (T.err) break;
+        T.queryskip(r + dist, c, dist);
+      } else {
+        T.diagpair(r, c);
+        r--; c--;
+      }
+    }
+    if (!T.err) {
+      if (r == 0 && c == 0) {
+      } else if (c == 0) {
+        T.queryskip(r, 1, r);
+      } else {
+        T.genomeskip(1, c, c);
+      }
+    }
+  } else if (p.variant == GDP_UPPER) {
+    while (r > 0 && c > 0 && !T.err) {
+      const int code = CELL(c, r);
+      if (code < 0) { T.err = GDP_ERR_BAND; break; }
+      if (code & 3) {
+        int dist = 1;
+        for (;;) {
+          const int e = CELL(c, r);
+          if (e < 0) { T.err = GDP_ERR_BAND; break; }
+          c--;
+          if (!(e & 4)) break;
+          dist++;
+        }
+        if (T.err) break;
+        T.genomeskip(r, c + dist, dist);
+      } else {
+        T.diagpair(r, c);
+        r--; c--;
+      }
+    }
+    if (!T.err && c != 0) T.genomeskip(1, c, c);
+  } else {
+    while (r > 0 && c > 0 && !T.err) {
+      const int code = CELL(c, r);
+      if (code < 0) { T.err = GDP_ERR_BAND; break; }
+      if (code & 3) {
+        int dist = 1;
+        for (;;) {
+          const int e = CELL(c, r);
+          if (e < 0) { T.err = GDP_ERR_BAND; break; }
+          r--;
+          if (!(e & 4)) break;
+          dist++;
+        }
+        if (T.err) break;
+        T.queryskip(r + dist, c, dist);
+      } else {
+        T.diagpair(r, c);
+        r--; c--;
+      }
+    }
+    if (!T.err && r != 0) T.queryskip(r, 1, r);
+  }
+#undef CELL
+#undef ABOVE
+}
+
 __global__ void __launch_bounds__(128)
 traceback_kernel (TbParams P) {
   const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
@@ -200,9 +296,7 @@ traceback_kernel (TbParams P) {
     gdp_result_t *res = P.res + pi;
     if (res->status != GDP_OK) continue;
     const gdp_meta_t m = P.meta[pi];
-    const int W = (res->precision == 8) ? 32 : 16;
-    DirCursor dc;
-    dc.init(p, W, P.dirs + (W == 16 ? m.dir16 : m.dir8));
+    int W = (res->precision == 8) ? 32 : 16;
     TbState T;
     T.p = &p;
     T.revp = (p.flags & GDP_FLAG_REVP) != 0;
@@ -214,101 +308,25 @@ traceback_kernel (TbParams P) {
     }
     T.out = P.recs + P.rec_off[pi];
     T.cap = (int64_t) p.rlength + p.glength + 2;
-    T.n = 0; T.score = T.nmatch = T.nmismatch = T.nopen = T.nindel = 0; T.err = 0;
     T.genome = P.genome; T.genomealt = P.genomealt ? P.genomealt : P.genome;
     T.genome_len = P.genome_len;
     T.tab = P.tab;
-    int r = p.tb_r, c = p.tb_c;
-    const bool lower = (p.variant == GDP_LOWER);
-    /* (x, y) of cell (c, r): lanes are rows except in the lower fill */
-#define CELL(cc, rr) (lower ? dc.cell((cc), (rr)) : dc.cell((rr), (cc)))
-    /* a full-band cell above the band derives from stale scratch in the reference */
-#define ABOVE(cc, rr) (p.variant == GDP_FULL && (rr) < (cc) - p.uband)
-    if (p.variant == GDP_FULL) {
-      while (r > 0 && c > 0 && !T.err) {
-        const int code = CELL(c, r);
-        if (code < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
-        const int dir = (code & 2) ? -2 : (code & 1) ? -1 : 0;
-        if (dir == -1) {
-          int dist = 1;
-          while (c > 0) {
-            const int e = CELL(c, r);
-            if (e < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
-            c--;
-            if (!(e & 4)) break;
-            dist++;
-          }
-          if (T.err) break;
-          T.genomeskip(r, c + dist, dist);
-        } else if (dir == -2) {
-          int dist = 1;
-          while (r > 0) {
-            const int f = CELL(c, r);
-            if (f < 0 || ABOVE(c, r)) { T.err = GDP_ERR_BAND; break; }
-            r--;
-            if (!(f & 8)) break;
-            dist++;
-          }
-          if (T.err) break;
-          T.queryskip(r + dist, c, dist);
-        } else {
-          T.diagpair(r, c);
-          r--; c--;
-        }
+    for (int attempt = 0; attempt < 2; attempt++) {
+      DirCursor dc;
+      dc.init(p, W, P.dirs + (W == 16 ? m.dir16 : m.dir8));
+      T.n = 0; T.score = T.nmatch = T.nmismatch = T.nopen = T.nindel = 0; T.err = 0;
+      tb_walk(p, dc, T);
+      /* An 8-bit walk that leaves the cells its fill wrote has no defined
+         result; a rerun pair then takes its 16-bit fill and traceback. */
+      if (T.err == GDP_ERR_BAND && W == 32 && m.dir16 >= 0) {
+        W = 16;
+        res->precision = 16;
+        res->rerun = 1;
+        res->score = m.final16;
+        continue;
       }
-      if (!T.err) {
-        if (r == 0 && c == 0) {
-        } else if (c == 0) {
-          T.queryskip(r, 1, r);
-        } else {
-          T.genomeskip(1, c, c);
-        }
-      }
-    } else if (p.variant == GDP_UPPER) {
-      while (r > 0 && c > 0 && !T.err) {
-        const int code = CELL(c, r);
-        if (code < 0) { T.err = GDP_ERR_BAND; break; }
-        if (code & 3) {
-          int dist = 1;
-          for (;;) {
-            const int e = CELL(c, r);
-            if (e < 0) { T.err = GDP_ERR_BAND; break; }
-            c--;
-            if (!(e & 4)) break;
-            dist++;
-          }
-          if (T.err) break;
-          T.genomeskip(r, c + dist, dist);
-        } else {
-          T.diagpair(r, c);
-          r--; c--;
-        }
-      }
-      if (!T.err && c != 0) T.genomeskip(1, c, c);
-    } else {
-      while (r > 0 && c > 0 && !T.err) {
-        const int code = CELL(c, r);
-        if (code < 0) { T.err = GDP_ERR_BAND; break; }
-        if (code & 3) {
-          int dist = 1;
-          for (;;) {
-            const int e = CELL(c, r);
-            if (e < 0) { T.err = GDP_ERR_BAND; break; }
-            r--;
-            if (!(e & 4)) break;
-            dist++;
-          }
-          if (T.err) break;
-          T.queryskip(r + dist, c, dist);
-        } else {
-          T.diagpair(r, c);
-          r--; c--;
-        }
-      }
-      if (!T.err && r != 0) T.queryskip(r, 1, r);
+      break;
     }
-#undef CELL
-#undef ABOVE
     res->tb_score = T.score;
     res->nmatches = T.nmatch;
     res->nmismatches = T.nmismatch;

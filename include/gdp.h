@@ -204,8 +204,8 @@ void *gdp_ctx_stream(gdp_ctx *ctx);
 /*
  * Per-kernel timing.  While enabled, every kernel launch of the context is
  * bracketed by CUDA events on its stream.  gdp_profile_read(ctx, id, ...)
- * returns, for kernel id 0..26 (0..23 fill kinds, 24 traceback, 25 result
- * initialisation, 26 integer-rate probe), its name, total device
+ * returns, for kernel id 0..27 (0..23 fill kinds, 24 traceback, 25 result
+ * initialisation, 26 integer-rate probe, 27 rerun-list compaction), its name, total device
  * milliseconds and launch count since the last reset.
  */
 int gdp_profile_enable(gdp_ctx *ctx, int on);

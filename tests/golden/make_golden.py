@@ -81,6 +81,9 @@ def main():
             m = oracle.domain_mask(int(q["variant"][0]), int(q["rlength"][0]), int(q["glength"][0]),
                                    int(q["lband"][0]), int(q["uband"][0])).ravel()
             sat = bool((o8["H"][m] >= 127).any()) or o8["score"] <= -98
+            if not sat and (q["flags"][0] & gdp.FLAG_TRACEBACK):
+                rest.align(q.copy(), 0, arena, want_matrix=False)
+                sat = bool(rest.lib.orc_last_tb_stale())   # undefined 8-bit traceback: rerun
             q["precision"] = 16 if sat else 8
         out = ref.align(q, 0, arena)
         rest.align(q, 0, arena, want_matrix=False)

@@ -15,10 +15,11 @@ def _as_precision(pairs, i, prec):
     return p
 
 
-def expected_precision(oracle, pairs, i, arena):
+def expected_precision(oracle, pairs, i, arena, restatement=None):
     """The rerun contract for an 8-bit pair flagged RERUN16: keep the 8-bit
     outputs unless the 8-bit fill reaches 127 inside the band or ends at or
-    below -98; then keep the 16-bit outputs."""
+    below -98, or (when it traces back) its 8-bit traceback would read cells
+    the 8-bit fill never wrote; then keep the 16-bit outputs."""
     p = pairs[i]
     if p["precision"] == 16:
         return 16
@@ -29,7 +30,14 @@ def expected_precision(oracle, pairs, i, arena):
     m = orc.domain_mask(int(p["variant"]), int(p["rlength"]), int(p["glength"]),
                         int(p["lband"]), int(p["uband"])).ravel()
     sat = (o["H"][m] >= 127).any() if m.any() else False
-    return 16 if (sat or o["score"] <= -98) else 8
+    if sat or o["score"] <= -98:
+        return 16
+    if restatement is not None and (p["flags"] & gdp.FLAG_TRACEBACK):
+        restatement.lib.orc_last_tb_stale.restype = ctypes.c_int
+        restatement.align(q, 0, arena, want_matrix=False)
+        if restatement.lib.orc_last_tb_stale():
+            return 16
+    return 8
 
 
 def check_fill(ctx, oracle, pairs, arena, max_report=5):
@@ -82,6 +90,10 @@ def check_traceback(ctx, oracle, restatement, pairs, arena, max_report=5):
     for i in range(pairs.size):
         p = pairs[i]
         prec = int(res["precision"][i])
+        want = expected_precision(oracle, pairs, i, arena, restatement)
+        if prec != want:
+            fails.append(f"pair {i}: kept precision {prec}, contract says {want}")
+            continue
         q = _as_precision(pairs, i, prec)
         o = oracle.align(q, 0, arena, want_matrix=False)
         restatement.align(q, 0, arena, want_matrix=False)

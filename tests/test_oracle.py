@@ -38,7 +38,13 @@ def _golden_precision(pairs, i, o8, restatement, arena):
         return int(p["precision"])
     m = orc.domain_mask(int(p["variant"]), int(p["rlength"]), int(p["glength"]),
                         int(p["lband"]), int(p["uband"])).ravel()
-    return 16 if ((o8["H"][m] >= 127).any() or o8["score"] <= -98) else 8
+    if (o8["H"][m] >= 127).any() or o8["score"] <= -98:
+        return 16
+    q = pairs[i:i + 1].copy()
+    q["precision"] = 8
+    restatement.lib.orc_last_tb_stale.restype = ctypes.c_int
+    restatement.align(q, 0, arena, want_matrix=False)
+    return 16 if restatement.lib.orc_last_tb_stale() else 8
 
 
 def test_restatement_matches_golden(restatement):
