@@ -287,7 +287,7 @@ fill_thread_kernel (FillParams P) {
 
 /* Keeps the rerun pairs whose 16-bit in-band maximum stays below 127: only
    those need the 8-bit pass (the others provably overflow in 8 bits). */
-__global__ void
+static __global__ void
 compact_rerun_kernel (const int32_t *list, const int32_t *count, const gdp_meta_t *meta,
                       int32_t *out, int32_t *out_count) {
   const int n = *count;

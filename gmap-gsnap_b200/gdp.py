@@ -87,6 +87,7 @@ def load(path=LIB_PATH):
     lib.gdp_profile_reset.argtypes = [vp]
     lib.gdp_measure_int_peak.argtypes = [vp]
     lib.gdp_measure_int_peak.restype = ctypes.c_double
+    lib.gdp_fill16_noalloc.argtypes = [i32, i32, vp, i64, vp, vp, i64, vp, vp]
     lib.gdp_fill_dump.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, vp, vp, vp]
     lib.gdp_launch_count.argtypes = [vp]
     lib.gdp_launch_count.restype = i64

@@ -216,6 +216,34 @@ int gdp_profile_reset(gdp_ctx *ctx);
    with an ALU/FMA-pipe probe kernel: the denominator of the fill roofline. */
 double gdp_measure_int_peak(gdp_ctx *ctx);
 
+/*
+ * No counterpart in the reference: a fill for callers that cannot allocate
+ * device memory (code running inside another framework's memory pool, a
+ * host that forbids allocation on its hot path, or a caller that owns all
+ * of its buffers).  It runs the 16-bit full-band fill (Dynprog_simd_16
+ * semantics) for device-resident pairs and arena, with no context, and
+ * allocates nothing: its working memory is a fixed file-scope device array
+ * of about 36 MB, held on each GPU that loads the library until exit.
+ *
+ *   npairs <= 65,536 per call, every pair full band and precision 16,
+ *   glength <= 1,023; otherwise the call returns GDP_ERR_LEN (too many
+ *   pairs) or the pair gets GDP_ERR_PARAM / GDP_ERR_LEN.
+ *
+ * Outputs: d_results[i] (status, score, precision) and pair i's direction
+ * words (the library's block-column layout), written to d_dirs starting at
+ * word d_results[i].rec_offset.  A pair whose words do not fit into
+ * dir_words_cap gets GDP_ERR_BUDGET.  Work is enqueued on `stream` (a
+ * cudaStream_t; NULL for the legacy stream).
+ *
+ * The first call on a device sets up that device (it takes the array
+ * addresses and uploads the tables for `mode`), so it should come before
+ * any stream capture; later calls must use the same mode.  All calls share
+ * the array: calls that overlap on the GPU race and must be ordered by the
+ * caller.
+ */
+int gdp_fill16_noalloc(int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
+                       uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results, void *stream);
+
 /* Kernel launches issued by the context since creation (one per kernel). */
 int64_t gdp_launch_count(gdp_ctx *ctx);
 
