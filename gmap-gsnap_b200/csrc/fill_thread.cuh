@@ -64,9 +64,35 @@ struct FillParams {
   const gdp_tables_t *tab;
 };
 
-/* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records the largest
-   in-band score), 2 = 8-bit pass of a rerun pair (skipped when the 16-bit
-   pass proved an overflow; stops at the first in-band 127). */
+/* Lanes lo..hi (0 <= lo <= hi <= 31) as a bit mask. */
+__device__ __forceinline__ uint32_t
+lane_range (int lo, int hi) {
+  const uint32_t upto = (hi >= 31) ? 0xffffffffu : ((1u << (hi + 1)) - 1u);
+  return upto & ~((1u << lo) - 1u);
+}
+
+/* max(a, b) and the tie rule of the reference: jump late takes a on a >= b,
+   jump early only on a > b. */
+template <bool LATE>
+__device__ __forceinline__ int
+tie_max (int a, int b, bool &a_wins) {
+  if (LATE) return __vibmax_s32(a, b, &a_wins);
+  bool q;
+  const int m = __vibmax_s32(b, a, &q);
+  a_wins = !q;
+  return m;
+}
+
+/* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records whether an
+   in-band score reaches 127), 2 = 8-bit pass of a rerun pair (skipped when
+   the 16-bit pass proved an overflow; stops at the first in-band 127).
+
+   Per block column the band geometry is reduced to a few lane masks that
+   are uniform over the column: the lanes of the F loop, the top cell
+   (src/dynprog_simd.c:6962-6974), the bottom cell (:6926-6945), the lanes
+   whose E is clamped (upper/lower E_mask, :7921, :7943) and the diagonal
+   cell (:7966-7969).  The lane loop is fully unrolled, so each mask test is
+   a test of a constant bit. */
 template <int W, int VARIANT, bool LATE, int MODE>
 __global__ void __launch_bounds__(128)
 fill_thread_kernel (FillParams P) {
@@ -99,41 +125,49 @@ fill_thread_kernel (FillParams P) {
     const char *sseq = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq);
     const char *salt = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq_alt);
     const int slen = (VARIANT == GDP_LOWER) ? p.rlength : p.glength;
+    /* domain band of the lane index relative to y: lanes x with y - dhi <= x <= y + dlo */
+    const int dlo = (VARIANT == GDP_FULL) ? lband : 0;
+    const int dhi = (VARIANT == GDP_FULL) ? uband : (VARIANT == GDP_UPPER ? uband : lband);
     uint32_t *dir = P.dirs + ((W == 16) ? mp->dir16 : mp->dir8);
     int2 *sc = P.scratch + slot;
     const int64_t scs = P.nslots;
-    int final_score = LO, maxh = LO;
-    bool aborted = false;
+    int final_score = LO;
+    bool reached = false;     /* an in-band score reached 127 */
 
     for (int xlo = 0; xlo <= g.X; xlo += W) {
       const int xhi = min(xlo + W - 1, g.X);
+      const int last = xhi - xlo;
       int y0, y1;
       gdp_block_sweep(&g, xlo, &y0, &y1);
       if (y1 < y0) continue;
 
-      /* lane profiles: 5 signed bytes per lane */
-      uint32_t plo[W], phi[W];
+      /* lane profiles: bytes 0..3 of plo = scores against classes A,C,G,T;
+         the class-N score of lane i is byte (i & 3) of phi4[i >> 2] */
+      uint32_t plo[W], phi4[W / 4];
+#pragma unroll
+      for (int j = 0; j < W / 4; j++) phi4[j] = 0;
 #pragma unroll
       for (int i = 0; i < W; i++) {
         const int x = xlo + i;
+        uint32_t lo, hi;
         if (VARIANT != GDP_LOWER) {
           const int q = (x == 0) ? 'N' : (x <= llen ? seqch(lseq, llen, x, revp) : 'N');
-          plo[i] = __ldg(&P.tab->profq_lo[mt][q]);
-          phi[i] = __ldg(&P.tab->profq_hi[mt][q]);
+          lo = __ldg(&P.tab->profq_lo[mt][q]);
+          hi = __ldg(&P.tab->profq_hi[mt][q]);
+        } else if (x == 0) {
+          /* 16-bit: column 0 scores against 'N' (:8689); 8-bit: against code 4 (:5459) */
+          const int c0 = (W == 32) ? 4 : 'N';
+          lo = __ldg(&P.tab->profg_lo[mt][c0]);
+          hi = __ldg(&P.tab->profg_hi[mt][c0]);
+        } else if (x <= llen) {
+          const int a = seqch(lseq, llen, x, revp), b = seqch(lalt, llen, x, revp);
+          lo = bytemax(__ldg(&P.tab->profg_lo[mt][a]), __ldg(&P.tab->profg_lo[mt][b]));
+          hi = bytemax(__ldg(&P.tab->profg_hi[mt][a]), __ldg(&P.tab->profg_hi[mt][b]));
         } else {
-          if (x == 0) {
-            /* 16-bit: column 0 scores against 'N' (:8689); 8-bit: against code 4 (:5459) */
-            const int c0 = (W == 32) ? 4 : 'N';
-            plo[i] = __ldg(&P.tab->profg_lo[mt][c0]);
-            phi[i] = __ldg(&P.tab->profg_hi[mt][c0]);
-          } else if (x <= llen) {
-            const int a = seqch(lseq, llen, x, revp), b = seqch(lalt, llen, x, revp);
-            plo[i] = bytemax(__ldg(&P.tab->profg_lo[mt][a]), __ldg(&P.tab->profg_lo[mt][b]));
-            phi[i] = bytemax(__ldg(&P.tab->profg_hi[mt][a]), __ldg(&P.tab->profg_hi[mt][b]));
-          } else {
-            plo[i] = 0; phi[i] = 0;
-          }
+          lo = 0; hi = 0;
         }
+        plo[i] = lo;
+        phi4[i >> 2] |= (hi & 0xffu) << (8 * (i & 3));
       }
       int H[W], E[W];
 #pragma unroll
@@ -143,18 +177,24 @@ fill_thread_kernel (FillParams P) {
       uint32_t *dcol = dir;
 
       for (int y = y0; y <= y1; y++) {
-        /* swept-column classes */
-        uint32_t selA, selB;
-        bool col0 = false;
+        /* swept-column classes -> PRMT selectors; class N (4) reads the
+           packed byte (i & 3) of phi4, i.e. byte 4 + (i & 3) of {phi4, plo} */
+        int ka, kb;
         if (VARIANT == GDP_LOWER) {
-          const int k = (y == 0) ? 4 : s_nt2int[seqch(sseq, slen, y, revp)];
-          selA = selB = GDP_SEL(k);
+          ka = kb = (y == 0) ? 4 : s_nt2int[seqch(sseq, slen, y, revp)];
         } else if (y == 0) {
-          selA = selB = GDP_SEL(4);
-          col0 = (VARIANT == GDP_FULL);
+          ka = kb = 4;
         } else {
-          selA = GDP_SEL(s_nt2int[seqch(sseq, slen, y, revp)]);
-          selB = GDP_SEL(s_nt2int[seqch(salt, slen, y, revp)]);
+          ka = s_nt2int[seqch(sseq, slen, y, revp)];
+          kb = s_nt2int[seqch(salt, slen, y, revp)];
+        }
+        const bool col0 = (VARIANT == GDP_FULL) && (y == 0);
+        uint32_t sA[4], sB[4];
+        {
+          const uint32_t dA = (ka == 4) ? 0x1111u : 0u, dB = (kb == 4) ? 0x1111u : 0u;
+          sA[0] = GDP_SEL(ka); sB[0] = GDP_SEL(kb);
+#pragma unroll
+          for (int k = 1; k < 4; k++) { sA[k] = sA[k - 1] + dA; sB[k] = sB[k - 1] + dB; }
         }
         int2 above = make_int2(LO, GDP_NEGINT);
         if (xlo > 0) above = sc[(int64_t) y * scs];
@@ -163,39 +203,56 @@ fill_thread_kernel (FillParams P) {
         else diag = (xlo == 0) ? LO : bot_prev;
         bot_prev = above.x;
 
-        uint32_t bH = 0, bV = 0, bE = 0, bF = 0;
+        /* lane masks of this column */
+        const int rel = y - xlo;                       /* lane index of x == y */
+        uint32_t fmask = 0, topmask = 0, botmask = 0, emask = 0, dmask = 0;
+        if (VARIANT == GDP_FULL) {
+          const int t = rel - uband, bt = rel + lband;  /* top and bottom lanes */
+          const int flo = max(0, t + 1), fhi = min(bt, last);
+          if (fhi >= flo) fmask = lane_range(flo, fhi);
+          if (t >= 0 && t <= last) topmask = 1u << t;
+          if (y > 0 && bt >= 0 && bt <= last) botmask = 1u << bt;
+        } else {
+          if (rel <= W - 1) emask = lane_range(max(rel, 0), W - 1);
+          if (rel >= 0 && rel <= last) dmask = 1u << rel;
+        }
+        uint32_t w[WORDS];
+#pragma unroll
+        for (int j = 0; j < WORDS; j++) w[j] = 0;
+
+        /* vector step (E, then H from the diagonal), :6862-6913 */
 #pragma unroll
         for (int i = 0; i < W; i++) {
-          const int x = xlo + i;
+          const uint32_t bit = 1u << i;
           const int Hold = H[i];
           int Eold = E[i];
-          const bool masked = (VARIANT != GDP_FULL) && (x >= y);
-          if (masked) Eold = LO;
-          const int T1 = max(Hold + open, LO);
-          bool pE = LATE ? (Eold >= T1) : (Eold > T1);
-          int Ee = max(max(Eold, T1) + ext, LO);
-          if (masked) Ee = LO;
+          if (VARIANT != GDP_FULL && (emask & bit)) Eold = LO;
+          const int T1 = __viaddmax_s32(Hold, open, LO);
+          bool pE;
+          const int m = tie_max<LATE>(Eold, T1, pE);
+          int Ee = __viaddmax_s32(m, ext, LO);
+          if (VARIANT != GDP_FULL && (emask & bit)) Ee = LO;
           int ps;
           if (VARIANT == GDP_FULL && col0) {
-            ps = (x == 0) ? 0 : LO;
+            ps = (xlo + i == 0) ? 0 : LO;     /* pairscores_col0 (:6668-6678) */
           } else if (VARIANT == GDP_LOWER) {
-            ps = prof_byte(plo[i], phi[i], selA);
+            ps = prof_byte(plo[i], phi4[i >> 2], sA[i & 3]);
           } else {
-            ps = max(prof_byte(plo[i], phi[i], selA), prof_byte(plo[i], phi[i], selB));
+            ps = max(prof_byte(plo[i], phi4[i >> 2], sA[i & 3]), prof_byte(plo[i], phi4[i >> 2], sB[i & 3]));
           }
-          const int Hv = min(max(diag + ps, LO), HI);
+          const int Hv = min(__viaddmax_s32(diag, ps, LO), HI);
           diag = Hold;
-          bool pN = LATE ? (Ee >= Hv) : (Ee > Hv);
-          int Hn = max(Hv, Ee);
+          bool pN;
+          int Hn = tie_max<LATE>(Ee, Hv, pN);
           if (VARIANT == GDP_FULL) {
-            if (x == y + lband && y > 0 && x <= xhi) { Hn = Hv; pE = false; pN = false; }
+            if (botmask & bit) { Hn = Hv; pE = false; pN = false; }
           } else {
-            if (x == y && x <= xhi) { pE = false; pN = false; }   /* diagonal fix (:7966-7969) */
+            if (dmask & bit) { pE = false; pN = false; }
           }
           H[i] = Hn;
           E[i] = Ee;
-          bE |= (uint32_t) pE << i;
-          bH |= (uint32_t) pN << i;
+          if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
+          if (pN) w[i >> 3] |= 1u << (i & 7);
         }
         if (VARIANT == GDP_FULL) {
           /* F loop over the in-band lanes (:6916-7000) */
@@ -204,36 +261,33 @@ fill_thread_kernel (FillParams P) {
           else { Fp = above.y; Hp = above.x; }
 #pragma unroll
           for (int i = 0; i < W; i++) {
-            const int d = xlo + i - y;
-            if (d == -uband) {
+            const uint32_t bit = 1u << i;
+            if (topmask & bit) {
               Fp = GDP_NEGINT + oe;
               Hp = H[i];
-            } else if (d > -uband && d <= lband && xlo + i <= xhi) {
-              const int s = Hp + open;
-              const bool pF = LATE ? (Fp >= s) : (Fp > s);
-              const int F = (pF ? Fp : s) + ext;
-              const bool pV = LATE ? (F >= H[i]) : (F > H[i]);
-              if (pV) H[i] = F;
-              Hp = H[i];
+            } else if (fmask & bit) {
+              bool pF, pV;
+              const int F = tie_max<LATE>(Fp, Hp + open, pF) + ext;
+              const int Hn = tie_max<LATE>(F, H[i], pV);
+              H[i] = Hn;
+              Hp = Hn;
               Fp = F;
-              bF |= (uint32_t) pF << i;
-              bV |= (uint32_t) pV << i;
+              if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
+              if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
             }
           }
           sc[(int64_t) y * scs] = make_int2(H[W - 1], Fp);
         } else {
           sc[(int64_t) y * scs] = make_int2(H[W - 1], 0);
         }
-        if (MODE != 0) {
+        if (MODE != 0 && !reached && y >= 1) {
+          /* in-band lanes: y - dhi <= x <= y + dlo, x >= 1 */
+          const int dl = max(rel - dhi, (xlo == 0) ? 1 : 0), dh = min(rel + dlo, last);
+          if (dh >= dl) {
+            const uint32_t dom = lane_range(max(dl, 0), dh);
 #pragma unroll
-          for (int i = 0; i < W; i++) {
-            const int x = xlo + i;
-            bool dom;
-            if (VARIANT == GDP_FULL) dom = (x - y >= -uband) && (x - y <= lband);
-            else if (VARIANT == GDP_UPPER) dom = (x <= y) && (x >= y - uband);
-            else dom = (x >= y - lband) && (x <= y);
-            dom = dom && x >= 1 && y >= 1 && x <= g.X;
-            if (dom) maxh = max(maxh, H[i]);
+            for (int i = 0; i < W; i++)
+              if ((dom & (1u << i)) && H[i] >= 127) reached = true;
           }
         }
         if (y == g.Y) {
@@ -245,17 +299,16 @@ fill_thread_kernel (FillParams P) {
 #pragma unroll
           for (int i = 0; i < W; i++) hd[i] = (int16_t) H[i];
         }
-        /* direction words */
-#pragma unroll
-        for (int j = 0; j < WORDS; j++) {
-          const uint32_t w = ((bH >> (8 * j)) & 0xFFu) | (((bV >> (8 * j)) & 0xFFu) << 8) |
-                             (((bE >> (8 * j)) & 0xFFu) << 16) | (((bF >> (8 * j)) & 0xFFu) << 24);
-          dcol[j] = w;
+        if (WORDS == 2) {
+          *reinterpret_cast<uint2 *>(dcol) = make_uint2(w[0], w[1]);
+        } else {
+          *reinterpret_cast<uint4 *>(dcol) = make_uint4(w[0], w[1], w[WORDS > 2 ? 2 : 0], w[WORDS > 3 ? 3 : 0]);
         }
         dcol += WORDS;
+        if (MODE == 2 && reached) break;
       }
       dir = dcol;
-      if (MODE == 2 && maxh >= HI) { aborted = true; break; }
+      if (MODE == 2 && reached) break;
     }
 
     /* the final cell must have been swept */
@@ -263,11 +316,11 @@ fill_thread_kernel (FillParams P) {
     gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
     const bool swept = (g.Y >= y0l && g.Y <= y1l);
     if (MODE == 1) {
-      mp->maxh16 = maxh;
+      mp->maxh16 = reached ? 127 : -32768;   /* >= 127 iff an in-band 16-bit score reached 127 */
       mp->final16 = final_score;
     }
     if (MODE == 2) {
-      const bool overflow = aborted || maxh >= HI || final_score <= -128 + 30;
+      const bool overflow = reached || final_score <= -128 + 30;
       mp->status8 = overflow ? 1 : 0;
       mp->final8 = final_score;
       if (!overflow) {

@@ -110,7 +110,7 @@ gdp_pair_words (const gdp_pair_t *p, int W) {
 typedef struct gdp_meta {
   int64_t dir16;      /* word offset of the 16-bit layout (-1: none) */
   int64_t dir8;       /* word offset of the 8-bit layout (-1: none) */
-  int32_t maxh16;     /* largest in-band 16-bit score (rerun pairs) */
+  int32_t maxh16;     /* rerun pairs: >= 127 iff an in-band 16-bit score reached 127 */
   int32_t status8;    /* 8-bit pass: 0 = kept, 1 = overflowed (use 16-bit) */
   int32_t final8;     /* 8-bit final score */
   int32_t final16;    /* 16-bit final score (rerun pairs) */

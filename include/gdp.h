@@ -230,8 +230,8 @@ double gdp_measure_int_peak(gdp_ctx *ctx);
  *   pairs) or the pair gets GDP_ERR_PARAM / GDP_ERR_LEN.
  *
  * Outputs: d_results[i] (status, score, precision) and pair i's direction
- * words (the library's block-column layout), written to d_dirs starting at
- * word d_results[i].rec_offset.  A pair whose words do not fit into
+ * words (the library's block-column layout), written to d_dirs (8-byte
+ * aligned) starting at word d_results[i].rec_offset.  A pair whose words do not fit into
  * dir_words_cap gets GDP_ERR_BUDGET.  Work is enqueued on `stream` (a
  * cudaStream_t; NULL for the legacy stream).
  *
