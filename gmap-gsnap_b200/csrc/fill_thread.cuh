@@ -93,8 +93,12 @@ tie_max (int a, int b, bool &a_wins) {
    whose E is clamped (upper/lower E_mask, :7921, :7943) and the diagonal
    cell (:7966-7969).  The lane loop is fully unrolled, so each mask test is
    a test of a constant bit. */
+#ifndef GDP_FILL_MINB
+#define GDP_FILL_MINB 1
+#endif
+
 template <int W, int VARIANT, bool LATE, int MODE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, (W == 16) ? GDP_FILL_MINB : 1)
 fill_thread_kernel (FillParams P) {
   constexpr int LO = (W == 32) ? -128 : -32768;
   constexpr int HI = (W == 32) ? 127 : 32767;

@@ -80,7 +80,7 @@ struct HostBuf {   /* pinned host memory */
 };
 
 constexpr int NKINDS = 24;   /* (W32, variant, late, pass) */
-constexpr int NBUCKETS = 64; /* work buckets for ordering inside a bin */
+constexpr int NBUCKETS = 64 * 32; /* (block count, sweep width) buckets inside a bin */
 
 inline int kind_id (int w32, int variant, int late, int pass) {
   return (((w32 * 3 + variant) * 2 + late) * 2) + pass;
@@ -453,11 +453,25 @@ validate (const gdp_pair_t &p, int64_t arena_bytes) {
   return GDP_OK;
 }
 
+/* Quasi-logarithmic class of v: exact below 16, then 4 classes per octave. */
 static inline int
-bucket_of (int64_t work) {
-  int b = 0;
-  while (work > 1 && b < NBUCKETS - 1) { work >>= 1; b++; }
-  return b;
+qlog (int64_t v) {
+  if (v < 16) return (int) (v < 0 ? 0 : v);
+  const int lg = 63 - __builtin_clzll((unsigned long long) v);
+  return 16 + (lg - 4) * 4 + (int) ((v >> (lg - 2)) & 3);
+}
+
+/* Work bucket of a pair at block height W: pairs of one bucket have the
+   same number of blocks (or nearly, for long pairs) and similar sweep
+   widths, so the threads of a warp step through their blocks and columns
+   together. */
+static inline int
+bucket_of (const gdp_pair_t &p, int W) {
+  gdp_geom_t g;
+  gdp_geom_of(&p, W, &g);
+  const int nblocks = g.X / W + 1;
+  const int width = W - 1 + g.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
+  return std::min(63, qlog(nblocks)) * 32 + std::min(31, qlog(width) / 2);
 }
 
 /* Fills ph for pairs[0..n) (pinned host buffers).  arena_bytes < 0 skips the
@@ -476,7 +490,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   int64_t *rec_off = ph.rec_off.as<int64_t>();
   /* counting sort by (kind, work bucket) */
   std::vector<int64_t> cnt((size_t) NKINDS * NBUCKETS, 0);
-  std::vector<uint16_t> key1(n, 0xffff), key2(n, 0xffff);
+  std::vector<uint32_t> key1(n, 0xffffffffu), key2(n, 0xffffffffu);
   int64_t words = 0, recs = 0, ntb = 0;
   int maxY[NKINDS] = {0};
   for (int64_t i = 0; i < n; i++) {
@@ -496,7 +510,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       const int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
       m.dir16 = words;
       words += (w + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
-      key1[i] = (uint16_t) (k * NBUCKETS + bucket_of(w));
+      key1[i] = (uint32_t) (k * NBUCKETS + bucket_of(p, 16));
       cnt[key1[i]]++;
       maxY[k] = std::max(maxY[k], Y);
     }
@@ -505,7 +519,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
       m.dir8 = words;
       words += (w + 3) & ~(int64_t) 3;
-      key2[i] = (uint16_t) (k * NBUCKETS + bucket_of(w));
+      key2[i] = (uint32_t) (k * NBUCKETS + bucket_of(p, 32));
       cnt[key2[i]]++;
       maxY[k] = std::max(maxY[k], Y);
     }
@@ -537,8 +551,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   ph.nlists = pos;
   int32_t *lists = ph.lists.as<int32_t>();
   for (int64_t i = 0; i < n; i++) {
-    if (key1[i] != 0xffff) lists[at[key1[i]]++] = (int32_t) i;
-    if (key2[i] != 0xffff) lists[at[key2[i]]++] = (int32_t) i;
+    if (key1[i] != 0xffffffffu) lists[at[key1[i]]++] = (int32_t) i;
+    if (key2[i] != 0xffffffffu) lists[at[key2[i]]++] = (int32_t) i;
     if (status[i] == GDP_OK && (pairs[i].flags & GDP_FLAG_TRACEBACK)) lists[tbpos++] = (int32_t) i;
   }
   ph.dir_words = words;

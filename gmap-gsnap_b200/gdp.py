@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libgdp.so")
+LIB_PATH = os.environ.get("GDP_LIB") or os.path.join(HERE, "lib", "libgdp.so")
 
 FULL, UPPER, LOWER = 0, 1, 2
 FLAG_JUMP_LATE, FLAG_REVP, FLAG_TRACEBACK, FLAG_RERUN16 = 1, 2, 4, 8
