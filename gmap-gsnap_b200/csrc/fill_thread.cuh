@@ -83,25 +83,275 @@ tie_max (int a, int b, bool &a_wins) {
   return m;
 }
 
+/* Per-pair constants of a fill at block height W. */
+struct PairView {
+  gdp_geom_t g;
+  bool revp;
+  int open, ext, oe, mt, lband, uband;
+  int dlo, dhi;                  /* in-band lanes of column y: y - dhi <= x <= y + dlo */
+  const char *lseq, *lalt, *sseq, *salt;
+  int llen, slen;
+};
+
+template <int W, int VARIANT>
+__device__ __forceinline__ void
+pair_view (const gdp_pair_t &p, const char *arena, PairView &v) {
+  gdp_geom_of(&p, W, &v.g);
+  v.revp = (p.flags & GDP_FLAG_REVP) != 0;
+  v.open = p.open; v.ext = p.extend; v.oe = p.open + p.extend;
+  v.mt = p.mismatchtype;
+  v.lband = p.lband; v.uband = p.uband;
+  v.dlo = (VARIANT == GDP_FULL) ? p.lband : 0;
+  v.dhi = (VARIANT == GDP_FULL) ? p.uband : (VARIANT == GDP_UPPER ? p.uband : p.lband);
+  v.lseq = arena + (VARIANT == GDP_LOWER ? p.gseq : p.rseq);
+  v.lalt = arena + (VARIANT == GDP_LOWER ? p.gseq_alt : p.rseq);
+  v.llen = (VARIANT == GDP_LOWER) ? p.glength : p.rlength;
+  v.sseq = arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq);
+  v.salt = arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq_alt);
+  v.slen = (VARIANT == GDP_LOWER) ? p.rlength : p.glength;
+}
+
+/* Classes (0..4) of swept column y for the two genome strings (lower: the
+   query class twice). */
+template <int VARIANT>
+__device__ __forceinline__ void
+column_classes (const PairView &v, const int8_t *nt2int, int y, int &ka, int &kb) {
+  if (VARIANT == GDP_LOWER) {
+    ka = kb = (y == 0) ? 4 : nt2int[seqch(v.sseq, v.slen, y, v.revp)];
+  } else if (y == 0) {
+    ka = kb = 4;
+  } else {
+    ka = nt2int[seqch(v.sseq, v.slen, y, v.revp)];
+    kb = nt2int[seqch(v.salt, v.slen, y, v.revp)];
+  }
+}
+
+/* The W lanes of one block: profiles and the (H, E) state of the last
+   swept column.  Fully unrolled loops keep the arrays in registers. */
+template <int W>
+struct Block {
+  int xlo, xhi, last, y0, y1;
+  uint32_t plo[W], phi4[W / 4];
+  int H[W], E[W];
+};
+
+/* Loads the lane profiles of block xlo and resets its state to the
+   reference's per-block start: H = NEG - open, E = NEG (late) / NEG + 1
+   (early) (src/dynprog_simd.c:6783-6799, :7038-7055). */
+template <int W, int VARIANT, bool LATE>
+__device__ __forceinline__ void
+block_start (Block<W> &B, const PairView &v, const gdp_tables_t *tab, int xlo) {
+  constexpr int LO = (W == 32) ? -128 : -32768;
+  B.xlo = xlo;
+  B.xhi = min(xlo + W - 1, v.g.X);
+  B.last = B.xhi - xlo;
+  gdp_block_sweep(&v.g, xlo, &B.y0, &B.y1);
+  /* bytes 0..3 of plo = scores against classes A,C,G,T; the class-N score
+     of lane i is byte (i & 3) of phi4[i >> 2] */
+#pragma unroll
+  for (int j = 0; j < W / 4; j++) B.phi4[j] = 0;
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    const int x = xlo + i;
+    uint32_t lo, hi;
+    if (VARIANT != GDP_LOWER) {
+      const int q = (x == 0) ? 'N' : (x <= v.llen ? seqch(v.lseq, v.llen, x, v.revp) : 'N');
+      lo = __ldg(&tab->profq_lo[v.mt][q]);
+      hi = __ldg(&tab->profq_hi[v.mt][q]);
+    } else if (x == 0) {
+      /* 16-bit: column 0 scores against 'N' (:8689); 8-bit: against code 4 (:5459) */
+      const int c0 = (W == 32) ? 4 : 'N';
+      lo = __ldg(&tab->profg_lo[v.mt][c0]);
+      hi = __ldg(&tab->profg_hi[v.mt][c0]);
+    } else if (x <= v.llen) {
+      const int a = seqch(v.lseq, v.llen, x, v.revp), b = seqch(v.lalt, v.llen, x, v.revp);
+      lo = bytemax(__ldg(&tab->profg_lo[v.mt][a]), __ldg(&tab->profg_lo[v.mt][b]));
+      hi = bytemax(__ldg(&tab->profg_hi[v.mt][a]), __ldg(&tab->profg_hi[v.mt][b]));
+    } else {
+      lo = 0; hi = 0;
+    }
+    B.plo[i] = lo;
+    B.phi4[i >> 2] |= (hi & 0xffu) << (8 * (i & 3));
+    B.H[i] = LO - v.open;
+    B.E[i] = LATE ? LO : LO + 1;
+  }
+}
+
+/*
+ * One swept column y of a block: the vector step (E, then H from the
+ * diagonal; src/dynprog_simd.c:6862-6913), the bottom-cell fix
+ * (:6926-6945) or the upper/lower E mask and diagonal fix (:7921-7969),
+ * and for the full band the F loop over the in-band lanes with the top-cell
+ * special case (:6950-7000).  Band geometry is reduced to lane masks that
+ * are uniform over the column.
+ *
+ *   diag   H[y-1][xlo-1] of the block above (final), or the reference's
+ *          row/column-0 values;
+ *   above  (H[y][xlo-1], FF[y]) of the block above.
+ * Writes the column's direction words to dcol (and scores to hd when not
+ * NULL).  Returns (H of the last lane, F carry) for the block below.
+ */
+template <int W, int VARIANT, bool LATE, int MODE>
+__device__ __forceinline__ int2
+block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int ka, int kb,
+              uint32_t *dcol, int16_t *hd, bool &reached, int &final_score) {
+  constexpr int LO = (W == 32) ? -128 : -32768;
+  constexpr int HI = (W == 32) ? 127 : 32767;
+  constexpr int WORDS = W / 8;
+  const int open = v.open, ext = v.ext;
+  const int xlo = B.xlo, last = B.last;
+  const bool col0 = (VARIANT == GDP_FULL) && (y == 0);
+  /* PRMT selectors; class N (4) reads byte 4 + (i & 3) of {phi4, plo} */
+  uint32_t sA[4], sB[4];
+  {
+    const uint32_t dA = (ka == 4) ? 0x1111u : 0u, dB = (kb == 4) ? 0x1111u : 0u;
+    sA[0] = GDP_SEL(ka); sB[0] = GDP_SEL(kb);
+#pragma unroll
+    for (int k = 1; k < 4; k++) { sA[k] = sA[k - 1] + dA; sB[k] = sB[k - 1] + dB; }
+  }
+  /* lane masks of this column */
+  const int rel = y - xlo;                       /* lane index of x == y */
+  uint32_t fmask = 0, topmask = 0, botmask = 0, emask = 0, dmask = 0;
+  if (VARIANT == GDP_FULL) {
+    const int t = rel - v.uband, bt = rel + v.lband;  /* top and bottom lanes */
+    const int flo = max(0, t + 1), fhi = min(bt, last);
+    if (fhi >= flo) fmask = lane_range(flo, fhi);
+    if (t >= 0 && t <= last) topmask = 1u << t;
+    if (y > 0 && bt >= 0 && bt <= last) botmask = 1u << bt;
+  } else {
+    if (rel <= W - 1) emask = lane_range(max(rel, 0), W - 1);
+    if (rel >= 0 && rel <= last) dmask = 1u << rel;
+  }
+  uint32_t w[WORDS];
+#pragma unroll
+  for (int j = 0; j < WORDS; j++) w[j] = 0;
+
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    const uint32_t bit = 1u << i;
+    const int Hold = B.H[i];
+    int Eold = B.E[i];
+    if (VARIANT != GDP_FULL && (emask & bit)) Eold = LO;
+    const int T1 = __viaddmax_s32(Hold, open, LO);
+    bool pE;
+    const int m = tie_max<LATE>(Eold, T1, pE);
+    int Ee = __viaddmax_s32(m, ext, LO);
+    if (VARIANT != GDP_FULL && (emask & bit)) Ee = LO;
+    int ps;
+    if (VARIANT == GDP_FULL && col0) {
+      ps = (xlo + i == 0) ? 0 : LO;     /* pairscores_col0 (:6668-6678) */
+    } else if (VARIANT == GDP_LOWER) {
+      ps = prof_byte(B.plo[i], B.phi4[i >> 2], sA[i & 3]);
+    } else {
+      ps = max(prof_byte(B.plo[i], B.phi4[i >> 2], sA[i & 3]), prof_byte(B.plo[i], B.phi4[i >> 2], sB[i & 3]));
+    }
+    const int Hv = min(__viaddmax_s32(diag, ps, LO), HI);
+    diag = Hold;
+    bool pN;
+    int Hn = tie_max<LATE>(Ee, Hv, pN);
+    if (VARIANT == GDP_FULL) {
+      if (botmask & bit) { Hn = Hv; pE = false; pN = false; }
+    } else {
+      if (dmask & bit) { pE = false; pN = false; }
+    }
+    B.H[i] = Hn;
+    B.E[i] = Ee;
+    if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
+    if (pN) w[i >> 3] |= 1u << (i & 7);
+  }
+  int2 out;
+  if (VARIANT == GDP_FULL) {
+    int Fp, Hp;
+    if (xlo == 0 || y >= xlo + v.uband) { Fp = GDP_NEGINT; Hp = GDP_NEGINT; }
+    else { Fp = above.y; Hp = above.x; }
+#pragma unroll
+    for (int i = 0; i < W; i++) {
+      const uint32_t bit = 1u << i;
+      if (topmask & bit) {
+        Fp = GDP_NEGINT + v.oe;
+        Hp = B.H[i];
+      } else if (fmask & bit) {
+        bool pF, pV;
+        const int F = tie_max<LATE>(Fp, Hp + open, pF) + ext;
+        const int Hn = tie_max<LATE>(F, B.H[i], pV);
+        B.H[i] = Hn;
+        Hp = Hn;
+        Fp = F;
+        if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
+        if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
+      }
+    }
+    out = make_int2(B.H[W - 1], Fp);
+  } else {
+    out = make_int2(B.H[W - 1], 0);
+  }
+  if (MODE != 0 && !reached && y >= 1) {
+    const int dl = max(rel - v.dhi, (xlo == 0) ? 1 : 0), dh = min(rel + v.dlo, last);
+    if (dh >= dl) {
+      const uint32_t dom = lane_range(max(dl, 0), dh);
+#pragma unroll
+      for (int i = 0; i < W; i++)
+        if ((dom & (1u << i)) && B.H[i] >= 127) reached = true;
+    }
+  }
+  if (y == v.g.Y) {
+#pragma unroll
+    for (int i = 0; i < W; i++) if (xlo + i == v.g.X) final_score = B.H[i];
+  }
+  if (hd != nullptr) {
+#pragma unroll
+    for (int i = 0; i < W; i++) hd[i] = (int16_t) B.H[i];
+  }
+  if (WORDS == 2) {
+    *reinterpret_cast<uint2 *>(dcol) = make_uint2(w[0], w[1]);
+  } else {
+    *reinterpret_cast<uint4 *>(dcol) = make_uint4(w[0], w[1], w[WORDS > 2 ? 2 : 0], w[WORDS > 3 ? 3 : 0]);
+  }
+  return out;
+}
+
+/* Writes the per-pair outcome of a fill (see MODE). */
+template <int W, int MODE>
+__device__ __forceinline__ void
+fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, bool reached, int final_score) {
+  int y0l, y1l;
+  gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
+  const bool swept = (g.Y >= y0l && g.Y <= y1l);   /* the final cell was filled */
+  if (MODE == 1) {
+    mp->maxh16 = reached ? 127 : -32768;   /* >= 127 iff an in-band 16-bit score reached 127 */
+    mp->final16 = final_score;
+  }
+  if (MODE == 2) {
+    const bool overflow = reached || final_score <= -128 + 30;
+    mp->status8 = overflow ? 1 : 0;
+    mp->final8 = final_score;
+    if (!overflow) {
+      P.res[pi].score = final_score;
+      P.res[pi].precision = 8;
+      P.res[pi].rerun = 0;
+    }
+  } else {
+    gdp_result_t *r = P.res + pi;
+    r->score = final_score;
+    r->precision = W == 16 ? 16 : 8;
+    r->rerun = (MODE == 1) ? 1 : 0;
+    if (!swept) r->status = GDP_ERR_BAND;
+  }
+}
+
+#ifndef GDP_FILL_MINB
+#define GDP_FILL_MINB 5
+#endif
+
 /* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records whether an
    in-band score reaches 127), 2 = 8-bit pass of a rerun pair (skipped when
    the 16-bit pass proved an overflow; stops at the first in-band 127).
-
-   Per block column the band geometry is reduced to a few lane masks that
-   are uniform over the column: the lanes of the F loop, the top cell
-   (src/dynprog_simd.c:6962-6974), the bottom cell (:6926-6945), the lanes
-   whose E is clamped (upper/lower E_mask, :7921, :7943) and the diagonal
-   cell (:7966-7969).  The lane loop is fully unrolled, so each mask test is
-   a test of a constant bit. */
-#ifndef GDP_FILL_MINB
-#define GDP_FILL_MINB 1
-#endif
-
+   One thread per pair; the next column's characters and carry are fetched
+   one column ahead. */
 template <int W, int VARIANT, bool LATE, int MODE>
 __global__ void __launch_bounds__(128, (W == 16) ? GDP_FILL_MINB : 1)
 fill_thread_kernel (FillParams P) {
   constexpr int LO = (W == 32) ? -128 : -32768;
-  constexpr int HI = (W == 32) ? 127 : 32767;
   constexpr int WORDS = W / 8;
   __shared__ int8_t s_nt2int[128];
   for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
@@ -117,228 +367,231 @@ fill_thread_kernel (FillParams P) {
       mp->status8 = 1;   /* the 16-bit scores reach 127, so the 8-bit fill overflows */
       continue;
     }
-    gdp_geom_t g;
-    gdp_geom_of(&p, W, &g);
-    const bool revp = (p.flags & GDP_FLAG_REVP) != 0;
-    const int open = p.open, ext = p.extend, oe = p.open + p.extend;
-    const int mt = p.mismatchtype;
-    const int lband = p.lband, uband = p.uband;
-    const char *lseq = P.arena + (VARIANT == GDP_LOWER ? p.gseq : p.rseq);
-    const char *lalt = P.arena + (VARIANT == GDP_LOWER ? p.gseq_alt : p.rseq);
-    const int llen = (VARIANT == GDP_LOWER) ? p.glength : p.rlength;
-    const char *sseq = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq);
-    const char *salt = P.arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq_alt);
-    const int slen = (VARIANT == GDP_LOWER) ? p.rlength : p.glength;
-    /* domain band of the lane index relative to y: lanes x with y - dhi <= x <= y + dlo */
-    const int dlo = (VARIANT == GDP_FULL) ? lband : 0;
-    const int dhi = (VARIANT == GDP_FULL) ? uband : (VARIANT == GDP_UPPER ? uband : lband);
+    PairView v;
+    pair_view<W, VARIANT>(p, P.arena, v);
     uint32_t *dir = P.dirs + ((W == 16) ? mp->dir16 : mp->dir8);
     int2 *sc = P.scratch + slot;
     const int64_t scs = P.nslots;
     int final_score = LO;
-    bool reached = false;     /* an in-band score reached 127 */
+    bool reached = false;
 
-    for (int xlo = 0; xlo <= g.X; xlo += W) {
-      const int xhi = min(xlo + W - 1, g.X);
-      const int last = xhi - xlo;
-      int y0, y1;
-      gdp_block_sweep(&g, xlo, &y0, &y1);
-      if (y1 < y0) continue;
-
-      /* lane profiles: bytes 0..3 of plo = scores against classes A,C,G,T;
-         the class-N score of lane i is byte (i & 3) of phi4[i >> 2] */
-      uint32_t plo[W], phi4[W / 4];
-#pragma unroll
-      for (int j = 0; j < W / 4; j++) phi4[j] = 0;
-#pragma unroll
-      for (int i = 0; i < W; i++) {
-        const int x = xlo + i;
-        uint32_t lo, hi;
-        if (VARIANT != GDP_LOWER) {
-          const int q = (x == 0) ? 'N' : (x <= llen ? seqch(lseq, llen, x, revp) : 'N');
-          lo = __ldg(&P.tab->profq_lo[mt][q]);
-          hi = __ldg(&P.tab->profq_hi[mt][q]);
-        } else if (x == 0) {
-          /* 16-bit: column 0 scores against 'N' (:8689); 8-bit: against code 4 (:5459) */
-          const int c0 = (W == 32) ? 4 : 'N';
-          lo = __ldg(&P.tab->profg_lo[mt][c0]);
-          hi = __ldg(&P.tab->profg_hi[mt][c0]);
-        } else if (x <= llen) {
-          const int a = seqch(lseq, llen, x, revp), b = seqch(lalt, llen, x, revp);
-          lo = bytemax(__ldg(&P.tab->profg_lo[mt][a]), __ldg(&P.tab->profg_lo[mt][b]));
-          hi = bytemax(__ldg(&P.tab->profg_hi[mt][a]), __ldg(&P.tab->profg_hi[mt][b]));
-        } else {
-          lo = 0; hi = 0;
-        }
-        plo[i] = lo;
-        phi4[i >> 2] |= (hi & 0xffu) << (8 * (i & 3));
-      }
-      int H[W], E[W];
-#pragma unroll
-      for (int i = 0; i < W; i++) { H[i] = LO - open; E[i] = LATE ? LO : LO + 1; }
+    for (int xlo = 0; xlo <= v.g.X; xlo += W) {
+      Block<W> B;
+      block_start<W, VARIANT, LATE>(B, v, P.tab, xlo);
+      if (B.y1 < B.y0) continue;
       int bot_prev = LO;   /* H[y-1][xlo-1] from the block above */
-      if (xlo > 0 && y0 > 0) bot_prev = sc[(int64_t) (y0 - 1) * scs].x;
+      if (xlo > 0 && B.y0 > 0) bot_prev = sc[(int64_t) (B.y0 - 1) * scs].x;
+      /* fetch column y0's inputs */
+      int ka, kb;
+      column_classes<VARIANT>(v, s_nt2int, B.y0, ka, kb);
+      int2 above = make_int2(LO, GDP_NEGINT);
+      if (xlo > 0) above = sc[(int64_t) B.y0 * scs];
       uint32_t *dcol = dir;
-
-      for (int y = y0; y <= y1; y++) {
-        /* swept-column classes -> PRMT selectors; class N (4) reads the
-           packed byte (i & 3) of phi4, i.e. byte 4 + (i & 3) of {phi4, plo} */
-        int ka, kb;
-        if (VARIANT == GDP_LOWER) {
-          ka = kb = (y == 0) ? 4 : s_nt2int[seqch(sseq, slen, y, revp)];
-        } else if (y == 0) {
-          ka = kb = 4;
-        } else {
-          ka = s_nt2int[seqch(sseq, slen, y, revp)];
-          kb = s_nt2int[seqch(salt, slen, y, revp)];
+      for (int y = B.y0; y <= B.y1; y++) {
+        /* prefetch column y + 1 */
+        int ka2 = 0, kb2 = 0;
+        int2 above2 = make_int2(LO, GDP_NEGINT);
+        if (y < B.y1) {
+          column_classes<VARIANT>(v, s_nt2int, y + 1, ka2, kb2);
+          if (xlo > 0) above2 = sc[(int64_t) (y + 1) * scs];
         }
-        const bool col0 = (VARIANT == GDP_FULL) && (y == 0);
-        uint32_t sA[4], sB[4];
-        {
-          const uint32_t dA = (ka == 4) ? 0x1111u : 0u, dB = (kb == 4) ? 0x1111u : 0u;
-          sA[0] = GDP_SEL(ka); sB[0] = GDP_SEL(kb);
-#pragma unroll
-          for (int k = 1; k < 4; k++) { sA[k] = sA[k - 1] + dA; sB[k] = sB[k - 1] + dB; }
-        }
-        int2 above = make_int2(LO, GDP_NEGINT);
-        if (xlo > 0) above = sc[(int64_t) y * scs];
         int diag;
         if (y == 0) diag = (VARIANT == GDP_FULL) ? (xlo == 0 ? 0 : LO) : 0;
         else diag = (xlo == 0) ? LO : bot_prev;
         bot_prev = above.x;
-
-        /* lane masks of this column */
-        const int rel = y - xlo;                       /* lane index of x == y */
-        uint32_t fmask = 0, topmask = 0, botmask = 0, emask = 0, dmask = 0;
-        if (VARIANT == GDP_FULL) {
-          const int t = rel - uband, bt = rel + lband;  /* top and bottom lanes */
-          const int flo = max(0, t + 1), fhi = min(bt, last);
-          if (fhi >= flo) fmask = lane_range(flo, fhi);
-          if (t >= 0 && t <= last) topmask = 1u << t;
-          if (y > 0 && bt >= 0 && bt <= last) botmask = 1u << bt;
-        } else {
-          if (rel <= W - 1) emask = lane_range(max(rel, 0), W - 1);
-          if (rel >= 0 && rel <= last) dmask = 1u << rel;
-        }
-        uint32_t w[WORDS];
-#pragma unroll
-        for (int j = 0; j < WORDS; j++) w[j] = 0;
-
-        /* vector step (E, then H from the diagonal), :6862-6913 */
-#pragma unroll
-        for (int i = 0; i < W; i++) {
-          const uint32_t bit = 1u << i;
-          const int Hold = H[i];
-          int Eold = E[i];
-          if (VARIANT != GDP_FULL && (emask & bit)) Eold = LO;
-          const int T1 = __viaddmax_s32(Hold, open, LO);
-          bool pE;
-          const int m = tie_max<LATE>(Eold, T1, pE);
-          int Ee = __viaddmax_s32(m, ext, LO);
-          if (VARIANT != GDP_FULL && (emask & bit)) Ee = LO;
-          int ps;
-          if (VARIANT == GDP_FULL && col0) {
-            ps = (xlo + i == 0) ? 0 : LO;     /* pairscores_col0 (:6668-6678) */
-          } else if (VARIANT == GDP_LOWER) {
-            ps = prof_byte(plo[i], phi4[i >> 2], sA[i & 3]);
-          } else {
-            ps = max(prof_byte(plo[i], phi4[i >> 2], sA[i & 3]), prof_byte(plo[i], phi4[i >> 2], sB[i & 3]));
-          }
-          const int Hv = min(__viaddmax_s32(diag, ps, LO), HI);
-          diag = Hold;
-          bool pN;
-          int Hn = tie_max<LATE>(Ee, Hv, pN);
-          if (VARIANT == GDP_FULL) {
-            if (botmask & bit) { Hn = Hv; pE = false; pN = false; }
-          } else {
-            if (dmask & bit) { pE = false; pN = false; }
-          }
-          H[i] = Hn;
-          E[i] = Ee;
-          if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
-          if (pN) w[i >> 3] |= 1u << (i & 7);
-        }
-        if (VARIANT == GDP_FULL) {
-          /* F loop over the in-band lanes (:6916-7000) */
-          int Fp, Hp;
-          if (xlo == 0 || y >= xlo + uband) { Fp = GDP_NEGINT; Hp = GDP_NEGINT; }
-          else { Fp = above.y; Hp = above.x; }
-#pragma unroll
-          for (int i = 0; i < W; i++) {
-            const uint32_t bit = 1u << i;
-            if (topmask & bit) {
-              Fp = GDP_NEGINT + oe;
-              Hp = H[i];
-            } else if (fmask & bit) {
-              bool pF, pV;
-              const int F = tie_max<LATE>(Fp, Hp + open, pF) + ext;
-              const int Hn = tie_max<LATE>(F, H[i], pV);
-              H[i] = Hn;
-              Hp = Hn;
-              Fp = F;
-              if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
-              if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
-            }
-          }
-          sc[(int64_t) y * scs] = make_int2(H[W - 1], Fp);
-        } else {
-          sc[(int64_t) y * scs] = make_int2(H[W - 1], 0);
-        }
-        if (MODE != 0 && !reached && y >= 1) {
-          /* in-band lanes: y - dhi <= x <= y + dlo, x >= 1 */
-          const int dl = max(rel - dhi, (xlo == 0) ? 1 : 0), dh = min(rel + dlo, last);
-          if (dh >= dl) {
-            const uint32_t dom = lane_range(max(dl, 0), dh);
-#pragma unroll
-            for (int i = 0; i < W; i++)
-              if ((dom & (1u << i)) && H[i] >= 127) reached = true;
-          }
-        }
-        if (y == g.Y) {
-#pragma unroll
-          for (int i = 0; i < W; i++) if (xlo + i == g.X) final_score = H[i];
-        }
-        if (P.hdump != nullptr) {
-          int16_t *hd = P.hdump + (dcol - P.dirs) * 8;
-#pragma unroll
-          for (int i = 0; i < W; i++) hd[i] = (int16_t) H[i];
-        }
-        if (WORDS == 2) {
-          *reinterpret_cast<uint2 *>(dcol) = make_uint2(w[0], w[1]);
-        } else {
-          *reinterpret_cast<uint4 *>(dcol) = make_uint4(w[0], w[1], w[WORDS > 2 ? 2 : 0], w[WORDS > 3 ? 3 : 0]);
-        }
+        int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
+        const int2 out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd,
+                                                              reached, final_score);
+        sc[(int64_t) y * scs] = out;
         dcol += WORDS;
+        ka = ka2; kb = kb2; above = above2;
         if (MODE == 2 && reached) break;
       }
       dir = dcol;
       if (MODE == 2 && reached) break;
     }
+    fill_finish<W, MODE>(P, pi, mp, v.g, reached, final_score);
+  }
+}
 
-    /* the final cell must have been swept */
-    int y0l, y1l;
-    gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
-    const bool swept = (g.Y >= y0l && g.Y <= y1l);
-    if (MODE == 1) {
-      mp->maxh16 = reached ? 127 : -32768;   /* >= 127 iff an in-band 16-bit score reached 127 */
-      mp->final16 = final_score;
+/*
+ * One warp per pair for long 16-bit pairs (plain fills).  Lane l owns the
+ * blocks b = l, l + 32, l + 64, ... and processes column y of block b at
+ * step t = y + b: block b needs the final column y (F carry, last lane H)
+ * and column y - 1 (diagonal) of block b - 1, which lane (l - 1) mod 32
+ * produced one and two steps earlier, so one rotation shuffle per step
+ * carries them.  A lane's next block starts after its previous one ends as
+ * long as a block sweeps fewer than 32 * 17 - 16 columns; the planner only
+ * sends pairs with narrower sweeps here.  Each lane runs block_column, the
+ * same column step as the one-thread-per-pair kernel.
+ */
+template <int VARIANT, bool LATE>
+__global__ void __launch_bounds__(128, 4)
+fill_warp_kernel (FillParams P) {
+  constexpr int W = 16, WORDS = 2, LO = -32768;
+  __shared__ int8_t s_nt2int[128];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
+  const int n = *P.count;
+  for (int64_t li = warp; li < n; li += nwarps) {
+    const int pi = __ldg(P.list + li);
+    const gdp_pair_t p = P.pairs[pi];
+    gdp_meta_t *mp = P.meta + pi;
+    PairView v;
+    pair_view<W, VARIANT>(p, P.arena, v);
+    uint32_t *dir = P.dirs + mp->dir16;
+    /* blocks that sweep something: 0 .. nb - 1 */
+    int nb = v.g.X / W + 1;
+    while (nb > 0) {
+      int a0, a1;
+      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+      if (a1 >= a0) break;
+      nb--;
     }
-    if (MODE == 2) {
-      const bool overflow = reached || final_score <= -128 + 30;
-      mp->status8 = overflow ? 1 : 0;
-      mp->final8 = final_score;
-      if (!overflow) {
-        P.res[pi].score = final_score;
-        P.res[pi].precision = 8;
-        P.res[pi].rerun = 0;
+    int tend = -1;
+    if (nb > 0) {
+      int a0, a1;
+      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+      tend = a1 + nb - 1;
+    }
+    /* this lane's first block and its word offset */
+    int b = lane;
+    int64_t boff = 0;
+    for (int k = 0; k < b && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
+    Block<W> B;
+    bool started = false;
+    int final_score = LO;
+    bool reached = false;
+    int2 mine = make_int2(LO, GDP_NEGINT);   /* this lane's output of the last step */
+    int bot_prev = LO;                         /* H[y-1][xlo-1] received a step ago */
+    for (int t = 0; t <= tend; t++) {
+      /* (H, F) of block b - 1 at column t - b, produced by the previous lane */
+      const int rx = __shfl_sync(0xffffffffu, mine.x, (lane + 31) & 31);
+      const int ry = __shfl_sync(0xffffffffu, mine.y, (lane + 31) & 31);
+      if (b < nb) {
+        if (!started) {
+          block_start<W, VARIANT, LATE>(B, v, P.tab, b * W);
+          started = true;
+        }
+        const int y = t - b;
+        if (y >= B.y0 && y <= B.y1) {
+          int ka, kb;
+          column_classes<VARIANT>(v, s_nt2int, y, ka, kb);
+          const int2 above = (b > 0) ? make_int2(rx, ry) : make_int2(LO, GDP_NEGINT);
+          int diag;
+          if (y == 0) diag = (VARIANT == GDP_FULL) ? (b == 0 ? 0 : LO) : 0;
+          else diag = (b == 0) ? LO : bot_prev;
+          uint32_t *dcol = dir + boff + (int64_t) (y - B.y0) * WORDS;
+          int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
+          mine = block_column<W, VARIANT, LATE, 0>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
+                                                   final_score);
+          if (y == B.y1) {
+            /* move to block b + 32 */
+            for (int k = b; k < b + 32 && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
+            b += 32;
+            started = false;
+          }
+        }
       }
-    } else {
-      gdp_result_t *r = P.res + pi;
-      r->score = final_score;
-      r->precision = W == 16 ? 16 : 8;
-      r->rerun = (MODE == 1) ? 1 : 0;
-      if (!swept) r->status = GDP_ERR_BAND;
+      bot_prev = rx;
     }
+    /* the lane that owned the final cell's block reports its score */
+    const int fs = __shfl_sync(0xffffffffu, final_score, (v.g.X / W) & 31);
+    if (lane == 0) fill_finish<W, 0>(P, pi, mp, v.g, false, fs);
+  }
+}
+
+/*
+ * One CTA of NW warps per pair for 16-bit plain fills whose blocks sweep
+ * too many columns for one warp (wide bands: cDNA gap fills, long reads
+ * with wide bands).  Same schedule as fill_warp_kernel over 32 * NW lanes:
+ * lane L owns blocks L, L + 32 NW, ... and processes column y of block b at
+ * step t = y + b.  Inside a warp the hand-off from block b - 1 is a
+ * shuffle; across warps the last lane of each warp leaves its output in a
+ * double-buffered shared slot, and one barrier per step orders it.
+ */
+template <int VARIANT, bool LATE, int NW>
+__global__ void __launch_bounds__(NW * 32)
+fill_cta_kernel (FillParams P) {
+  constexpr int W = 16, WORDS = 2, LO = -32768, NL = NW * 32;
+  __shared__ int8_t s_nt2int[128];
+  __shared__ int2 s_hand[2][NW];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
+  __syncthreads();
+  const int L = threadIdx.x, lane = L & 31, wid = L >> 5;
+  const int n = *P.count;
+  for (int64_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const int pi = __ldg(P.list + li);
+    const gdp_pair_t p = P.pairs[pi];
+    gdp_meta_t *mp = P.meta + pi;
+    PairView v;
+    pair_view<W, VARIANT>(p, P.arena, v);
+    uint32_t *dir = P.dirs + mp->dir16;
+    int nb = v.g.X / W + 1;
+    while (nb > 0) {
+      int a0, a1;
+      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+      if (a1 >= a0) break;
+      nb--;
+    }
+    int tend = -1;
+    if (nb > 0) {
+      int a0, a1;
+      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+      tend = a1 + nb - 1;
+    }
+    int b = L;
+    int64_t boff = 0;
+    for (int k = 0; k < b && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
+    Block<W> B;
+    bool started = false, reached = false;
+    int final_score = LO;
+    int2 mine = make_int2(LO, GDP_NEGINT);
+    int bot_prev = LO;
+    if (L < NW) s_hand[1][L] = make_int2(LO, GDP_NEGINT);
+    __syncthreads();
+    for (int t = 0; t <= tend; t++) {
+      /* (H, F) of block b - 1 at column t - b from the previous lane */
+      int rx = __shfl_sync(0xffffffffu, mine.x, (lane + 31) & 31);
+      int ry = __shfl_sync(0xffffffffu, mine.y, (lane + 31) & 31);
+      if (lane == 0) {
+        const int2 h = s_hand[(t + 1) & 1][(wid + NW - 1) % NW];
+        rx = h.x;
+        ry = h.y;
+      }
+      if (b < nb) {
+        if (!started) {
+          block_start<W, VARIANT, LATE>(B, v, P.tab, b * W);
+          started = true;
+        }
+        const int y = t - b;
+        if (y >= B.y0 && y <= B.y1) {
+          int ka, kb;
+          column_classes<VARIANT>(v, s_nt2int, y, ka, kb);
+          const int2 above = (b > 0) ? make_int2(rx, ry) : make_int2(LO, GDP_NEGINT);
+          int diag;
+          if (y == 0) diag = (VARIANT == GDP_FULL) ? (b == 0 ? 0 : LO) : 0;
+          else diag = (b == 0) ? LO : bot_prev;
+          uint32_t *dcol = dir + boff + (int64_t) (y - B.y0) * WORDS;
+          int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
+          mine = block_column<W, VARIANT, LATE, 0>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
+                                                   final_score);
+          if (y == B.y1) {
+            for (int k = b; k < b + NL && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
+            b += NL;
+            started = false;
+          }
+        }
+      }
+      bot_prev = rx;
+      if (lane == 31) s_hand[t & 1][wid] = mine;
+      __syncthreads();
+    }
+    if (L == ((v.g.X / W) % NL)) fill_finish<W, 0>(P, pi, mp, v.g, false, final_score);
+    __syncthreads();
   }
 }
 

@@ -79,11 +79,23 @@ struct HostBuf {   /* pinned host memory */
   template <class T> T *as () const { return (T *) p; }
 };
 
-constexpr int NKINDS = 24;   /* (W32, variant, late, pass) */
+constexpr int NTHREADKINDS = 24;   /* one thread per pair: (W32, variant, late, pass) */
+constexpr int NWARPKINDS = 6;      /* one warp per pair (16-bit plain): 24 + variant * 2 + late */
+constexpr int NCTAKINDS = 24;      /* one CTA per pair (16-bit plain): 30 + (variant * 2 + late) * 4 + log2(NW) - 1 */
+constexpr int NKINDS = NTHREADKINDS + NWARPKINDS + NCTAKINDS;
+constexpr int CTA_NW[4] = {2, 4, 8, 16};
 constexpr int NBUCKETS = 64 * 32; /* (block count, sweep width) buckets inside a bin */
 
 inline int kind_id (int w32, int variant, int late, int pass) {
   return (((w32 * 3 + variant) * 2 + late) * 2) + pass;
+}
+
+inline int warp_kind_id (int variant, int late) {
+  return NTHREADKINDS + variant * 2 + late;
+}
+
+inline int cta_kind_id (int variant, int late, int nwi) {
+  return NTHREADKINDS + NWARPKINDS + (variant * 2 + late) * 4 + nwi;
 }
 
 }  // namespace
@@ -141,6 +153,8 @@ struct gdp_ctx {
   uint64_t genome_len = 0;
   int64_t budget = 0;
   int64_t wave = 131072;
+  int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
+  int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
   DevBuf arena, scratch;
   Slot slot[2];
   std::atomic<int64_t> launches{0};
@@ -150,21 +164,38 @@ struct gdp_ctx {
   bool profiling = false;
   struct Timed { int id; cudaEvent_t a, b; };
   std::vector<Timed> timed;
-  double prof_ms[32] = {0};
-  int64_t prof_n[32] = {0};
+  double prof_ms[64] = {0};
+  int64_t prof_n[64] = {0};
 };
 
-/* kernel ids for profiling: 0..23 fill kinds, 24 traceback, 25 init,
-   26 integer probe, 27 rerun compaction, 28 record compaction */
-#define NPROF 29
+/* kernel ids for profiling: 0..NKINDS-1 fill kinds, then traceback, init,
+   integer probe, rerun compaction, record compaction */
+#define PROF_TB (NKINDS)
+#define PROF_INIT (NKINDS + 1)
+#define PROF_PEAK (NKINDS + 2)
+#define PROF_RERUN (NKINDS + 3)
+#define PROF_RECS (NKINDS + 4)
+#define NPROF (NKINDS + 5)
 static const char *
 kernel_name (int id) {
-  static char buf[32][48];
-  if (id == 24) return "traceback_kernel";
-  if (id == 25) return "init_results_kernel";
-  if (id == 26) return "int_peak_kernel";
-  if (id == 27) return "compact_rerun_kernel";
-  if (id == 28) return "compact_records_kernel";
+  static char buf[NPROF][48];
+  if (id == PROF_TB) return "traceback_kernel";
+  if (id == PROF_INIT) return "init_results_kernel";
+  if (id == PROF_PEAK) return "int_peak_kernel";
+  if (id == PROF_RERUN) return "compact_rerun_kernel";
+  if (id == PROF_RECS) return "compact_records_kernel";
+  if (id >= NTHREADKINDS + NWARPKINDS) {
+    const int c = id - NTHREADKINDS - NWARPKINDS, vl = c / 4, variant = vl / 2, late = vl & 1;
+    snprintf(buf[id], sizeof(buf[id]), "fill_cta<W16,%s,%s,%dwarps>",
+             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early", CTA_NW[c % 4]);
+    return buf[id];
+  }
+  if (id >= NTHREADKINDS) {
+    const int variant = (id - NTHREADKINDS) / 2, late = (id - NTHREADKINDS) & 1;
+    snprintf(buf[id], sizeof(buf[id]), "fill_warp<W16,%s,%s>",
+             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early");
+    return buf[id];
+  }
   const int pass = id & 1, late = (id >> 1) & 1, vw = id >> 2, variant = vw % 3, w32 = vw / 3;
   snprintf(buf[id], sizeof(buf[id]), "fill_thread<W%d,%s,%s,%s>", w32 ? 32 : 16,
            variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early",
@@ -266,6 +297,8 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   }
   const char *w = getenv("GDP_WAVE_PAIRS");
   if (w && atol(w) > 0) ctx->wave = atol(w);
+  const char *wx = getenv("GDP_WARP_MIN_X");
+  if (wx && atoi(wx) > 0) ctx->warp_min_x = atoi(wx);
   *out = ctx;
   return GDP_OK;
 }
@@ -335,7 +368,7 @@ extern "C" int
 gdp_profile_reset (gdp_ctx *ctx) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   prof_collect(ctx);
-  for (int i = 0; i < 32; i++) { ctx->prof_ms[i] = 0; ctx->prof_n[i] = 0; }
+  for (int i = 0; i < 64; i++) { ctx->prof_ms[i] = 0; ctx->prof_n[i] = 0; }
   return GDP_OK;
 }
 
@@ -507,7 +540,20 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     const int Y = (p.variant == GDP_LOWER) ? p.rlength : p.glength;
     if (p.precision == 16 || rerun) {
       const int64_t w = gdp_pair_words(&p, 16);
-      const int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
+      gdp_geom_t g16;
+      gdp_geom_of(&p, 16, &g16);
+      const int sweep = 15 + g16.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
+      int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
+      if (!rerun && g16.X >= ctx->warp_min_x) {
+        if (sweep <= ctx->warp_max_sweep) {
+          k = warp_kind_id(p.variant, late);
+        } else {
+          /* enough lanes that a lane's next block starts after its last one ends */
+          for (int nwi = 0; nwi < 4; nwi++) {
+            if (sweep + 16 < CTA_NW[nwi] * 32 * 17 - 16) { k = cta_kind_id(p.variant, late, nwi); break; }
+          }
+        }
+      }
       m.dir16 = words;
       words += (w + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
       key1[i] = (uint32_t) (k * NBUCKETS + bucket_of(p, 16));
@@ -530,6 +576,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     }
   }
   /* offsets: kinds in order, heaviest bucket first inside a kind */
+  static_assert(NKINDS * NBUCKETS < (1 << 30), "bucket keys fit in 32 bits");
   std::vector<int64_t> at((size_t) NKINDS * NBUCKETS, 0);
   int64_t pos = 0;
   for (int k = 0; k < NKINDS; k++) {
@@ -689,6 +736,45 @@ fill_grid (gdp_ctx *ctx, int64_t count) {
   return (int) std::max<int64_t>(1, std::min<int64_t>((count + 127) / 128, (int64_t) ctx->nsm * 16));
 }
 
+/* warp kinds: one warp per pair, 4 pairs per block of 128 */
+static inline int
+warp_grid (gdp_ctx *ctx, int64_t count) {
+  return (int) std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t) ctx->nsm * 16));
+}
+
+template <int V, bool L>
+static void launch_cta (int nwi, FillParams P, int grid, cudaStream_t s) {
+  switch (CTA_NW[nwi]) {
+  case 2: fill_cta_kernel<V, L, 2><<<grid, 64, 0, s>>>(P); break;
+  case 4: fill_cta_kernel<V, L, 4><<<grid, 128, 0, s>>>(P); break;
+  case 8: fill_cta_kernel<V, L, 8><<<grid, 256, 0, s>>>(P); break;
+  default: fill_cta_kernel<V, L, 16><<<grid, 512, 0, s>>>(P); break;
+  }
+}
+
+static void
+launch_cta_kind (int k, FillParams P, int grid, cudaStream_t s) {
+  const int c = k - NTHREADKINDS - NWARPKINDS, vl = c / 4, variant = vl / 2, late = vl & 1, nwi = c % 4;
+  if (variant == GDP_FULL) { if (late) launch_cta<GDP_FULL, true>(nwi, P, grid, s); else launch_cta<GDP_FULL, false>(nwi, P, grid, s); }
+  else if (variant == GDP_UPPER) { if (late) launch_cta<GDP_UPPER, true>(nwi, P, grid, s); else launch_cta<GDP_UPPER, false>(nwi, P, grid, s); }
+  else { if (late) launch_cta<GDP_LOWER, true>(nwi, P, grid, s); else launch_cta<GDP_LOWER, false>(nwi, P, grid, s); }
+}
+
+static void
+launch_warp_kind (int k, FillParams P, int grid, cudaStream_t s) {
+  const int variant = (k - NTHREADKINDS) / 2, late = (k - NTHREADKINDS) & 1;
+  if (variant == GDP_FULL) {
+    if (late) fill_warp_kernel<GDP_FULL, true><<<grid, 128, 0, s>>>(P);
+    else fill_warp_kernel<GDP_FULL, false><<<grid, 128, 0, s>>>(P);
+  } else if (variant == GDP_UPPER) {
+    if (late) fill_warp_kernel<GDP_UPPER, true><<<grid, 128, 0, s>>>(P);
+    else fill_warp_kernel<GDP_UPPER, false><<<grid, 128, 0, s>>>(P);
+  } else {
+    if (late) fill_warp_kernel<GDP_LOWER, true><<<grid, 128, 0, s>>>(P);
+    else fill_warp_kernel<GDP_LOWER, false><<<grid, 128, 0, s>>>(P);
+  }
+}
+
 /* Enqueues fills and tracebacks of a planned batch on the compute stream.
    d_slots receives records at the plan's slot offsets. */
 static int
@@ -701,12 +787,12 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   prof_begin(ctx, &ev0);
   init_results_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
       d_res, pd.status.as<int32_t>(), d_pairs, n);
-  prof_end(ctx, 25, ev0);
+  prof_end(ctx, PROF_INIT, ev0);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   CK(ctx, cudaMemcpyAsync(pd.meta.p, pd.meta0.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToDevice, s));
   size_t need = 0;
-  for (int k = 0; k < NKINDS; k++) {
+  for (int k = 0; k < NTHREADKINDS; k++) {
     if (!ph.counts[k]) continue;
     need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
@@ -714,10 +800,13 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs */
   for (int round = 0; round < 2; round++) {
     for (int k = 0; k < NKINDS; k++) {
-      const int w32 = (k >> 2) / 3, pass = k & 1;
+      const bool warp = k >= NTHREADKINDS && k < NTHREADKINDS + NWARPKINDS;
+      const bool cta = k >= NTHREADKINDS + NWARPKINDS;
+      const int w32 = (warp || cta) ? 0 : (k >> 2) / 3, pass = (warp || cta) ? 0 : (k & 1);
       const bool second = (w32 == 1 && pass == 1);
       if ((round == 0) == second || !ph.counts[k]) continue;
-      const int grid = fill_grid(ctx, ph.counts[k]);
+      const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], (int64_t) ctx->nsm * 8))
+                           : warp ? warp_grid(ctx, ph.counts[k]) : fill_grid(ctx, ph.counts[k]);
       FillParams P;
       P.pairs = d_pairs; P.arena = d_arena;
       P.list = pd.lists.as<int32_t>() + ph.start[k];
@@ -731,7 +820,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
         compact_rerun_kernel<<<cg, 256, 0, s>>>(P.list, P.count, pd.meta.as<gdp_meta_t>(),
                                                 pd.work.as<int32_t>() + ph.start[k],
                                                 pd.work_counts.as<int32_t>() + k);
-        prof_end(ctx, 27, evc);
+        prof_end(ctx, PROF_RERUN, evc);
         ctx->launches++;
         CK(ctx, cudaGetLastError());
         P.list = pd.work.as<int32_t>() + ph.start[k];
@@ -747,7 +836,9 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.tab = ctx->d_tab;
       cudaEvent_t ev = nullptr;
       prof_begin(ctx, &ev);
-      launch_kind(k, P, grid, s);
+      if (cta) launch_cta_kind(k, P, grid, s);
+      else if (warp) launch_warp_kind(k, P, grid, s);
+      else launch_kind(k, P, grid, s);
       prof_end(ctx, k, ev);
       ctx->launches++;
       CK(ctx, cudaGetLastError());
@@ -766,7 +857,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     cudaEvent_t ev = nullptr;
     prof_begin(ctx, &ev);
     traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, s>>>(T);
-    prof_end(ctx, 24, ev);
+    prof_end(ctx, PROF_TB, ev);
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
@@ -795,7 +886,7 @@ compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_
   const int grid = (int) std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t) ctx->nsm * 16));
   compact_records_kernel<<<grid, 256, 0, s>>>(d_res, pd.rec_off.as<int64_t>(), d_slots,
                                               pd.nrec_scan.as<int64_t>(), n, out, pd.total.as<int64_t>());
-  prof_end(ctx, 28, ev);
+  prof_end(ctx, PROF_RECS, ev);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   return GDP_OK;

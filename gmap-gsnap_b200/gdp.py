@@ -208,7 +208,7 @@ class Context:
         """{kernel name: (total ms, launches)} since the last reset."""
         out = {}
         name = ctypes.create_string_buffer(64)
-        for k in range(28):
+        for k in range(64):
             ms, n = ctypes.c_double(0), ctypes.c_int64(0)
             self.lib.gdp_profile_read(self.h, k, name, 64, ctypes.byref(ms), ctypes.byref(n))
             if n.value:

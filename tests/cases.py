@@ -51,7 +51,7 @@ def _mutate(rng, src, sub, indel):
 
 
 def random_cases(seed, n, variants=(0, 1, 2), precisions=(8, 16), max_len=90,
-                 genome_len=1 << 16, exotic=True):
+                 genome_len=1 << 16, exotic=True, min_len=1, extras=(0, 1, 2, 3, 5, 8, 13, 20, 31, 40)):
     """Returns (pairs, arena) with n random cases."""
     rng = np.random.default_rng(seed)
     pairs = np.zeros(n, dtype=gdp.PAIR_DTYPE)
@@ -60,11 +60,12 @@ def random_cases(seed, n, variants=(0, 1, 2), precisions=(8, 16), max_len=90,
     for i in range(n):
         variant = int(rng.choice(variants))
         prec = int(rng.choice(precisions))
-        rl = int(rng.integers(1, max_len + 1))
+        rl = int(rng.integers(min_len, max_len + 1))
         kind = rng.random()
         base = _seq(rng, rl, exotic and rng.random() < 0.3)
         if kind < 0.15:
-            gseq = _seq(rng, int(rng.integers(1, max_len + 1)), exotic and rng.random() < 0.3)  # unrelated
+            gseq = _seq(rng, max(1, rl + int(rng.integers(-rl // 8 - 1, rl // 8 + 2))),
+                        exotic and rng.random() < 0.3)  # unrelated
         else:
             gseq = _mutate(rng, base, rng.choice([0.0, 0.02, 0.1, 0.3]), rng.choice([0.0, 0.02, 0.08]))
         gl = len(gseq)
@@ -83,7 +84,7 @@ def random_cases(seed, n, variants=(0, 1, 2), precisions=(8, 16), max_len=90,
             galt[m] = rng.choice(np.frombuffer(ACGT, np.uint8), size=int(m.sum()))
         ruc = np.array([c - 32 if 97 <= c <= 122 else c for c in base], dtype=np.uint8)
         # bands: keep (rl, gl) inside the band, as Dynprog_compute_bands does
-        extra = int(rng.choice([0, 1, 2, 3, 5, 8, 13, 20, 31, 40]))
+        extra = int(rng.choice(list(extras)))
         if variant == 0:
             lb = max(0, rl - gl) + int(rng.integers(0, extra + 1))
             ub = max(0, gl - rl) + int(rng.integers(0, extra + 1))

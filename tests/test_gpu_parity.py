@@ -56,6 +56,44 @@ def test_traceback_random(env, seed):
     assert not fails, "\n".join(fails)
 
 
+@pytest.mark.parametrize("seed,variants", [(301, (0,)), (302, (1,)), (303, (2,))])
+def test_long_pairs_one_warp_per_pair(env, seed, variants):
+    """Pairs with at least 512 lanes and a sweep of at most 496 columns per
+    block run one warp per pair (lane l owns blocks l, l+32, ...); they must
+    be bit-exact like the one-thread-per-pair fills."""
+    ctx, ref, rest = env
+    pairs, arena = cases.random_cases(seed, 10, variants=variants, precisions=(16,), min_len=530,
+                                      max_len=1400, extras=(0, 3, 10, 40, 90))
+    ctx.profile(True)
+    ctx.profile_reset()
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+    kernels = ctx.profile_read()
+    ctx.profile(False)
+    assert any(k.startswith("fill_warp") for k in kernels), kernels
+
+
+@pytest.mark.parametrize("seed,variants", [(311, (0,)), (312, (1,)), (313, (2,))])
+def test_wide_bands_one_cta_per_pair(env, seed, variants):
+    """Long pairs whose blocks sweep more columns than one warp can pipeline
+    run one CTA per pair (2 to 16 warps, shared-memory hand-off between
+    warps); bit-exact like the other fills."""
+    ctx, ref, rest = env
+    pairs, arena = cases.random_cases(seed, 5, variants=variants, precisions=(16,), min_len=520,
+                                      max_len=900, extras=(500, 700))
+    ctx.profile(True)
+    ctx.profile_reset()
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+    kernels = ctx.profile_read()
+    ctx.profile(False)
+    assert any(k.startswith("fill_cta") for k in kernels), kernels
+
+
 def test_rerun_contract(env, gdplib):
     """8-bit pairs with the 16-bit rerun: the kept precision follows the
     overflow rule, and the kept outputs are bit-exact with that precision."""
