@@ -82,7 +82,15 @@ def test_wide_bands_one_cta_per_pair(env, seed, variants):
     warps); bit-exact like the other fills."""
     ctx, ref, rest = env
     pairs, arena = cases.random_cases(seed, 5, variants=variants, precisions=(16,), min_len=520,
-                                      max_len=900, extras=(500, 700))
+                                      max_len=900, extras=(0, 40))
+    # widen the band past what one warp can pipeline (sweep > 496 columns per block)
+    if variants[0] == 0:
+        pairs["lband"] += 260
+        pairs["uband"] += 300
+    elif variants[0] == 1:
+        pairs["uband"] += 560
+    else:
+        pairs["lband"] += 560
     ctx.profile(True)
     ctx.profile_reset()
     fails = parity.check_fill(ctx, ref, pairs, arena)
