@@ -50,6 +50,14 @@ typedef struct gdp_tables {
 extern "C"
 #endif
 void gdp_build_tables(gdp_tables_t *t, int mode);
+#ifdef __cplusplus
+extern "C"
+#endif
+void gdp_tables_derive(gdp_tables_t *t);   /* class profiles from pd */
+#ifdef __cplusplus
+extern "C"
+#endif
+void gdp_workload_genomecomp(const char *genome, int64_t n, uint32_t *blocks);   /* workload.c */
 
 /* Geometry of a pair in lane/sweep terms. */
 typedef struct gdp_geom {

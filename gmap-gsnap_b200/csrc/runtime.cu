@@ -852,6 +852,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     T.dirs = pd.dirs.as<uint32_t>(); T.meta = pd.meta.as<gdp_meta_t>(); T.res = d_res; T.recs = d_slots;
     T.rec_off = pd.rec_off.as<int64_t>();
     T.genome = ctx->d_genome; T.genomealt = ctx->d_genomealt;
+    T.genome_base = 0;
     T.genome_len = ctx->genome_len;
     T.tab = ctx->d_tab;
     cudaEvent_t ev = nullptr;
@@ -1107,4 +1108,146 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
   dpairs.release();
   dres.release();
   return rc;
+}
+
+/* ------------------------------------------------------------------ */
+/* Single-pair fill and traceback for the reference-signature entry    */
+/* points (dropin.cu)                                                  */
+/* ------------------------------------------------------------------ */
+
+#include "gdp_dropin_internal.h"
+
+struct gdpi_fill {
+  gdp_pair_t pair;
+  gdp_plan pl;
+  DevBuf dpairs, darena, dres, dlist, drecs, drecoff, dgenome, dgenomealt;
+  std::vector<uint32_t> words;     /* host copy of the pair's direction words */
+  std::vector<int16_t> scores;     /* host copy of the swept cells' scores (8 per word) */
+  gdp_result_t res;
+  gdp_meta_t meta;
+};
+
+gdpi_fill *gdpi_fill_new () { return new gdpi_fill(); }
+
+int
+gdpi_fill_run (gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const char *arena, int64_t arena_bytes) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  f->pair = *p;
+  f->pair.flags &= ~GDP_FLAG_TRACEBACK;
+  f->res.status = GDP_ERR_PARAM;
+  cudaStream_t s = ctx->stream;
+  int rc = plan_build(ctx, &f->pair, 1, arena_bytes, f->pl.h);
+  if (rc == GDP_OK) rc = plan_upload(ctx, f->pl.h, f->pl.d, true, s);
+  if (rc == GDP_OK) {
+    cudaError_t e = f->dpairs.ensure(sizeof(gdp_pair_t));
+    if (e == cudaSuccess) e = f->darena.ensure(std::max<int64_t>(arena_bytes, 16));
+    if (e == cudaSuccess) e = f->dres.ensure(sizeof(gdp_result_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f->dpairs.p, &f->pair, sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f->darena.p, arena, arena_bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) rc = set_err(ctx, "single-pair staging", e);
+  }
+  if (rc == GDP_OK)
+    rc = plan_run(ctx, f->pl.h, f->pl.d, f->dpairs.as<gdp_pair_t>(), f->darena.as<char>(), f->dres.as<gdp_result_t>(), nullptr);
+  if (rc == GDP_OK) {
+    const int64_t nw = std::max<int64_t>(f->pl.h.dir_words, 1);
+    if ((int64_t) f->words.size() < nw) f->words.resize(nw);
+    if ((int64_t) f->scores.size() < nw * 8) f->scores.resize(nw * 8);
+    cudaError_t e = cudaMemcpyAsync(&f->res, f->dres.p, sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&f->meta, f->pl.d.meta.p, sizeof(gdp_meta_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && f->pl.h.dir_words > 0)
+      e = cudaMemcpyAsync(f->words.data(), f->pl.d.dirs.p, f->pl.h.dir_words * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && f->pl.h.dir_words > 0)
+      e = cudaMemcpyAsync(f->scores.data(), f->pl.d.hdump.p, f->pl.h.dir_words * 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = set_err(ctx, "single-pair results", e);
+  }
+  if (rc != GDP_OK) f->res.status = rc;
+  return rc;
+}
+
+const uint32_t *gdpi_fill_words (const gdpi_fill *f) { return f->words.data(); }
+const int16_t *gdpi_fill_scores (const gdpi_fill *f) { return f->scores.data(); }
+int gdpi_fill_width (const gdpi_fill *f) { return f->res.precision == 8 ? 32 : 16; }
+int64_t gdpi_fill_base (const gdpi_fill *f) { return f->res.precision == 8 ? f->meta.dir8 : f->meta.dir16; }
+const gdp_result_t *gdpi_fill_result (const gdpi_fill *f) { return &f->res; }
+const gdp_pair_t *gdpi_fill_pair (const gdpi_fill *f) { return &f->pair; }
+
+int
+gdpi_traceback_one (gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const char *arena, int64_t arena_bytes,
+                    const uint32_t *gblocks, const uint32_t *galtblocks, uint64_t gbase, uint64_t glen,
+                    gdp_result_t *res, std::vector<gdp_rec_t> *recs) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const int64_t cap = (int64_t) p->rlength + p->glength + 2;
+  const size_t gwords = (size_t) ((glen + 31) / 32) * 3;
+  const int32_t one[2] = {0, 1};
+  const int64_t zero = 0;
+  if (f->res.status != GDP_OK) return GDP_ERR_PARAM;   /* no usable fill behind this traceback */
+  gdp_pair_t q = *p;
+  q.flags |= GDP_FLAG_TRACEBACK;
+  CK(ctx, f->dpairs.ensure(sizeof(gdp_pair_t)));
+  CK(ctx, f->darena.ensure(std::max<int64_t>(arena_bytes, 16)));
+  CK(ctx, f->dlist.ensure(2 * sizeof(int32_t)));
+  CK(ctx, f->drecs.ensure(cap * sizeof(gdp_rec_t)));
+  CK(ctx, f->drecoff.ensure(sizeof(int64_t)));
+  CK(ctx, cudaMemcpyAsync(f->dpairs.p, &q, sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(f->darena.p, arena, arena_bytes, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(f->dlist.p, one, sizeof(one), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(f->drecoff.p, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(f->dres.p, &f->res, sizeof(gdp_result_t), cudaMemcpyHostToDevice, s));
+  if (gblocks && gwords > 0) {
+    CK(ctx, f->dgenome.ensure(gwords * 4));
+    CK(ctx, f->dgenomealt.ensure(gwords * 4));
+    CK(ctx, cudaMemcpyAsync(f->dgenome.p, gblocks, gwords * 4, cudaMemcpyHostToDevice, s));
+    CK(ctx, cudaMemcpyAsync(f->dgenomealt.p, galtblocks ? galtblocks : gblocks, gwords * 4, cudaMemcpyHostToDevice, s));
+  }
+  TbParams T;
+  T.pairs = f->dpairs.as<gdp_pair_t>();
+  T.arena = f->darena.as<char>();
+  T.list = f->dlist.as<int32_t>();
+  T.count = f->dlist.as<int32_t>() + 1;
+  T.dirs = f->pl.d.dirs.as<uint32_t>();
+  T.meta = f->pl.d.meta.as<gdp_meta_t>();
+  T.res = f->dres.as<gdp_result_t>();
+  T.recs = f->drecs.as<gdp_rec_t>();
+  T.rec_off = f->drecoff.as<int64_t>();
+  T.genome = (gblocks && gwords > 0) ? f->dgenome.as<uint32_t>() : nullptr;
+  T.genomealt = (gblocks && gwords > 0) ? f->dgenomealt.as<uint32_t>() : nullptr;
+  T.genome_base = gbase;
+  T.genome_len = glen;
+  T.tab = ctx->d_tab;
+  traceback_kernel<<<1, 32, 0, s>>>(T);
+  ctx->launches++;
+  CK(ctx, cudaGetLastError());
+  CK(ctx, cudaMemcpyAsync(res, f->dres.p, sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  recs->resize(std::max(res->nrecs, 0));
+  if (res->nrecs > 0) {
+    CK(ctx, cudaMemcpy(recs->data(), f->drecs.p, res->nrecs * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost));
+  }
+  return GDP_OK;
+}
+
+void
+gdpi_fill_free (gdpi_fill *f) {
+  if (!f) return;
+  f->pl.d.release();
+  f->pl.h.release();
+  f->dpairs.release(); f->darena.release(); f->dres.release(); f->dlist.release();
+  f->drecs.release(); f->drecoff.release(); f->dgenome.release(); f->dgenomealt.release();
+  delete f;
+}
+
+/* Replaces the context's substitution / consistency tables with the
+   caller's own (a GMAP process that ran Dynprog_init). */
+int
+gdpi_set_tables (gdp_ctx *ctx, const gdp_tables_t *t) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  memcpy(ctx->h_tab, t, sizeof(gdp_tables_t));
+  CK(ctx, cudaMemcpyAsync(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GDP_OK;
 }

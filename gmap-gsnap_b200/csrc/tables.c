@@ -48,6 +48,26 @@ pack4 (int a, int b, int c, int d) {
          ((uint32_t) (uint8_t) c << 16) | ((uint32_t) (uint8_t) d << 24);
 }
 
+/* The packed class profiles the fill kernels read, from pd. */
+void
+gdp_tables_derive (gdp_tables_t *t) {
+  static const char ACGTN[5] = {'A', 'C', 'G', 'T', 'N'};
+  int c1, mt;
+  for (mt = 0; mt < 4; mt++) {
+    for (c1 = 0; c1 < 128; c1++) {
+      int k, q[5], g[5];
+      for (k = 0; k < 5; k++) {
+        q[k] = t->pd[mt][c1][(int) ACGTN[k]];
+        g[k] = t->pd[mt][(int) ACGTN[k]][c1];
+      }
+      t->profq_lo[mt][c1] = pack4(q[0], q[1], q[2], q[3]);
+      t->profq_hi[mt][c1] = pack4(q[4], 0, 0, 0);
+      t->profg_lo[mt][c1] = pack4(g[0], g[1], g[2], g[3]);
+      t->profg_hi[mt][c1] = pack4(g[4], 0, 0, 0);
+    }
+  }
+}
+
 void
 gdp_build_tables (gdp_tables_t *t, int mode) {
   static const int mismatch[4] = {-3, -2, -1, -5};
@@ -57,8 +77,7 @@ gdp_build_tables (gdp_tables_t *t, int mode) {
                                   {'V','G'},{'V','A'},{'V','C'},{'D','G'},{'D','A'},{'D','T'},
                                   {'N','T'},{'N','C'},{'N','A'},{'N','G'},
                                   {'X','T'},{'X','C'},{'X','A'},{'X','G'},{'N','N'},{'X','X'}};
-  static const char ACGTN[5] = {'A', 'C', 'G', 'T', 'N'};
-  int c1, c2, i, mt;
+  int c1, c2, i;
   memset(t, 0, sizeof(*t));
   for (i = 0; i < 128; i++) t->nt2int[i] = 4;
   t->nt2int['A'] = t->nt2int['a'] = 0;
@@ -81,17 +100,5 @@ gdp_build_tables (gdp_tables_t *t, int mode) {
   case 6: mark(t, 'C', 'T', 3, mode, 1, 1); mark(t, 'G', 'A', 3, mode, 1, 2); break;  /* TTOC_NONSTRANDED */
   default: break;
   }
-  for (mt = 0; mt < 4; mt++) {
-    for (c1 = 0; c1 < 128; c1++) {
-      int k, q[5], g[5];
-      for (k = 0; k < 5; k++) {
-        q[k] = t->pd[mt][c1][(int) ACGTN[k]];
-        g[k] = t->pd[mt][(int) ACGTN[k]][c1];
-      }
-      t->profq_lo[mt][c1] = pack4(q[0], q[1], q[2], q[3]);
-      t->profq_hi[mt][c1] = pack4(q[4], 0, 0, 0);
-      t->profg_lo[mt][c1] = pack4(g[0], g[1], g[2], g[3]);
-      t->profg_hi[mt][c1] = pack4(g[4], 0, 0, 0);
-    }
-  }
+  gdp_tables_derive(t);
 }

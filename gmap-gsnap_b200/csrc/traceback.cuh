@@ -30,6 +30,7 @@ struct TbParams {
   gdp_rec_t *recs;
   const int64_t *rec_off;
   const uint32_t *genome, *genomealt;   /* genomecomp blocks, may be NULL */
+  uint64_t genome_base;                  /* absolute position of the blocks' first nt */
   uint64_t genome_len;
   const gdp_tables_t *tab;
 };
@@ -101,7 +102,7 @@ struct TbState {
   int score, nmatch, nmismatch, nopen, nindel;
   int err;
   const uint32_t *genome, *genomealt;
-  uint64_t genome_len;
+  uint64_t genome_base, genome_len;
   const gdp_tables_t *tab;
 
   __device__ void push (int qpos, int gpos, char cdna, char comp, char g, char ga) {
@@ -134,16 +135,18 @@ struct TbState {
     if (p->watsonp) {
       pos = p->chroffset + (uint32_t) gp;
       if (pos < p->chroffset || pos >= p->chrhigh) { *alt = '*'; return '*'; }
-      if (pos >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
-      const char c = gnt_decode(genome, pos, true);
-      *alt = (c == 'N') ? c : gnt_decode(genomealt, pos, false);
+      if (pos < genome_base || pos - genome_base >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
+      const uint32_t rp = (uint32_t) (pos - genome_base);
+      const char c = gnt_decode(genome, rp, true);
+      *alt = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
       return c;
     }
     pos = p->chrhigh - (uint32_t) gp;
     if (pos < p->chroffset || pos >= p->chrhigh) { *alt = '*'; return '*'; }
-    if (pos >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
-    const char c = gnt_decode(genome, pos, true);
-    const char ca = (c == 'N') ? c : gnt_decode(genomealt, pos, false);
+    if (pos < genome_base || pos - genome_base >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
+    const uint32_t rp = (uint32_t) (pos - genome_base);
+    const char c = gnt_decode(genome, rp, true);
+    const char ca = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
     *alt = gnt_compl(ca);
     return gnt_compl(c);
   }
@@ -309,6 +312,7 @@ traceback_kernel (TbParams P) {
     T.out = P.recs + P.rec_off[pi];
     T.cap = (int64_t) p.rlength + p.glength + 2;
     T.genome = P.genome; T.genomealt = P.genomealt ? P.genomealt : P.genome;
+    T.genome_base = P.genome_base;
     T.genome_len = P.genome_len;
     T.tab = P.tab;
     for (int attempt = 0; attempt < 2; attempt++) {

@@ -6,6 +6,12 @@ Two CPU oracles with one interface:
   * Restatement: oracle/liboracle.so, this repository's plain-C restatement
     of the same algorithm (oracle/gdp_oracle.c), pinned against the first.
 
+A third library with the same interface hosts the product instead of
+checking it: oracle/_ref/libgmapenv.so is GMAP's own list / pairpool /
+dynprog code with src/dynprog_simd.c removed, so its Dynprog_simd_* and
+Dynprog_traceback_* calls land in the product's reference-signature entry
+points (libgdp.so).  Tests compare it against the reference library.
+
 Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline / reference
 arm import this module, and only as the checker or the timed CPU baseline.
 """
@@ -17,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libgdpref.so")
 REF_LIB_NOFLUSH = os.path.join(HERE, "_ref", "libgdpref_noflush.so")
+GMAPENV_LIB = os.path.join(HERE, "_ref", "libgmapenv.so")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 
 
@@ -27,11 +34,11 @@ def _ptr(a):
 class CpuOracle:
     """Wraps libgdpref.so (prefix 'ref_') or liboracle.so (prefix 'orc_')."""
 
-    def __init__(self, path, prefix):
+    def __init__(self, path, prefix, mode=ctypes.DEFAULT_MODE):
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.path = path
-        self.lib = ctypes.CDLL(path)
+        self.lib = ctypes.CDLL(path, mode=mode)
         vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
         self._init = getattr(self.lib, prefix + "init")
         self._init.argtypes = [i32]
@@ -104,6 +111,18 @@ def restatement():
 
 def reference_available():
     return os.path.exists(REF_LIB)
+
+
+def gmap_environment():
+    """GMAP's host code around the product's reference-signature entry
+    points.  Loaded into the global symbol scope, so that libgdp.so finds
+    GMAP's Pairpool_push, Genome_get_char and tables there; load it before
+    any other library that defines those names."""
+    return CpuOracle(GMAPENV_LIB, "ref_", mode=ctypes.RTLD_GLOBAL)
+
+
+def gmap_environment_available():
+    return os.path.exists(GMAPENV_LIB)
 
 
 def domain_mask(variant, rlength, glength, lband, uband):

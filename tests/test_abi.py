@@ -1,5 +1,6 @@
 """C-ABI checks that need no GPU: libgdp.so loads, exports every function
-include/gdp.h declares, and its host-side helpers behave."""
+include/gdp.h and include/gdp_dynprog_simd.h declare, and its host-side
+helpers behave."""
 import os
 import re
 import subprocess
@@ -25,7 +26,11 @@ def _exported(path):
 
 def test_library_exports_every_declared_symbol(gdplib):
     exported = _exported(gdp.LIB_PATH)
-    missing = [n for n in _declared("gdp.h") if n not in exported]
+    headers = sorted(h for h in os.listdir(os.path.join(ROOT, "include")) if h.endswith(".h"))
+    assert "gdp.h" in headers and "gdp_dynprog_simd.h" in headers
+    declared = [n for h in headers for n in _declared(h)]
+    assert sum(n.startswith("Dynprog_") for n in declared) == 12
+    missing = [n for n in declared if n not in exported]
     assert not missing, missing
 
 
