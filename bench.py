@@ -167,6 +167,106 @@ def cpu_baseline(lib, name, seed, target_seconds, threads=None):
                       f"{secs:.2f} s wall on {threads} threads", "seconds": secs, "pairs": n, "cells": cells}
 
 
+def per_pair_vs_batched(lib, ctx, seed, npairs=20000, nsample=500):
+    """The same mixed-length pairs (70/25/5 short/long/cDNA) aligned as one
+    batch and as one plan per pair (every pair its own kernel launches),
+    both device-resident, timed with CUDA events on the context's stream."""
+    import torch
+    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+    pairs, arena = gdp.make_pairs(lib, gdp.WL_MIX, seed, genome, npairs)
+    ctx.set_genome(blocks, None, genome.size)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    d_arena = torch.from_numpy(arena).cuda()
+    d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    plan = ctypes.c_void_p()
+    assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan)) == 0, ctx.error()
+    d_recs = torch.empty(max(int(lib.gdp_plan_total_recs(plan)), 1) * gdp.REC_DTYPE.itemsize, dtype=torch.uint8,
+                         device="cuda")
+    batch_ms = timed(lambda: lib.gdp_plan_execute(ctx.h, plan, ctypes.c_void_p(d_pairs.data_ptr()),
+                                                  ctypes.c_void_p(d_arena.data_ptr()),
+                                                  ctypes.c_void_p(d_res.data_ptr()),
+                                                  ctypes.c_void_p(d_recs.data_ptr())), 2)
+    batch_res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE).copy()
+    lib.gdp_plan_destroy(plan)
+    cells = gdp.band_cells(pairs)
+
+    sample = np.arange(min(nsample, pairs.size))
+    plans, offs, tot = [], [], 0
+    for i in sample:
+        pl = ctypes.c_void_p()
+        assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs[i:i + 1]), 1, ctypes.byref(pl)) == 0, ctx.error()
+        plans.append(pl)
+        offs.append(tot)
+        tot += max(int(lib.gdp_plan_total_recs(pl)), 1)
+    d_recs1 = torch.empty(tot * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    pb, ab, rb, cb = d_pairs.data_ptr(), d_arena.data_ptr(), d_res.data_ptr(), d_recs1.data_ptr()
+
+    def one_by_one():
+        for k, i in enumerate(sample):
+            lib.gdp_plan_execute(ctx.h, plans[k], ctypes.c_void_p(pb + int(i) * gdp.PAIR_DTYPE.itemsize),
+                                 ctypes.c_void_p(ab), ctypes.c_void_p(rb + int(i) * gdp.RESULT_DTYPE.itemsize),
+                                 ctypes.c_void_p(cb + offs[k] * gdp.REC_DTYPE.itemsize))
+
+    pair_ms = timed(one_by_one, 1)
+    one_res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+    for pl in plans:
+        lib.gdp_plan_destroy(pl)
+    same = all(np.array_equal(one_res[k][sample], batch_res[k][sample])
+               for k in ("status", "score", "tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs"))
+    batched = float(cells.sum()) / (batch_ms * 1e-3) / 1e9
+    per_pair = float(cells[sample].sum()) / (pair_ms * 1e-3) / 1e9
+    return {"workload": f"mix 70/25/5 short/long/cDNA, {pairs.size} pairs ({int(cells.sum())} cells)",
+            "batched_gcups": round(batched, 3), "per_pair_gcups": round(per_pair, 3),
+            "per_pair_sample": f"first {sample.size} of the same pairs, one plan (own launches) per pair",
+            "ratio": round(batched / per_pair, 2),
+            "batched_alignments_per_s": round(pairs.size / (batch_ms * 1e-3), 1),
+            "per_pair_alignments_per_s": round(sample.size / (pair_ms * 1e-3), 1),
+            "results_identical": bool(same)}
+
+
+def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000):
+    """The serving loop under Poisson load: single-pair requests of the
+    mixed distribution, genome windows extracted on the device from a
+    resident 100 Mbp genome, admission by a 40 GB direction budget."""
+    genome, blocks = gdp.make_genome(lib, 4242, 100_000_000)
+    pool, arena = gdp.make_resident_pairs(lib, gdp.WL_MIX, seed, genome, pool_size)
+    cells = gdp.band_cells(pool)
+    srv = gdp.Server(lib, device=device, workers=2, budget=40 << 30, blocks=blocks, length=genome.size)
+    srv.drive(pool, arena, 100_000, rate=1e6, seed=1)       # warm-up: buffers reach their working sizes
+    rows = []
+    for k, rate in enumerate(rates):
+        n = int(min(max_requests, max(200, rate * seconds_per_rate)))
+        lat, elapsed, _ = srv.drive(pool, arena, n, rate=rate, seed=100 + k)
+        served = cells[np.arange(n) % pool.size].sum()
+        rows.append({"offered_per_s": rate, "requests": n,
+                     "sustained_per_s": round(n / elapsed, 1),
+                     "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                     "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                     "gcups": round(float(served) / elapsed / 1e9, 2)})
+    st = srv.stats()
+    srv.close()
+    knee = max((r["offered_per_s"] for r in rows if r["sustained_per_s"] >= 0.95 * r["offered_per_s"]),
+               default=None)
+    return {"genome": "100 Mbp seeded random, resident (genomecomp, 2-bit + N flags)",
+            "requests": "single pairs of the 70/25/5 short/long/cDNA mix, device-extracted windows",
+            "workers": 2, "dir_budget_gb": 40, "sweep": rows, "knee_offered_per_s": knee,
+            "batches": st["batches"], "max_batch_pairs": st["max_batch_pairs"],
+            "peak_admitted_dir_gb": round(st["peak_reserved_bytes"] / 2**30, 3)}
+
+
 def run_reference_arm(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
@@ -316,6 +416,12 @@ def run_gdp(args):
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     lib.gdp_plan_destroy(plan)
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_per_pair:
+        extra["per_pair_vs_batched"] = per_pair_vs_batched(lib, ctx, args.seed + 7)
+    if rank == 0 and world == 1 and not args.no_serving:
+        extra["serving"] = serving_sweep(lib, local, args.seed + 8,
+                                         [1e3, 1e4, 5e4, 1e5, 2e5, 3e5, 5e5, 1e6])
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm = None
     if os.path.exists(peaks_path):
@@ -349,6 +455,7 @@ def run_gdp(args):
             "bad_status_pairs": bad,
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
@@ -368,6 +475,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-pair", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

@@ -352,7 +352,10 @@ stage_genome_window (DropinThread &t, const gdp_pair_t &p, Genome_T genome, Geno
   const bool revp = (p.flags & GDP_FLAG_REVP) != 0;
   const int gl = p.glength;
   uint64_t lo = UINT64_MAX, hi = 0;
-  for (int k = 0; k < gl; k++) {
+  /* genome skips address coordinates c - dist .. c - 1; the E walk that
+     reaches column 0 leaves them one past the window (src/dynprog_simd.c:9174),
+     so a margin of two on either side covers every reachable position */
+  for (int k = -2; k < gl + 2; k++) {
     const int gp = p.genomeoffset + (revp ? -k : k);
     const uint32_t pos = p.watsonp ? p.chroffset + (uint32_t) gp : p.chrhigh - (uint32_t) gp;
     if (pos < p.chroffset || pos >= p.chrhigh) continue;

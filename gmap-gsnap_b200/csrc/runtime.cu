@@ -53,7 +53,8 @@ struct DevBuf {
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
-    size_t grow = want + want / 4 + 4096;
+    /* grow geometrically: a buffer that keeps growing is reallocated rarely */
+    size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     cudaError_t e = cudaMalloc(&p, grow);
     if (e == cudaSuccess) bytes = grow;
     return e;
@@ -70,7 +71,8 @@ struct HostBuf {   /* pinned host memory */
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    size_t grow = want + want / 4 + 4096;
+    /* grow geometrically: a buffer that keeps growing is reallocated rarely */
+    size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     cudaError_t e = cudaHostAlloc(&p, grow, cudaHostAllocDefault);
     if (e == cudaSuccess) bytes = grow;
     return e;
@@ -109,6 +111,7 @@ struct PlanHost {
   int32_t counts[NKINDS + 1] = {0};
   int maxY[NKINDS] = {0};
   int64_t dir_words = 0, total_recs = 0;
+  int64_t nwindow = 0;   /* pairs whose genome window the device extracts */
   void release () { lists.release(); meta.release(); status.release(); rec_off.release(); }
 };
 
@@ -175,7 +178,8 @@ struct gdp_ctx {
 #define PROF_PEAK (NKINDS + 2)
 #define PROF_RERUN (NKINDS + 3)
 #define PROF_RECS (NKINDS + 4)
-#define NPROF (NKINDS + 5)
+#define PROF_WINDOW (NKINDS + 5)
+#define NPROF (NKINDS + 6)
 static const char *
 kernel_name (int id) {
   static char buf[NPROF][48];
@@ -184,6 +188,7 @@ kernel_name (int id) {
   if (id == PROF_PEAK) return "int_peak_kernel";
   if (id == PROF_RERUN) return "compact_rerun_kernel";
   if (id == PROF_RECS) return "compact_records_kernel";
+  if (id == PROF_WINDOW) return "window_kernel";
   if (id >= NTHREADKINDS + NWARPKINDS) {
     const int c = id - NTHREADKINDS - NWARPKINDS, vl = c / 4, variant = vl / 2, late = vl & 1;
     snprintf(buf[id], sizeof(buf[id]), "fill_cta<W16,%s,%s,%dwarps>",
@@ -467,7 +472,7 @@ gdp_set_genome (gdp_ctx *ctx, const uint32_t *blocks, const uint32_t *altblocks,
 /* ------------------------------------------------------------------ */
 
 static int
-validate (const gdp_pair_t &p, int64_t arena_bytes) {
+validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   if (p.variant < GDP_FULL || p.variant > GDP_LOWER) return GDP_ERR_PARAM;
   if (p.precision != 8 && p.precision != 16) return GDP_ERR_PARAM;
   if (p.mismatchtype < 0 || p.mismatchtype > 3) return GDP_ERR_PARAM;
@@ -482,6 +487,17 @@ validate (const gdp_pair_t &p, int64_t arena_bytes) {
   }
   if (p.flags & GDP_FLAG_TRACEBACK) {
     if (p.tb_r < 0 || p.tb_c < 0 || p.tb_r > p.rlength || p.tb_c > p.glength) return GDP_ERR_BAND;
+  }
+  if (p.flags & GDP_FLAG_GWINDOW) {
+    /* the window's positions inside [chroffset, chrhigh) must be resident */
+    const int64_t g0 = (p.flags & GDP_FLAG_REVP) ? (int64_t) p.genomeoffset - (p.glength - 1) : p.genomeoffset;
+    const int64_t g1 = g0 + p.glength - 1;
+    int64_t lo, hi;
+    if (p.watsonp) { lo = (int64_t) p.chroffset + g0; hi = (int64_t) p.chroffset + g1; }
+    else { lo = (int64_t) p.chrhigh - g1; hi = (int64_t) p.chrhigh - g0; }
+    lo = std::max<int64_t>(lo, p.chroffset);
+    hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
+    if (genome_len == 0 || (lo <= hi && (uint64_t) hi >= genome_len)) return GDP_ERR_NOGENOME;
   }
   return GDP_OK;
 }
@@ -524,7 +540,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   /* counting sort by (kind, work bucket) */
   std::vector<int64_t> cnt((size_t) NKINDS * NBUCKETS, 0);
   std::vector<uint32_t> key1(n, 0xffffffffu), key2(n, 0xffffffffu);
-  int64_t words = 0, recs = 0, ntb = 0;
+  int64_t words = 0, recs = 0, ntb = 0, nwindow = 0;
   int maxY[NKINDS] = {0};
   for (int64_t i = 0; i < n; i++) {
     const gdp_pair_t &p = pairs[i];
@@ -532,7 +548,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     m.dir16 = m.dir8 = -1;
     m.maxh16 = -32768; m.status8 = 0; m.final8 = 0; m.final16 = 0;
     rec_off[i] = 0;
-    const int st = validate(p, arena_bytes);
+    const int st = validate(p, arena_bytes, ctx->genome_len);
+    if (st == GDP_OK && (p.flags & GDP_FLAG_GWINDOW)) nwindow++;
     status[i] = st;
     if (st != GDP_OK) continue;
     const int late = (p.flags & GDP_FLAG_JUMP_LATE) ? 1 : 0;
@@ -604,6 +621,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   }
   ph.dir_words = words;
   ph.total_recs = recs;
+  ph.nwindow = nwindow;
   return GDP_OK;
 }
 
@@ -791,6 +809,16 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   CK(ctx, cudaMemcpyAsync(pd.meta.p, pd.meta0.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToDevice, s));
+  if (ph.nwindow > 0) {
+    cudaEvent_t evw = nullptr;
+    prof_begin(ctx, &evw);
+    window_kernel<<<(int) std::min<int64_t>(n, (int64_t) ctx->nsm * 16), 256, 0, s>>>(
+        d_pairs, pd.status.as<int32_t>(), n, const_cast<char *>(d_arena), ctx->d_genome,
+        ctx->d_genomealt ? ctx->d_genomealt : ctx->d_genome, ctx->genome_len);
+    prof_end(ctx, PROF_WINDOW, evw);
+    ctx->launches++;
+    CK(ctx, cudaGetLastError());
+  }
   size_t need = 0;
   for (int k = 0; k < NTHREADKINDS; k++) {
     if (!ph.counts[k]) continue;

@@ -92,6 +92,55 @@ gnt_compl (char c) {
   return c == 'A' ? 'T' : c == 'C' ? 'G' : c == 'G' ? 'C' : c == 'T' ? 'A' : c;
 }
 
+/*
+ * Genome character at genomic coordinate gp of a pair, as get_genomic_nt
+ * reads it (src/pairpool.c:1015-1063): chroffset + gp on the plus strand,
+ * the complement of chrhigh - gp on the minus strand, '*' outside
+ * [chroffset, chrhigh); 32-bit unsigned coordinates.  `genome` holds
+ * genomecomp blocks starting at absolute position `base` and covering `len`
+ * nt.  Returns 0 when the position lies outside those blocks.
+ */
+__device__ __forceinline__ char
+genomic_char (const gdp_pair_t &p, int gp, const uint32_t *genome, const uint32_t *genomealt, uint64_t base,
+              uint64_t len, char *alt) {
+  const uint32_t pos = p.watsonp ? p.chroffset + (uint32_t) gp : p.chrhigh - (uint32_t) gp;
+  if (pos < p.chroffset || pos >= p.chrhigh) { *alt = '*'; return '*'; }
+  if (genome == nullptr || pos < base || pos - base >= len) { *alt = 'N'; return 0; }
+  const uint32_t rp = (uint32_t) (pos - base);
+  const char c = gnt_decode(genome, rp, true);
+  const char ca = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
+  if (p.watsonp) { *alt = ca; return c; }
+  *alt = gnt_compl(ca);
+  return gnt_compl(c);
+}
+
+/*
+ * Genome windows of the pairs flagged GDP_FLAG_GWINDOW, read from the
+ * resident genome into the arena at gseq (and gseq_alt when it differs):
+ * window character j is the genome character at genomic coordinate
+ * genomeoffset + j (revp: genomeoffset - (glength - 1) + j), the positions
+ * the traceback's genome skips address.  One block per pair.
+ */
+__global__ void __launch_bounds__(256)
+window_kernel (const gdp_pair_t *pairs, const int32_t *status, int64_t n, char *arena, const uint32_t *genome,
+               const uint32_t *genomealt, uint64_t genome_len) {
+  for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const gdp_pair_t p = pairs[i];
+    if (!(p.flags & GDP_FLAG_GWINDOW) || status[i] != GDP_OK) continue;
+    const int gl = p.glength;
+    const int g0 = (p.flags & GDP_FLAG_REVP) ? p.genomeoffset - (gl - 1) : p.genomeoffset;
+    char *w = arena + p.gseq, *wa = arena + p.gseq_alt;
+    const bool same = (p.gseq_alt == p.gseq);
+    for (int j = threadIdx.x; j < gl; j += blockDim.x) {
+      char a;
+      char c = genomic_char(p, g0 + j, genome, genomealt, 0, genome_len, &a);
+      if (c == 0) { c = 'N'; a = 'N'; }
+      w[j] = c;
+      if (!same) wa[j] = a;
+    }
+  }
+}
+
 struct TbState {
   const gdp_pair_t *p;
   const char *rseq, *ruc, *gseq, *galt;   /* reference-convention pointers (revp: last char) */
@@ -128,27 +177,11 @@ struct TbState {
     }
     n++;
   }
-  /* get_genomic_nt (src/pairpool.c:1015-1063); coordinates are 32-bit unsigned */
+  /* get_genomic_nt (src/pairpool.c:1015-1063) */
   __device__ char genomic_nt (char *alt, int gp) {
-    if (genome == nullptr) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
-    uint32_t pos;
-    if (p->watsonp) {
-      pos = p->chroffset + (uint32_t) gp;
-      if (pos < p->chroffset || pos >= p->chrhigh) { *alt = '*'; return '*'; }
-      if (pos < genome_base || pos - genome_base >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
-      const uint32_t rp = (uint32_t) (pos - genome_base);
-      const char c = gnt_decode(genome, rp, true);
-      *alt = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
-      return c;
-    }
-    pos = p->chrhigh - (uint32_t) gp;
-    if (pos < p->chroffset || pos >= p->chrhigh) { *alt = '*'; return '*'; }
-    if (pos < genome_base || pos - genome_base >= genome_len) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
-    const uint32_t rp = (uint32_t) (pos - genome_base);
-    const char c = gnt_decode(genome, rp, true);
-    const char ca = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
-    *alt = gnt_compl(ca);
-    return gnt_compl(c);
+    const char c = genomic_char(*p, gp, genome, genomealt, genome_base, genome_len, alt);
+    if (c == 0) { err = GDP_ERR_NOGENOME; *alt = 'N'; return 'N'; }
+    return c;
   }
   __device__ void queryskip (int r, int c, int dist) {
     int qc = r - 1, gc = c - 1, step;

@@ -289,6 +289,123 @@ make_pair (rng_t *r, int kind, const char *genome, int64_t glen_total,
 }
 
 /*
+ * One pair whose genome window is a slice of the genome, for callers that
+ * keep the genome resident on the device (GDP_FLAG_GWINDOW): the window is
+ * genome[pos, pos + glength), written to the arena as well, and the read is
+ * its mutated copy, its length clamped so that (rlength, glength) stays in
+ * the band.  Same length, band and mutation distributions as make_pair.
+ */
+static int64_t
+make_pair_resident (rng_t *r, int kind, const char *genome, int64_t glen_total,
+                    gdp_pair_t *p, char *arena, int64_t off, int64_t cap) {
+  int glength, rlength, lband, uband, prec = 16, flags, n, lo, hi;
+  int random_window = 0;
+  int64_t pos, used;
+  mut_t m;
+  char *w, *q, *tmp;
+  if (kind == WL_CDNA) {
+    /* its window is already a genome slice */
+    used = make_pair(r, kind, genome, glen_total, p, arena, off, cap);
+    if (used >= 0) p->flags = (int8_t) (p->flags | GDP_FLAG_GWINDOW);
+    return used;
+  }
+  memset(p, 0, sizeof(*p));
+  flags = GDP_FLAG_JUMP_LATE | GDP_FLAG_TRACEBACK | GDP_FLAG_GWINDOW;
+  switch (kind) {
+  case WL_FIXED:
+    glength = 160; lband = uband = 10; m.sub = 0.02; m.indel = 0.005; m.geom_mean = 0;
+    break;
+  case WL_SHORT:
+    glength = rng_int(r, 75, 300); lband = rng_int(r, 3, 30); uband = rng_int(r, 3, 30);
+    m.sub = 0.03; m.indel = 0.01; m.geom_mean = 0; prec = 8; flags |= GDP_FLAG_RERUN16;
+    random_window = rng_unif(r) < 0.05;
+    break;
+  case WL_LONG:
+  default:
+    glength = rng_int(r, 1000, 10000); lband = rng_int(r, 50, 200); uband = rng_int(r, 50, 200);
+    m.sub = 0.03; m.indel = 0.01; m.geom_mean = 0;
+    break;
+  }
+  /* the read length range that keeps (rlength, glength) in the band */
+  lo = glength - uband; hi = glength + lband;
+  if (kind == WL_FIXED) lo = hi = 150;
+  if (lo < 1) lo = 1;
+  if (off + (int64_t) glength + 2 * (int64_t) hi + 4096 > cap) return -1;
+  pos = (int64_t) (rng_next(r) % (uint64_t) (glen_total - 2 * (glength + hi + 512)));
+  w = arena + off;
+  memcpy(w, genome + pos, glength);
+  q = w + glength + 64;
+  tmp = (char *) malloc((size_t) hi * 2 + (size_t) glength * 2 + 128);
+  if (random_window) {
+    int64_t p2 = (int64_t) (rng_next(r) % (uint64_t) (glen_total - 2 * (hi + 512)));
+    n = rng_int(r, lo, hi);
+    memcpy(tmp, genome + p2, n);
+  } else {
+    n = mutate(r, w, glength, tmp, hi + 64, &m);
+  }
+  if (n > hi) n = hi;
+  if (n < lo) {
+    memcpy(tmp + n, genome + pos + glength, lo - n);   /* continue into the flank */
+    n = lo;
+  }
+  rlength = n;
+  memcpy(q, tmp, rlength);
+  free(tmp);
+  upcase(q, q + rlength, rlength);
+  p->rseq = (int64_t) (q - arena);
+  p->rseq_uc = p->rseq + rlength;
+  p->gseq = off;
+  p->gseq_alt = off;
+  p->rlength = rlength;
+  p->glength = glength;
+  p->lband = lband;
+  p->uband = uband;
+  p->variant = GDP_FULL;
+  p->precision = (int8_t) prec;
+  p->mismatchtype = GDP_HIGHQ;
+  p->flags = (int8_t) flags;
+  p->open = -8;
+  p->extend = -3;
+  p->tb_r = rlength;
+  p->tb_c = glength;
+  p->genomeoffset = (int32_t) pos;
+  p->chroffset = 0;
+  p->chrhigh = (uint32_t) glen_total;
+  p->watsonp = 1;
+  p->dynprogindex = 1;
+  return (int64_t) (q - arena) + 2 * rlength - off;
+}
+
+/*
+ * Like gdp_workload_pairs, with every genome window a slice of `genome`
+ * and flagged GDP_FLAG_GWINDOW (genomeoffset = the slice's first position,
+ * chroffset 0, chrhigh genome_length, plus strand).  The window bytes are
+ * also written to the arena, so the same pairs without the flag are an
+ * equivalent host-window batch.
+ */
+int64_t
+gdp_workload_resident_pairs (int kind, uint64_t seed, const char *genome, int64_t genome_length,
+                             int64_t npairs, gdp_pair_t *pairs, char *arena, int64_t arena_cap,
+                             int64_t *arena_used) {
+  rng_t r;
+  int64_t i, off = 0;
+  rng_seed(&r, seed);
+  for (i = 0; i < npairs; i++) {
+    int k = kind;
+    int64_t used;
+    if (kind == 4) {
+      double u = rng_unif(&r);
+      k = (u < 0.70) ? WL_SHORT : (u < 0.95) ? WL_LONG : WL_CDNA;
+    }
+    used = make_pair_resident(&r, k, genome, genome_length, &pairs[i], arena, off, arena_cap);
+    if (used < 0) break;
+    off += (used + 15) & ~(int64_t) 15;
+  }
+  if (arena_used) *arena_used = off;
+  return i;
+}
+
+/*
  * Generates npairs pairs.  kind: 1 fixed-150, 2 short, 3 cdna, 5 long,
  * 4 = the mixed batch (70% short / 25% long / 5% cdna).  Returns the number
  * of pairs generated (fewer if the arena is full); *arena_used gets the

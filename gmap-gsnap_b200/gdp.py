@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("GDP_LIB") or os.path.join(HERE, "lib", "libgdp.so")
 
 FULL, UPPER, LOWER = 0, 1, 2
-FLAG_JUMP_LATE, FLAG_REVP, FLAG_TRACEBACK, FLAG_RERUN16 = 1, 2, 4, 8
+FLAG_JUMP_LATE, FLAG_REVP, FLAG_TRACEBACK, FLAG_RERUN16, FLAG_GWINDOW = 1, 2, 4, 8, 16
 HIGHQ, MEDQ, LOWQ, ENDQ = 0, 1, 2, 3
 STATUS = {0: "GDP_OK", 1: "GDP_ERR_LEN", 2: "GDP_ERR_BAND", 3: "GDP_ERR_PARAM",
           4: "GDP_ERR_BUDGET", 5: "GDP_ERR_TIMEOUT", 6: "GDP_ERR_CUDA",
@@ -100,6 +100,17 @@ def load(path=LIB_PATH):
     lib.gdp_workload_pairs.restype = i64
     lib.gdp_pair_cells.argtypes = [vp]
     lib.gdp_pair_cells.restype = i64
+    lib.gdp_workload_resident_pairs.argtypes = lib.gdp_workload_pairs.argtypes
+    lib.gdp_workload_resident_pairs.restype = i64
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.gdp_server_create.argtypes = [i32, i32, i32, i64, i64, vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+    lib.gdp_server_submit.argtypes = [vp, vp, i64, vp, i64]
+    lib.gdp_server_submit.restype = i64
+    lib.gdp_server_wait.argtypes = [vp, i64, vp, vp, i64, ctypes.POINTER(i64), dp]
+    lib.gdp_server_drive.argtypes = [vp, vp, i64, vp, i64, ctypes.c_double, ctypes.c_uint64, vp, vp, dp]
+    lib.gdp_server_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                     ctypes.POINTER(i64), dp]
+    lib.gdp_server_destroy.argtypes = [vp]
     return lib
 
 
@@ -134,6 +145,23 @@ def make_pairs(lib, kind, seed, genome, npairs, arena_bytes=None):
     used = ctypes.c_int64(0)
     n = lib.gdp_workload_pairs(kind, seed, _ptr(genome), genome.size, npairs, _ptr(pairs),
                                _ptr(arena), arena_bytes, ctypes.byref(used))
+    if n != npairs:
+        raise RuntimeError(f"arena too small: generated {n} of {npairs} pairs")
+    return pairs, arena[:max(used.value, 1)].copy()
+
+
+def make_resident_pairs(lib, kind, seed, genome, npairs, arena_bytes=None):
+    """Like make_pairs, but every genome window is a slice of `genome`
+    flagged FLAG_GWINDOW (the device extracts it from the resident genome);
+    the arena still holds the window bytes."""
+    if arena_bytes is None:
+        per = {WL_FIXED: 700, WL_SHORT: 1400, WL_CDNA: 16000, WL_MIX: 12000, WL_LONG: 36000}[kind]
+        arena_bytes = npairs * per + (1 << 16)
+    pairs = np.zeros(npairs, dtype=PAIR_DTYPE)
+    arena = np.zeros(arena_bytes, dtype=np.uint8)
+    used = ctypes.c_int64(0)
+    n = lib.gdp_workload_resident_pairs(kind, seed, _ptr(genome), genome.size, npairs, _ptr(pairs),
+                                        _ptr(arena), arena_bytes, ctypes.byref(used))
     if n != npairs:
         raise RuntimeError(f"arena too small: generated {n} of {npairs} pairs")
     return pairs, arena[:max(used.value, 1)].copy()
@@ -254,3 +282,67 @@ class Context:
         if rc != 0:
             raise RuntimeError(f"gdp_fill_dump: {STATUS.get(rc, rc)} {self.error()}")
         return offs, H, dN, dE, dF, results
+
+
+class Server:
+    """The continuous-batching request loop (gdp_server_*)."""
+
+    def __init__(self, lib, device=0, mode=0, workers=2, budget=0, max_batch=0, blocks=None, altblocks=None,
+                 length=None):
+        self.lib = lib
+        if blocks is not None and length is None:
+            length = blocks.size // 3 * 32
+        h = ctypes.c_void_p()
+        rc = lib.gdp_server_create(device, mode, workers, budget, max_batch, _ptr(blocks), _ptr(altblocks),
+                                   length or 0, ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"gdp_server_create failed: {STATUS.get(rc, rc)}")
+        self.h = h
+        self._keep = (blocks, altblocks)
+
+    def close(self):
+        if self.h:
+            self.lib.gdp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, pairs, arena):
+        rid = self.lib.gdp_server_submit(self.h, _ptr(pairs), pairs.size, _ptr(arena), arena.size)
+        if rid < 0:
+            raise RuntimeError(f"gdp_server_submit: {STATUS.get(-rid, rid)}")
+        return rid, pairs.size, int((pairs["rlength"].astype(np.int64) + pairs["glength"] + 2).sum())
+
+    def wait(self, ticket):
+        rid, n, cap = ticket
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        recs = np.zeros(max(cap, 1), dtype=REC_DTYPE)
+        nrecs, lat = ctypes.c_int64(0), ctypes.c_double(0)
+        rc = self.lib.gdp_server_wait(self.h, rid, _ptr(results), _ptr(recs), cap, ctypes.byref(nrecs),
+                                      ctypes.byref(lat))
+        if rc not in (0, 4):     # GDP_ERR_BUDGET is a per-request outcome, in results["status"]
+            raise RuntimeError(f"gdp_server_wait: {STATUS.get(rc, rc)}")
+        return results, recs[:nrecs.value], lat.value
+
+    def drive(self, pool, arena, nrequests, rate, seed=1, want_results=False):
+        """Poisson load: returns (latencies ms, elapsed s, results or None)."""
+        lat = np.zeros(nrequests, dtype=np.float64)
+        res = np.zeros(nrequests, dtype=RESULT_DTYPE) if want_results else None
+        el = ctypes.c_double(0)
+        rc = self.lib.gdp_server_drive(self.h, _ptr(pool), pool.size, _ptr(arena), nrequests, rate, seed,
+                                       _ptr(res), _ptr(lat), ctypes.byref(el))
+        if rc != 0:
+            raise RuntimeError(f"gdp_server_drive: {STATUS.get(rc, rc)}")
+        return lat, el.value, res
+
+    def stats(self):
+        b, p, m, pk = (ctypes.c_int64(0) for _ in range(4))
+        busy = ctypes.c_double(0)
+        self.lib.gdp_server_stats(self.h, ctypes.byref(b), ctypes.byref(p), ctypes.byref(m), ctypes.byref(pk),
+                                  ctypes.byref(busy))
+        return {"batches": b.value, "pairs": p.value, "max_batch_pairs": m.value,
+                "peak_reserved_bytes": pk.value, "busy_s": busy.value}

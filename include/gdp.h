@@ -48,7 +48,8 @@ enum {
   GDP_FLAG_JUMP_LATE = 1,   /* jump_late_p */
   GDP_FLAG_REVP = 2,        /* revp: sequences are read backwards from their last character */
   GDP_FLAG_TRACEBACK = 4,   /* run Dynprog_traceback_* from (tb_r, tb_c) */
-  GDP_FLAG_RERUN16 = 8      /* precision 8: rerun in 16-bit when the 8-bit fill overflows */
+  GDP_FLAG_RERUN16 = 8,     /* precision 8: rerun in 16-bit when the 8-bit fill overflows */
+  GDP_FLAG_GWINDOW = 16     /* the genome window comes from the resident genome (see below) */
 };
 
 /* Mismatch types (src/dynprog.h:53) */
@@ -64,7 +65,7 @@ enum {
   GDP_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
   GDP_ERR_CUDA = 6,      /* a CUDA call failed */
   GDP_ERR_RECS = 7,      /* traceback record buffer too small */
-  GDP_ERR_NOGENOME = 8   /* a traceback needs genome characters but no genome is loaded */
+  GDP_ERR_NOGENOME = 8   /* genome characters are needed beyond the resident genome (or none is loaded) */
 };
 
 /*
@@ -72,6 +73,16 @@ enum {
  * sequence arena.  Every sequence is stored forward in memory; with
  * GDP_FLAG_REVP the reference's convention (a pointer to the last character,
  * indexed seq[1-r]) is applied by the library.
+ *
+ * GDP_FLAG_GWINDOW: the device writes the genome window itself, from the
+ * genome made resident by gdp_set_genome, into the arena at gseq (and at
+ * gseq_alt from the alternate genome, when gseq_alt != gseq), before the
+ * fill; the caller only reserves those glength bytes.  Window character j
+ * is the character the traceback reads for genomic coordinate
+ * genomeoffset + j (revp: genomeoffset - (glength - 1) + j): chroffset + gp
+ * on the plus strand, the complement of chrhigh - gp on the minus strand,
+ * '*' outside [chroffset, chrhigh) (get_genomic_nt, src/pairpool.c:1015).
+ * A window that reaches past the resident genome gets GDP_ERR_NOGENOME.
  */
 typedef struct gdp_pair {
   int64_t rseq;          /* rsequence, rlength bytes */
@@ -204,9 +215,10 @@ void *gdp_ctx_stream(gdp_ctx *ctx);
 /*
  * Per-kernel timing.  While enabled, every kernel launch of the context is
  * bracketed by CUDA events on its stream.  gdp_profile_read(ctx, id, ...)
- * returns, for kernel id 0..27 (0..23 fill kinds, 24 traceback, 25 result
- * initialisation, 26 integer-rate probe, 27 rerun-list compaction), its name, total device
- * milliseconds and launch count since the last reset.
+ * returns, for kernel id 0..63 (the fill kinds first, then the traceback,
+ * result initialisation, integer-rate probe, rerun-list compaction, record
+ * compaction and window extraction; unused ids have an empty name), its
+ * name, total device milliseconds and launch count since the last reset.
  */
 int gdp_profile_enable(gdp_ctx *ctx, int on);
 int gdp_profile_read(gdp_ctx *ctx, int id, char *name, int name_cap, double *ms, int64_t *launches);
@@ -243,6 +255,44 @@ double gdp_measure_int_peak(gdp_ctx *ctx);
  */
 int gdp_fill16_noalloc(int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
                        uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results, void *stream);
+
+/*
+ * Serving loop (continuous batching).  A server owns `nworkers` contexts
+ * on `device` (tables of `mode`), each holding the resident genome (may be
+ * NULL).  Requests of one or more pairs are submitted from any thread and
+ * admitted in arrival order while the direction-matrix memory of the
+ * admitted, unfinished requests stays within `dir_budget_bytes` (0: 40 GB);
+ * a worker takes every admitted waiting request (up to `max_batch_pairs`
+ * pairs; 0: 131,072) as one batch.  With two or more workers, batches
+ * overlap on the device.  Results do not depend on the batching.
+ *
+ * gdp_server_submit copies the request and returns its id (>= 0), or
+ * -GDP_ERR_* when it is malformed; a request larger than the budget
+ * completes at once with GDP_ERR_BUDGET.  gdp_server_wait blocks until the
+ * request is done and copies its results (rec_offset relative to `recs`),
+ * records and latency (submit to results on the host, in ms).
+ *
+ * gdp_server_drive is a load generator: `nrequests` single-pair requests,
+ * request k being pool[k % npool] (offsets into `arena`), submitted from the
+ * calling thread at Poisson arrival times of `rate` requests per second.
+ * It returns when all are done, with each request's latency, optionally its
+ * result (results_out may be NULL; records are not kept), and the elapsed
+ * time from the first arrival to the last completion.
+ */
+typedef struct gdp_server gdp_server;
+int gdp_server_create(int device, int mode, int nworkers, int64_t dir_budget_bytes, int64_t max_batch_pairs,
+                      const uint32_t *genome_blocks, const uint32_t *alt_blocks, uint64_t genome_length,
+                      gdp_server **server);
+int64_t gdp_server_submit(gdp_server *server, const gdp_pair_t *pairs, int64_t npairs, const char *arena,
+                          int64_t arena_bytes);
+int gdp_server_wait(gdp_server *server, int64_t id, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                    int64_t *nrecs, double *latency_ms);
+int gdp_server_drive(gdp_server *server, const gdp_pair_t *pool, int64_t npool, const char *arena,
+                     int64_t nrequests, double rate, uint64_t seed, gdp_result_t *results_out,
+                     double *latency_ms, double *elapsed_s);
+int gdp_server_stats(gdp_server *server, int64_t *batches, int64_t *pairs, int64_t *max_batch_pairs,
+                     int64_t *peak_reserved_bytes, double *busy_s);
+void gdp_server_destroy(gdp_server *server);
 
 /* Kernel launches issued by the context since creation (one per kernel). */
 int64_t gdp_launch_count(gdp_ctx *ctx);

@@ -1,0 +1,194 @@
+"""Device genome windows and the continuous-batching serving loop.
+
+* Windows extracted on the device from the resident genome
+  (GDP_FLAG_GWINDOW) give the same results as the same windows supplied by
+  the host, on both strands, with revp and past the chromosome bounds.
+* A request's results (scores, traceback counters, Pair records) are the
+  same when it runs alone and when it is batched with others, through the
+  submit/wait API and under the Poisson load generator.
+* Admission keeps the admitted direction memory within the budget.
+"""
+import numpy as np
+import pytest
+
+import gdp
+
+pytestmark = pytest.mark.gpu
+
+GENOME_LEN = 1 << 22
+COMPL = bytes.maketrans(b"ACGTN*", b"TGCAN*")
+
+
+@pytest.fixture(scope="module")
+def genome(gdplib):
+    return gdp.make_genome(gdplib, 515, GENOME_LEN)
+
+
+def _host_window(g, p):
+    """The window the device should extract (get_genomic_nt semantics)."""
+    gl = int(p["glength"])
+    g0 = int(p["genomeoffset"]) - (gl - 1) if p["flags"] & gdp.FLAG_REVP else int(p["genomeoffset"])
+    out = np.empty(gl, np.uint8)
+    lo, hi = int(p["chroffset"]), int(p["chrhigh"])
+    for j in range(gl):
+        gp = g0 + j
+        pos = (lo + gp) & 0xFFFFFFFF if p["watsonp"] else (hi - gp) & 0xFFFFFFFF
+        if pos < lo or pos >= hi:
+            out[j] = ord("*")
+        else:
+            c = g[pos]
+            out[j] = c if p["watsonp"] else bytes([c]).translate(COMPL)[0]
+    return out
+
+
+def _same(ra, rb, keys=("status", "score", "precision", "rerun", "tb_score", "nmatches", "nmismatches",
+                        "nopens", "nindels", "nrecs")):
+    return all(np.array_equal(ra[k], rb[k]) for k in keys)
+
+
+def test_device_windows_equal_host_windows(gdplib, genome):
+    g, blocks = genome
+    pairs, arena = gdp.make_resident_pairs(gdplib, gdp.WL_SHORT, 21, g, 1500)
+    rng = np.random.default_rng(5)
+    # vary strand, revp and chromosome bounds; the host arena gets the same windows
+    crick = rng.random(pairs.size) < 0.4
+    pairs["watsonp"][crick] = 0
+    pairs["chrhigh"][crick] = GENOME_LEN - 1 - pairs["chroffset"][crick]
+    rev = rng.random(pairs.size) < 0.3
+    pairs["flags"][rev] |= gdp.FLAG_REVP
+    tight = rng.random(pairs.size) < 0.1      # windows that cross chrhigh / chroffset
+    for i in np.nonzero(tight)[0]:
+        p = pairs[i]
+        if p["watsonp"]:
+            p["chrhigh"] = p["chroffset"] + p["genomeoffset"] + p["glength"] // 2
+        else:
+            p["chroffset"] = p["chrhigh"] - p["genomeoffset"] - p["glength"] // 2
+    host = pairs.copy()
+    host["flags"] &= ~np.int8(gdp.FLAG_GWINDOW)
+    harena = arena.copy()
+    for i in range(pairs.size):
+        gs = int(pairs["gseq"][i])
+        harena[gs:gs + int(pairs["glength"][i])] = _host_window(g, pairs[i])
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, None, GENOME_LEN)
+    ctx.profile(True)
+    rd, recd = ctx.align(pairs, arena)
+    prof = ctx.profile_read()
+    rh, rech = ctx.align(host, harena)
+    ctx.close()
+    assert "window_kernel" in prof
+    assert (rd["status"] == 0).all() and (rh["status"] == 0).all()
+    assert _same(rd, rh)
+    assert recd.tobytes() == rech.tobytes()
+
+
+def test_window_beyond_the_resident_genome(gdplib, genome):
+    g, blocks = genome
+    pairs, arena = gdp.make_resident_pairs(gdplib, gdp.WL_FIXED, 22, g, 4)
+    pairs["genomeoffset"][1] = GENOME_LEN - 50       # runs past the genome
+    pairs["chrhigh"][1] = GENOME_LEN + 1000
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, None, GENOME_LEN)
+    res, _ = ctx.align(pairs, arena)
+    ctx.close()
+    assert res["status"][1] == 8                    # GDP_ERR_NOGENOME
+    assert (res["status"][[0, 2, 3]] == 0).all()
+
+
+def _requests(gdplib, g):
+    """Forty requests of 1..12 pairs: short reads, long reads and cDNA pairs,
+    with device and host windows."""
+    a, aa = gdp.make_resident_pairs(gdplib, gdp.WL_SHORT, 31, g, 300)
+    b, ba = gdp.make_resident_pairs(gdplib, gdp.WL_LONG, 32, g, 6)
+    c, ca = gdp.make_pairs(gdplib, gdp.WL_CDNA, 33, g, 8)
+    rng = np.random.default_rng(34)
+    out = []
+    ia = 0
+    for k in range(40):
+        if k % 10 == 3:
+            out.append((b[k // 10:k // 10 + 1], ba))
+        elif k % 10 == 7:
+            out.append((c[k // 10:k // 10 + 2], ca))
+        else:
+            n = int(rng.integers(1, 13))
+            out.append((a[ia:ia + n], aa))
+            ia += n
+    return out
+
+
+def test_results_same_alone_and_in_the_mix(gdplib, genome):
+    g, blocks = genome
+    reqs = _requests(gdplib, g)
+    srv = gdp.Server(gdplib, workers=2, max_batch=48, budget=256 << 20, blocks=blocks, length=GENOME_LEN)
+    alone = []
+    for pairs, arena in reqs:
+        alone.append(srv.wait(srv.submit(pairs, arena)))
+    tickets = [srv.submit(pairs, arena) for pairs, arena in reqs]
+    mixed = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert st["batches"] > len(reqs) + 1     # the mixed round really batched
+    for k, ((ra, reca, _), (rm, recm, _)) in enumerate(zip(alone, mixed)):
+        assert (ra["status"] == 0).all(), k
+        assert _same(ra, rm), k
+        assert np.array_equal(ra["rec_offset"], rm["rec_offset"]), k
+        assert reca.tobytes() == recm.tobytes(), k
+    # and equal to one direct batch of everything
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, None, GENOME_LEN)
+    for k, (pairs, arena) in enumerate(reqs):
+        rd, recd = ctx.align(pairs, arena)
+        assert _same(rd, alone[k][0]), k
+        assert recd.tobytes() == alone[k][1].tobytes(), k
+    ctx.close()
+
+
+def test_poisson_load_matches_alone(gdplib, genome):
+    g, blocks = genome
+    pool, arena = gdp.make_resident_pairs(gdplib, gdp.WL_SHORT, 41, g, 2000)
+    srv = gdp.Server(gdplib, workers=2, blocks=blocks, length=GENOME_LEN)
+    lat, elapsed, res = srv.drive(pool, arena, 6000, rate=200000.0, seed=3, want_results=True)
+    st = srv.stats()
+    ref = []
+    for i in range(50):
+        ref.append(srv.wait(srv.submit(pool[i:i + 1], arena))[0])
+    srv.close()
+    assert elapsed > 0 and (lat > 0).all()
+    assert st["pairs"] >= 6000 and st["batches"] < 6000   # requests were batched
+    for k in range(6000):
+        i = k % pool.size
+        if i < 50:
+            assert _same(res[k:k + 1], ref[i]), k
+    direct = gdp.Context(gdplib)
+    direct.set_genome(blocks, None, GENOME_LEN)
+    rd, _ = direct.align(pool, arena)
+    direct.close()
+    assert _same(res[:2000], rd)
+
+
+def _dir_bytes(p):
+    """Direction bytes of one full-band 16-bit pair (its block-column words)."""
+    X, Y, lb, ub, W = int(p["rlength"]), int(p["glength"]), int(p["lband"]), int(p["uband"]), 16
+    words = 0
+    for xlo in range(0, X + 1, W):
+        y0, y1 = max(xlo - lb, 0), min(min(xlo + W - 1, X) + ub, Y)
+        words += max(0, y1 - y0 + 1) * (W // 8)
+    return ((words + 3) & ~3) * 4
+
+
+def test_admission_respects_the_budget(gdplib, genome):
+    g, blocks = genome
+    pairs, arena = gdp.make_resident_pairs(gdplib, gdp.WL_LONG, 51, g, 12)
+    sizes = [_dir_bytes(p) for p in pairs]
+    budget = int(max(sizes) * 1.5)
+    assert sum(sizes) > budget
+    srv = gdp.Server(gdplib, workers=2, budget=budget, blocks=blocks, length=GENOME_LEN)
+    tickets = [srv.submit(pairs[i:i + 1], arena) for i in range(pairs.size)]
+    big = srv.submit(pairs, arena)                  # all twelve at once exceed the budget
+    out = [srv.wait(t) for t in tickets]
+    rbig, _, _ = srv.wait(big)
+    st = srv.stats()
+    srv.close()
+    assert all((r["status"] == 0).all() for r, _, _ in out)
+    assert (rbig["status"] == 4).all()              # GDP_ERR_BUDGET
+    assert 0 < st["peak_reserved_bytes"] <= budget
