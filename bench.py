@@ -117,24 +117,26 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(world, value):
+def _reduce(world, value, op):
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(world, value):
+    """The slowest rank's time: the whole job ends when it does."""
+    import torch.distributed as dist
+    return _reduce(world, value, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(world, value):
-    if world == 1:
-        return value
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(world, value, dist.ReduceOp.SUM if world > 1 else None)
 
 
 def make_workload(lib, name, npairs, seed, genome_len=1 << 24):

@@ -339,8 +339,106 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
   }
 }
 
+/*
+ * A steady column: every lane of a full block lies inside the band.  For
+ * the full fill that means no top and no bottom band cell in the block
+ * (lane 0 below the top edge, lane W-1 above the bottom edge); for the
+ * upper and lower fills, the diagonal has passed the block (no E mask, no
+ * diagonal fix).  Those columns need none of the lane masks of
+ * block_column, and in the bands of long pairs they are most of the work.
+ * The result equals block_column's for the same column.  `vmax` collects
+ * the in-band scores (MODE != 0).
+ */
+template <int W, int VARIANT, bool LATE, int MODE>
+__device__ __forceinline__ int2
+block_column_steady (Block<W> &B, const PairView &v, int diag, int2 above, int ka, int kb, uint32_t *dcol,
+                     int &vmax) {
+  constexpr int LO = (W == 32) ? -128 : -32768;
+  constexpr int HI = (W == 32) ? 127 : 32767;
+  constexpr int WORDS = W / 8;
+  const int open = v.open, ext = v.ext;
+  uint32_t sA[4], sB[4];
+  {
+    const uint32_t dA = (ka == 4) ? 0x1111u : 0u, dB = (kb == 4) ? 0x1111u : 0u;
+    sA[0] = GDP_SEL(ka); sB[0] = GDP_SEL(kb);
+#pragma unroll
+    for (int k = 1; k < 4; k++) { sA[k] = sA[k - 1] + dA; sB[k] = sB[k - 1] + dB; }
+  }
+  uint32_t w[WORDS];
+#pragma unroll
+  for (int j = 0; j < WORDS; j++) w[j] = 0;
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    const int Hold = B.H[i];
+    const int T1 = __viaddmax_s32(Hold, open, LO);
+    bool pE;
+    const int m = tie_max<LATE>(B.E[i], T1, pE);
+    const int Ee = __viaddmax_s32(m, ext, LO);
+    int ps;
+    if (VARIANT == GDP_LOWER) {
+      ps = prof_byte(B.plo[i], B.phi4[i >> 2], sA[i & 3]);
+    } else {
+      ps = max(prof_byte(B.plo[i], B.phi4[i >> 2], sA[i & 3]), prof_byte(B.plo[i], B.phi4[i >> 2], sB[i & 3]));
+    }
+    const int Hv = min(__viaddmax_s32(diag, ps, LO), HI);
+    diag = Hold;
+    bool pN;
+    B.H[i] = tie_max<LATE>(Ee, Hv, pN);
+    B.E[i] = Ee;
+    if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
+    if (pN) w[i >> 3] |= 1u << (i & 7);
+  }
+  int2 out;
+  if (VARIANT == GDP_FULL) {
+    int Fp = GDP_NEGINT, Hp = GDP_NEGINT;
+    if (B.xlo > 0) { Fp = above.y; Hp = above.x; }
+#pragma unroll
+    for (int i = 0; i < W; i++) {
+      bool pF, pV;
+      const int F = tie_max<LATE>(Fp, Hp + open, pF) + ext;
+      const int Hn = tie_max<LATE>(F, B.H[i], pV);
+      B.H[i] = Hn;
+      Hp = Hn;
+      Fp = F;
+      if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
+      if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
+    }
+    out = make_int2(B.H[W - 1], Fp);
+  } else {
+    out = make_int2(B.H[W - 1], 0);
+  }
+  if (MODE != 0) {
+#pragma unroll
+    for (int i = 0; i < W; i++) vmax = max(vmax, B.H[i]);
+  }
+  if (WORDS == 2) {
+    *reinterpret_cast<uint2 *>(dcol) = make_uint2(w[0], w[1]);
+  } else {
+    *reinterpret_cast<uint4 *>(dcol) = make_uint4(w[0], w[1], w[WORDS > 2 ? 2 : 0], w[WORDS > 3 ? 3 : 0]);
+  }
+  return out;
+}
+
+/* Whether column y of the full block at xlo is steady (see
+   block_column_steady).  For the upper and lower fills with an in-band
+   score check (MODE != 0) the column must also hold no lane above the band,
+   so that every lane's score counts. */
+template <int W, int VARIANT, int MODE>
+__device__ __forceinline__ bool
+column_steady (const PairView &v, int xlo, int y) {
+  const int rel = y - xlo;
+  if (VARIANT == GDP_FULL) return rel < v.uband && rel + v.lband > W - 1;
+  return rel > W - 1 && (MODE == 0 || rel <= v.g.band_hi);
+}
+
+/* Steady columns take block_column_steady in the one-thread-per-pair
+   16-bit fills (0 switches that off). */
+#ifndef GDP_STEADY
+#define GDP_STEADY 1
+#endif
+
 #ifndef GDP_FILL_MINB
-#define GDP_FILL_MINB 5
+#define GDP_FILL_MINB 4
 #endif
 
 /* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records whether an
@@ -361,6 +459,7 @@ fill_thread_kernel (FillParams P) {
   const int n = *P.count;
   for (int64_t li = slot; li < n; li += P.nslots) {
     const int pi = __ldg(P.list + li);
+    if (pi < 0) continue;   /* padding: warps hold pairs of one band width */
     const gdp_pair_t p = P.pairs[pi];
     gdp_meta_t *mp = P.meta + pi;
     if (MODE == 2 && mp->maxh16 >= 127) {
@@ -374,6 +473,7 @@ fill_thread_kernel (FillParams P) {
     const int64_t scs = P.nslots;
     int final_score = LO;
     bool reached = false;
+    int vmax = LO;   /* in-band scores of the steady columns */
 
     for (int xlo = 0; xlo <= v.g.X; xlo += W) {
       Block<W> B;
@@ -400,8 +500,16 @@ fill_thread_kernel (FillParams P) {
         else diag = (xlo == 0) ? LO : bot_prev;
         bot_prev = above.x;
         int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
-        const int2 out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd,
-                                                              reached, final_score);
+        int2 out;
+        if constexpr (W == 16 && MODE != 2 && GDP_STEADY) {
+          if (hd == nullptr && B.last == W - 1 && y >= 1 && y != v.g.Y && column_steady<W, VARIANT, MODE>(v, xlo, y))
+            out = block_column_steady<W, VARIANT, LATE, MODE>(B, v, diag, above, ka, kb, dcol, vmax);
+          else
+            out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
+                                                       final_score);
+        } else {
+          out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached, final_score);
+        }
         sc[(int64_t) y * scs] = out;
         dcol += WORDS;
         ka = ka2; kb = kb2; above = above2;
@@ -410,55 +518,74 @@ fill_thread_kernel (FillParams P) {
       dir = dcol;
       if (MODE == 2 && reached) break;
     }
+    if (vmax >= 127) reached = true;
     fill_finish<W, MODE>(P, pi, mp, v.g, reached, final_score);
   }
 }
 
 /*
- * One warp per pair for long 16-bit pairs (plain fills).  Lane l owns the
- * blocks b = l, l + 32, l + 64, ... and processes column y of block b at
- * step t = y + b: block b needs the final column y (F carry, last lane H)
- * and column y - 1 (diagonal) of block b - 1, which lane (l - 1) mod 32
- * produced one and two steps earlier, so one rotation shuffle per step
- * carries them.  A lane's next block starts after its previous one ends as
- * long as a block sweeps fewer than 32 * 17 - 16 columns; the planner only
- * sends pairs with narrower sweeps here.  Each lane runs block_column, the
- * same column step as the one-thread-per-pair kernel.
+ * One group of K lanes (K = 8, 16 or 32; 32 / K pairs per warp) per long
+ * 16-bit pair (plain fills).  Lane l of a group owns the blocks b = l,
+ * l + K, l + 2K, ... and processes column y of block b at step t = y + b:
+ * block b needs the final column y (F carry, last lane H) and column y - 1
+ * (diagonal) of block b - 1, which the previous lane of the group produced
+ * one and two steps earlier, so one rotation shuffle inside the group per
+ * step carries them.  A lane's next block starts after its previous one
+ * ends as long as a block sweeps fewer than 17 K - 16 columns; the planner
+ * picks the smallest K that allows the pair's sweep, so lanes idle between
+ * blocks for at most a few steps.  Each lane runs block_column, the same
+ * column step as the one-thread-per-pair kernel.
  */
-template <int VARIANT, bool LATE>
+template <int VARIANT, bool LATE, int K>
 __global__ void __launch_bounds__(128, 4)
 fill_warp_kernel (FillParams P) {
-  constexpr int W = 16, WORDS = 2, LO = -32768;
+  constexpr int W = 16, WORDS = 2, LO = -32768, G = 32 / K;
+  static_assert(K == 8 || K == 16 || K == 32, "group sizes divide the warp");
   __shared__ int8_t s_nt2int[128];
   for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, glane = lane & (K - 1), group = lane / K;
+  const int prev = group * K + ((glane + K - 1) & (K - 1));   /* previous lane of the group */
   const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
   const int n = *P.count;
-  for (int64_t li = warp; li < n; li += nwarps) {
-    const int pi = __ldg(P.list + li);
-    const gdp_pair_t p = P.pairs[pi];
-    gdp_meta_t *mp = P.meta + pi;
+  /* every lane of the warp stays in both loops: the shuffles need all 32 */
+  for (int64_t base = warp * G; base < n; base += nwarps * G) {
+    const int64_t li = base + group;
+    const bool valid = li < n;
+    const int pi = valid ? __ldg(P.list + li) : -1;
+    gdp_pair_t p;
+    if (valid) {
+      p = P.pairs[pi];
+    } else {
+      memset(&p, 0, sizeof(p));
+      p.rlength = p.glength = 1;
+    }
+    gdp_meta_t *mp = valid ? P.meta + pi : nullptr;
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
-    uint32_t *dir = P.dirs + mp->dir16;
+    uint32_t *dir = valid ? P.dirs + mp->dir16 : nullptr;
     /* blocks that sweep something: 0 .. nb - 1 */
-    int nb = v.g.X / W + 1;
-    while (nb > 0) {
-      int a0, a1;
-      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
-      if (a1 >= a0) break;
-      nb--;
+    int nb = 0, tend = -1;
+    if (valid) {
+      nb = v.g.X / W + 1;
+      while (nb > 0) {
+        int a0, a1;
+        gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+        if (a1 >= a0) break;
+        nb--;
+      }
+      if (nb > 0) {
+        int a0, a1;
+        gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
+        tend = a1 + nb - 1;
+      }
     }
-    int tend = -1;
-    if (nb > 0) {
-      int a0, a1;
-      gdp_block_sweep(&v.g, (nb - 1) * W, &a0, &a1);
-      tend = a1 + nb - 1;
-    }
+    int tmax = tend;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmax = max(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
     /* this lane's first block and its word offset */
-    int b = lane;
+    int b = glane;
     int64_t boff = 0;
     for (int k = 0; k < b && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
     Block<W> B;
@@ -467,10 +594,10 @@ fill_warp_kernel (FillParams P) {
     bool reached = false;
     int2 mine = make_int2(LO, GDP_NEGINT);   /* this lane's output of the last step */
     int bot_prev = LO;                         /* H[y-1][xlo-1] received a step ago */
-    for (int t = 0; t <= tend; t++) {
+    for (int t = 0; t <= tmax; t++) {
       /* (H, F) of block b - 1 at column t - b, produced by the previous lane */
-      const int rx = __shfl_sync(0xffffffffu, mine.x, (lane + 31) & 31);
-      const int ry = __shfl_sync(0xffffffffu, mine.y, (lane + 31) & 31);
+      const int rx = __shfl_sync(0xffffffffu, mine.x, prev);
+      const int ry = __shfl_sync(0xffffffffu, mine.y, prev);
       if (b < nb) {
         if (!started) {
           block_start<W, VARIANT, LATE>(B, v, P.tab, b * W);
@@ -489,9 +616,9 @@ fill_warp_kernel (FillParams P) {
           mine = block_column<W, VARIANT, LATE, 0>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
                                                    final_score);
           if (y == B.y1) {
-            /* move to block b + 32 */
-            for (int k = b; k < b + 32 && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
-            b += 32;
+            /* move to block b + K */
+            for (int k = b; k < b + K && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
+            b += K;
             started = false;
           }
         }
@@ -499,8 +626,8 @@ fill_warp_kernel (FillParams P) {
       bot_prev = rx;
     }
     /* the lane that owned the final cell's block reports its score */
-    const int fs = __shfl_sync(0xffffffffu, final_score, (v.g.X / W) & 31);
-    if (lane == 0) fill_finish<W, 0>(P, pi, mp, v.g, false, fs);
+    const int fs = __shfl_sync(0xffffffffu, final_score, group * K + ((v.g.X / W) & (K - 1)));
+    if (valid && glane == 0) fill_finish<W, 0>(P, pi, mp, v.g, false, fs);
   }
 }
 
@@ -603,7 +730,7 @@ compact_rerun_kernel (const int32_t *list, const int32_t *count, const gdp_meta_
   const int n = *count;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int pi = list[i];
-    const bool need = meta[pi].maxh16 < 127;
+    const bool need = pi >= 0 && meta[pi].maxh16 < 127;
     const unsigned mask = __ballot_sync(__activemask(), need);
     const int lane = threadIdx.x & 31;
     int base = 0;

@@ -40,6 +40,7 @@
 #include "gdp_internal.h"
 #include "fill_thread.cuh"
 #include "traceback.cuh"
+#include "traceback_warp.cuh"
 
 #define GDP_VERSION "gdp-b200 0.2"
 
@@ -82,18 +83,18 @@ struct HostBuf {   /* pinned host memory */
 };
 
 constexpr int NTHREADKINDS = 24;   /* one thread per pair: (W32, variant, late, pass) */
-constexpr int NWARPKINDS = 6;      /* one warp per pair (16-bit plain): 24 + variant * 2 + late */
+constexpr int NWARPKINDS = 18;     /* K lanes per pair (16-bit plain): 24 + (variant * 2 + late) * 3 + log2(K) - 3 */
+constexpr int WARP_K[3] = {8, 16, 32};
 constexpr int NCTAKINDS = 24;      /* one CTA per pair (16-bit plain): 30 + (variant * 2 + late) * 4 + log2(NW) - 1 */
 constexpr int NKINDS = NTHREADKINDS + NWARPKINDS + NCTAKINDS;
 constexpr int CTA_NW[4] = {2, 4, 8, 16};
-constexpr int NBUCKETS = 64 * 32; /* (block count, sweep width) buckets inside a bin */
 
 inline int kind_id (int w32, int variant, int late, int pass) {
   return (((w32 * 3 + variant) * 2 + late) * 2) + pass;
 }
 
-inline int warp_kind_id (int variant, int late) {
-  return NTHREADKINDS + variant * 2 + late;
+inline int warp_kind_id (int variant, int late, int kg) {
+  return NTHREADKINDS + (variant * 2 + late) * 3 + kg;
 }
 
 inline int cta_kind_id (int variant, int late, int nwi) {
@@ -150,6 +151,9 @@ struct gdp_ctx {
   int nsm = 148;
   cudaStream_t stream = nullptr;        /* compute */
   cudaStream_t h2d = nullptr, d2h = nullptr;
+  /* the one-warp/one-CTA-per-pair fill kinds run beside the thread kinds */
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
@@ -158,6 +162,7 @@ struct gdp_ctx {
   int64_t wave = 131072;
   int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
   int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
+  bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
   DevBuf arena, scratch;
   Slot slot[2];
   std::atomic<int64_t> launches{0};
@@ -167,8 +172,8 @@ struct gdp_ctx {
   bool profiling = false;
   struct Timed { int id; cudaEvent_t a, b; };
   std::vector<Timed> timed;
-  double prof_ms[64] = {0};
-  int64_t prof_n[64] = {0};
+  double prof_ms[128] = {0};
+  int64_t prof_n[128] = {0};
 };
 
 /* kernel ids for profiling: 0..NKINDS-1 fill kinds, then traceback, init,
@@ -183,7 +188,7 @@ struct gdp_ctx {
 static const char *
 kernel_name (int id) {
   static char buf[NPROF][48];
-  if (id == PROF_TB) return "traceback_kernel";
+  if (id == PROF_TB) return "traceback";
   if (id == PROF_INIT) return "init_results_kernel";
   if (id == PROF_PEAK) return "int_peak_kernel";
   if (id == PROF_RERUN) return "compact_rerun_kernel";
@@ -196,9 +201,9 @@ kernel_name (int id) {
     return buf[id];
   }
   if (id >= NTHREADKINDS) {
-    const int variant = (id - NTHREADKINDS) / 2, late = (id - NTHREADKINDS) & 1;
-    snprintf(buf[id], sizeof(buf[id]), "fill_warp<W16,%s,%s>",
-             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early");
+    const int c = id - NTHREADKINDS, vl = c / 3, variant = vl / 2, late = vl & 1;
+    snprintf(buf[id], sizeof(buf[id]), "fill_warp<W16,%s,%s,%dlanes>",
+             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early", WARP_K[c % 3]);
     return buf[id];
   }
   const int pass = id & 1, late = (id >> 1) & 1, vw = id >> 2, variant = vw % 3, w32 = vw / 3;
@@ -209,18 +214,18 @@ kernel_name (int id) {
 }
 
 static void
-prof_begin (gdp_ctx *ctx, cudaEvent_t *a) {
+prof_begin (gdp_ctx *ctx, cudaEvent_t *a, cudaStream_t s = nullptr) {
   if (!ctx->profiling) return;
   cudaEventCreate(a);
-  cudaEventRecord(*a, ctx->stream);
+  cudaEventRecord(*a, s ? s : ctx->stream);
 }
 
 static void
-prof_end (gdp_ctx *ctx, int id, cudaEvent_t a) {
+prof_end (gdp_ctx *ctx, int id, cudaEvent_t a, cudaStream_t s = nullptr) {
   if (!ctx->profiling) return;
   cudaEvent_t b;
   cudaEventCreate(&b);
-  cudaEventRecord(b, ctx->stream);
+  cudaEventRecord(b, s ? s : ctx->stream);
   ctx->timed.push_back({id, a, b});
 }
 
@@ -267,6 +272,11 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+  for (int k = 0; k < 2; k++) {
+    if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
+    if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   free(ctx->h_tab);
   delete ctx;
 }
@@ -282,7 +292,12 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side[1], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->join_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->join_ev[1], cudaEventDisableTiming) != cudaSuccess) {
     gdp_ctx_destroy(ctx);
     return GDP_ERR_CUDA;
   }
@@ -304,6 +319,8 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   if (w && atol(w) > 0) ctx->wave = atol(w);
   const char *wx = getenv("GDP_WARP_MIN_X");
   if (wx && atoi(wx) > 0) ctx->warp_min_x = atoi(wx);
+  const char *tw = getenv("GDP_TB_WARP");
+  if (tw && *tw) ctx->tb_warp = atoi(tw) != 0;
   *out = ctx;
   return GDP_OK;
 }
@@ -373,7 +390,7 @@ extern "C" int
 gdp_profile_reset (gdp_ctx *ctx) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   prof_collect(ctx);
-  for (int i = 0; i < 64; i++) { ctx->prof_ms[i] = 0; ctx->prof_n[i] = 0; }
+  for (int i = 0; i < 128; i++) { ctx->prof_ms[i] = 0; ctx->prof_n[i] = 0; }
   return GDP_OK;
 }
 
@@ -502,25 +519,48 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   return GDP_OK;
 }
 
-/* Quasi-logarithmic class of v: exact below 16, then 4 classes per octave. */
-static inline int
-qlog (int64_t v) {
-  if (v < 16) return (int) (v < 0 ? 0 : v);
-  const int lg = 63 - __builtin_clzll((unsigned long long) v);
-  return 16 + (lg - 4) * 4 + (int) ((v >> (lg - 2)) & 3);
-}
-
-/* Work bucket of a pair at block height W: pairs of one bucket have the
-   same number of blocks (or nearly, for long pairs) and similar sweep
-   widths, so the threads of a warp step through their blocks and columns
-   together. */
-static inline int
-bucket_of (const gdp_pair_t &p, int W) {
+/* Sort key of a pair's fill inside its kind (22 bits): wider bands first,
+   and inside one band width (lband + uband) more blocks first.  Threads
+   that share the band width and run the same block in lock step are in the
+   same column phase at the same step: the phase of the j-th swept column of
+   a block depends on j and lband + uband only (while the sweep is not cut
+   at column 0 or glength). */
+static inline uint32_t
+work_key (const gdp_pair_t &p, int W) {
   gdp_geom_t g;
   gdp_geom_of(&p, W, &g);
-  const int nblocks = g.X / W + 1;
-  const int width = W - 1 + g.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
-  return std::min(63, qlog(nblocks)) * 32 + std::min(31, qlog(width) / 2);
+  const int nb = std::min(63, g.X / W + 1);
+  const int lb = (p.variant == GDP_FULL) ? p.lband : 0;
+  const int band = std::min(255, lb + g.band_hi);
+  return (uint32_t) (255 - band) << 14 | (uint32_t) (63 - nb) << 8 | (uint32_t) std::min(255, lb);
+}
+
+/* Kinds whose warps are padded to pairs of one band width: the 16-bit
+   one-thread-per-pair fills, which run phase-specialised columns. */
+static inline bool
+padded_kind (int k) {
+  return k < NTHREADKINDS && ((k >> 2) / 3) == 0;
+}
+
+/* LSD radix sort of (key, value) by the low `bits` bits of key, 10 bits
+   per pass. */
+static void
+radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int bits) {
+  const size_t n = key.size();
+  std::vector<uint32_t> k2(n);
+  std::vector<int32_t> v2(n);
+  for (int shift = 0; shift < bits; shift += 10) {
+    size_t cnt[1025] = {0};
+    for (size_t i = 0; i < n; i++) cnt[((key[i] >> shift) & 1023u) + 1]++;
+    for (int d = 0; d < 1024; d++) cnt[d + 1] += cnt[d];
+    for (size_t i = 0; i < n; i++) {
+      const size_t at = cnt[(key[i] >> shift) & 1023u]++;
+      k2[at] = key[i];
+      v2[at] = val[i];
+    }
+    key.swap(k2);
+    val.swap(v2);
+  }
 }
 
 /* Fills ph for pairs[0..n) (pinned host buffers).  arena_bytes < 0 skips the
@@ -537,9 +577,11 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   gdp_meta_t *meta = ph.meta.as<gdp_meta_t>();
   int32_t *status = ph.status.as<int32_t>();
   int64_t *rec_off = ph.rec_off.as<int64_t>();
-  /* counting sort by (kind, work bucket) */
-  std::vector<int64_t> cnt((size_t) NKINDS * NBUCKETS, 0);
-  std::vector<uint32_t> key1(n, 0xffffffffu), key2(n, 0xffffffffu);
+  /* fill entries (kind << 22 | work key, pair), sorted below */
+  std::vector<uint32_t> keys;
+  std::vector<int32_t> vals;
+  keys.reserve(n);
+  vals.reserve(n);
   int64_t words = 0, recs = 0, ntb = 0, nwindow = 0;
   int maxY[NKINDS] = {0};
   for (int64_t i = 0; i < n; i++) {
@@ -563,7 +605,11 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
       if (!rerun && g16.X >= ctx->warp_min_x) {
         if (sweep <= ctx->warp_max_sweep) {
-          k = warp_kind_id(p.variant, late);
+          /* the smallest lane group whose blocks do not overlap in time */
+          int kg = 2;
+          for (int q = 0; q < 2; q++)
+            if (sweep <= WARP_K[q] * 17 - 48) { kg = q; break; }
+          k = warp_kind_id(p.variant, late, kg);
         } else {
           /* enough lanes that a lane's next block starts after its last one ends */
           for (int nwi = 0; nwi < 4; nwi++) {
@@ -573,8 +619,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       }
       m.dir16 = words;
       words += (w + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
-      key1[i] = (uint32_t) (k * NBUCKETS + bucket_of(p, 16));
-      cnt[key1[i]]++;
+      keys.push_back((uint32_t) k << 22 | work_key(p, 16));
+      vals.push_back((int32_t) i);
       maxY[k] = std::max(maxY[k], Y);
     }
     if (p.precision == 8) {
@@ -582,8 +628,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
       m.dir8 = words;
       words += (w + 3) & ~(int64_t) 3;
-      key2[i] = (uint32_t) (k * NBUCKETS + bucket_of(p, 32));
-      cnt[key2[i]]++;
+      keys.push_back((uint32_t) k << 22 | work_key(p, 32));
+      vals.push_back((int32_t) i);
       maxY[k] = std::max(maxY[k], Y);
     }
     if (p.flags & GDP_FLAG_TRACEBACK) {
@@ -592,33 +638,37 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       ntb++;
     }
   }
-  /* offsets: kinds in order, heaviest bucket first inside a kind */
-  static_assert(NKINDS * NBUCKETS < (1 << 30), "bucket keys fit in 32 bits");
-  std::vector<int64_t> at((size_t) NKINDS * NBUCKETS, 0);
+  static_assert(NKINDS < (1 << 9), "kind ids fit above the 22-bit work key");
+  radix_sort(keys, vals, 31);
+  /* padded kinds: every band-width group starts a warp (-1 = no pair) */
+  int64_t groups = 0;
+  for (size_t i = 0; i < keys.size(); i++) {
+    const bool group_end = (i + 1 == keys.size()) || (keys[i + 1] >> 14) != (keys[i] >> 14);
+    if (group_end && padded_kind((int) (keys[i] >> 22))) groups++;
+  }
+  e = ph.lists.ensure((size_t) std::max<int64_t>((int64_t) keys.size() + 31 * groups + ntb, 1) * sizeof(int32_t));
+  if (e != cudaSuccess) return set_err(ctx, "pinned plan lists", e);
+  int32_t *lists = ph.lists.as<int32_t>();
   int64_t pos = 0;
+  size_t ei = 0;
   for (int k = 0; k < NKINDS; k++) {
     ph.start[k] = pos;
-    int64_t c = 0;
-    for (int b = NBUCKETS - 1; b >= 0; b--) {
-      at[(size_t) k * NBUCKETS + b] = pos;
-      pos += cnt[(size_t) k * NBUCKETS + b];
-      c += cnt[(size_t) k * NBUCKETS + b];
+    while (ei < keys.size() && (int) (keys[ei] >> 22) == k) {
+      lists[pos++] = vals[ei];
+      const bool group_end = (ei + 1 == keys.size()) || (keys[ei + 1] >> 14) != (keys[ei] >> 14);
+      if (group_end && padded_kind(k))
+        while ((pos - ph.start[k]) & 31) lists[pos++] = -1;
+      ei++;
     }
-    ph.counts[k] = (int32_t) c;
+    ph.counts[k] = (int32_t) (pos - ph.start[k]);
     ph.maxY[k] = maxY[k];
   }
   ph.start[NKINDS] = pos;
   ph.counts[NKINDS] = (int32_t) ntb;
-  int64_t tbpos = pos;
-  pos += ntb;
+  for (int64_t i = 0; i < n; i++)
+    if (status[i] == GDP_OK && (pairs[i].flags & GDP_FLAG_TRACEBACK)) lists[pos++] = (int32_t) i;
   ph.start[NKINDS + 1] = pos;
   ph.nlists = pos;
-  int32_t *lists = ph.lists.as<int32_t>();
-  for (int64_t i = 0; i < n; i++) {
-    if (key1[i] != 0xffffffffu) lists[at[key1[i]]++] = (int32_t) i;
-    if (key2[i] != 0xffffffffu) lists[at[key2[i]]++] = (int32_t) i;
-    if (status[i] == GDP_OK && (pairs[i].flags & GDP_FLAG_TRACEBACK)) lists[tbpos++] = (int32_t) i;
-  }
   ph.dir_words = words;
   ph.total_recs = recs;
   ph.nwindow = nwindow;
@@ -754,10 +804,11 @@ fill_grid (gdp_ctx *ctx, int64_t count) {
   return (int) std::max<int64_t>(1, std::min<int64_t>((count + 127) / 128, (int64_t) ctx->nsm * 16));
 }
 
-/* warp kinds: one warp per pair, 4 pairs per block of 128 */
+/* warp kinds: K lanes per pair, 128 / K pairs per block of 128 */
 static inline int
-warp_grid (gdp_ctx *ctx, int64_t count) {
-  return (int) std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t) ctx->nsm * 16));
+warp_grid (gdp_ctx *ctx, int64_t count, int K) {
+  const int per_block = 128 / K;
+  return (int) std::max<int64_t>(1, std::min<int64_t>((count + per_block - 1) / per_block, (int64_t) ctx->nsm * 16));
 }
 
 template <int V, bool L>
@@ -778,19 +829,21 @@ launch_cta_kind (int k, FillParams P, int grid, cudaStream_t s) {
   else { if (late) launch_cta<GDP_LOWER, true>(nwi, P, grid, s); else launch_cta<GDP_LOWER, false>(nwi, P, grid, s); }
 }
 
+template <int V, bool L>
+static void launch_warp (int kg, FillParams P, int grid, cudaStream_t s) {
+  switch (WARP_K[kg]) {
+  case 8: fill_warp_kernel<V, L, 8><<<grid, 128, 0, s>>>(P); break;
+  case 16: fill_warp_kernel<V, L, 16><<<grid, 128, 0, s>>>(P); break;
+  default: fill_warp_kernel<V, L, 32><<<grid, 128, 0, s>>>(P); break;
+  }
+}
+
 static void
 launch_warp_kind (int k, FillParams P, int grid, cudaStream_t s) {
-  const int variant = (k - NTHREADKINDS) / 2, late = (k - NTHREADKINDS) & 1;
-  if (variant == GDP_FULL) {
-    if (late) fill_warp_kernel<GDP_FULL, true><<<grid, 128, 0, s>>>(P);
-    else fill_warp_kernel<GDP_FULL, false><<<grid, 128, 0, s>>>(P);
-  } else if (variant == GDP_UPPER) {
-    if (late) fill_warp_kernel<GDP_UPPER, true><<<grid, 128, 0, s>>>(P);
-    else fill_warp_kernel<GDP_UPPER, false><<<grid, 128, 0, s>>>(P);
-  } else {
-    if (late) fill_warp_kernel<GDP_LOWER, true><<<grid, 128, 0, s>>>(P);
-    else fill_warp_kernel<GDP_LOWER, false><<<grid, 128, 0, s>>>(P);
-  }
+  const int c = k - NTHREADKINDS, vl = c / 3, variant = vl / 2, late = vl & 1, kg = c % 3;
+  if (variant == GDP_FULL) { if (late) launch_warp<GDP_FULL, true>(kg, P, grid, s); else launch_warp<GDP_FULL, false>(kg, P, grid, s); }
+  else if (variant == GDP_UPPER) { if (late) launch_warp<GDP_UPPER, true>(kg, P, grid, s); else launch_warp<GDP_UPPER, false>(kg, P, grid, s); }
+  else { if (late) launch_warp<GDP_LOWER, true>(kg, P, grid, s); else launch_warp<GDP_LOWER, false>(kg, P, grid, s); }
 }
 
 /* Enqueues fills and tracebacks of a planned batch on the compute stream.
@@ -825,16 +878,24 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
   CK(ctx, ctx->scratch.ensure(std::max<size_t>(need, 64)));
-  /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs */
+  /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs.
+     The one-warp / one-CTA-per-pair kinds (no scratch) go first, on the
+     two side streams, so that they run beside the one-thread-per-pair
+     kinds, which share the scratch and stay in order on the main stream. */
+  bool forked = false;
+  int side = 0;
+  CK(ctx, cudaEventRecord(ctx->fork_ev, s));
   for (int round = 0; round < 2; round++) {
-    for (int k = 0; k < NKINDS; k++) {
+    for (int kk = 0; kk < NKINDS; kk++) {
+      const int k = (round == 0) ? (kk + NTHREADKINDS) % NKINDS : kk;
       const bool warp = k >= NTHREADKINDS && k < NTHREADKINDS + NWARPKINDS;
       const bool cta = k >= NTHREADKINDS + NWARPKINDS;
       const int w32 = (warp || cta) ? 0 : (k >> 2) / 3, pass = (warp || cta) ? 0 : (k & 1);
       const bool second = (w32 == 1 && pass == 1);
       if ((round == 0) == second || !ph.counts[k]) continue;
       const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], (int64_t) ctx->nsm * 8))
-                           : warp ? warp_grid(ctx, ph.counts[k]) : fill_grid(ctx, ph.counts[k]);
+                           : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
+                                  : fill_grid(ctx, ph.counts[k]);
       FillParams P;
       P.pairs = d_pairs; P.arena = d_arena;
       P.list = pd.lists.as<int32_t>() + ph.start[k];
@@ -862,14 +923,29 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
+      cudaStream_t ks = s;
+      if (warp || cta) {
+        if (!forked) {
+          for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(ctx->side[q], ctx->fork_ev, 0));
+          forked = true;
+        }
+        ks = ctx->side[side];
+        side ^= 1;
+      }
       cudaEvent_t ev = nullptr;
-      prof_begin(ctx, &ev);
-      if (cta) launch_cta_kind(k, P, grid, s);
-      else if (warp) launch_warp_kind(k, P, grid, s);
-      else launch_kind(k, P, grid, s);
-      prof_end(ctx, k, ev);
+      prof_begin(ctx, &ev, ks);
+      if (cta) launch_cta_kind(k, P, grid, ks);
+      else if (warp) launch_warp_kind(k, P, grid, ks);
+      else launch_kind(k, P, grid, ks);
+      prof_end(ctx, k, ev, ks);
       ctx->launches++;
       CK(ctx, cudaGetLastError());
+    }
+  }
+  if (forked) {
+    for (int q = 0; q < 2; q++) {
+      CK(ctx, cudaEventRecord(ctx->join_ev[q], ctx->side[q]));
+      CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
     }
   }
   if (ph.counts[NKINDS] > 0) {
@@ -885,7 +961,12 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     T.tab = ctx->d_tab;
     cudaEvent_t ev = nullptr;
     prof_begin(ctx, &ev);
-    traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, s>>>(T);
+    if (ctx->tb_warp) {
+      const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, (int64_t) ctx->nsm * 16));
+      traceback_warp_kernel<<<g, 128, 0, s>>>(T);
+    } else {
+      traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, s>>>(T);
+    }
     prof_end(ctx, PROF_TB, ev);
     ctx->launches++;
     CK(ctx, cudaGetLastError());
@@ -1246,7 +1327,8 @@ gdpi_traceback_one (gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const char 
   T.genome_base = gbase;
   T.genome_len = glen;
   T.tab = ctx->d_tab;
-  traceback_kernel<<<1, 32, 0, s>>>(T);
+  if (ctx->tb_warp) traceback_warp_kernel<<<1, 32, 0, s>>>(T);
+  else traceback_kernel<<<1, 32, 0, s>>>(T);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   CK(ctx, cudaMemcpyAsync(res, f->dres.p, sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s));

@@ -176,6 +176,19 @@ def pair_cells(lib, pairs):
     return out
 
 
+def shard_indices(pairs, world, rank):
+    """Pair indices of `rank`'s shard when a batch is spread over `world`
+    GPUs.  Pairs are independent, so a shard is any subset; to balance the
+    work, pairs are ranked by in-band cells and dealt out in snake order
+    (0, 1, .., world-1, world-1, .., 0, ...), which keeps the cell totals of
+    the shards within one large pair of each other."""
+    order = np.argsort(-band_cells(pairs), kind="stable")
+    k = np.arange(order.size)
+    turn = k % (2 * world)
+    owner = np.where(turn < world, turn, 2 * world - 1 - turn)
+    return np.sort(order[owner == rank])
+
+
 def band_cells(pairs):
     """In-band cells per pair over the reference's compare domain (same as
     pair_cells), vectorised over the band's diagonals d = r - c."""
@@ -236,7 +249,7 @@ class Context:
         """{kernel name: (total ms, launches)} since the last reset."""
         out = {}
         name = ctypes.create_string_buffer(64)
-        for k in range(64):
+        for k in range(128):
             ms, n = ctypes.c_double(0), ctypes.c_int64(0)
             self.lib.gdp_profile_read(self.h, k, name, 64, ctypes.byref(ms), ctypes.byref(n))
             if n.value:

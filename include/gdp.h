@@ -215,7 +215,7 @@ void *gdp_ctx_stream(gdp_ctx *ctx);
 /*
  * Per-kernel timing.  While enabled, every kernel launch of the context is
  * bracketed by CUDA events on its stream.  gdp_profile_read(ctx, id, ...)
- * returns, for kernel id 0..63 (the fill kinds first, then the traceback,
+ * returns, for kernel id 0..127 (the fill kinds first, then the traceback,
  * result initialisation, integer-rate probe, rerun-list compaction, record
  * compaction and window extraction; unused ids have an empty name), its
  * name, total device milliseconds and launch count since the last reset.
