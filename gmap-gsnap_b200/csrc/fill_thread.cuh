@@ -432,9 +432,13 @@ column_steady (const PairView &v, int xlo, int y) {
 }
 
 /* Steady columns take block_column_steady in the one-thread-per-pair
-   16-bit fills (0 switches that off). */
+   16-bit fills (GDP_STEADY) and 8-bit fills (GDP_STEADY8); 0 switches it
+   off. */
 #ifndef GDP_STEADY
 #define GDP_STEADY 1
+#endif
+#ifndef GDP_STEADY8
+#define GDP_STEADY8 0
 #endif
 
 #ifndef GDP_FILL_MINB
@@ -501,10 +505,11 @@ fill_thread_kernel (FillParams P) {
         bot_prev = above.x;
         int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
         int2 out;
-        if constexpr (W == 16 && MODE != 2 && GDP_STEADY) {
-          if (hd == nullptr && B.last == W - 1 && y >= 1 && y != v.g.Y && column_steady<W, VARIANT, MODE>(v, xlo, y))
+        if constexpr ((W == 16 && MODE != 2 && GDP_STEADY) || (W == 32 && GDP_STEADY8)) {
+          if (hd == nullptr && B.last == W - 1 && y >= 1 && y != v.g.Y && column_steady<W, VARIANT, MODE>(v, xlo, y)) {
             out = block_column_steady<W, VARIANT, LATE, MODE>(B, v, diag, above, ka, kb, dcol, vmax);
-          else
+            if (MODE == 2 && vmax >= 127) reached = true;
+          } else
             out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
                                                        final_score);
         } else {

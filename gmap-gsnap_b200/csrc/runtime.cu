@@ -34,6 +34,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -133,6 +134,11 @@ struct PlanDev {
 struct gdp_plan {
   PlanHost h;
   PlanDev d;
+  /* optional CUDA graph of the plan's launches for one set of device pointers */
+  bool use_graph = false;
+  cudaGraphExec_t gexec = nullptr;
+  const void *gkey[4] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t glaunches = 0;
 };
 
 /* One in-flight wave of gdp_align_batch. */
@@ -163,6 +169,8 @@ struct gdp_ctx {
   int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
   int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
   bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
+  int group_slack = 48;     /* lane groups of K lanes take sweeps up to 17 K - group_slack columns */
+  int plan_threads = 8;     /* host threads of the planner */
   DevBuf arena, scratch;
   Slot slot[2];
   std::atomic<int64_t> launches{0};
@@ -319,6 +327,9 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   if (w && atol(w) > 0) ctx->wave = atol(w);
   const char *wx = getenv("GDP_WARP_MIN_X");
   if (wx && atoi(wx) > 0) ctx->warp_min_x = atoi(wx);
+  ctx->plan_threads = (int) std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const char *pt = getenv("GDP_PLAN_THREADS");
+  if (pt && atoi(pt) > 0) ctx->plan_threads = atoi(pt);
   const char *tw = getenv("GDP_TB_WARP");
   if (tw && *tw) ctx->tb_warp = atoi(tw) != 0;
   *out = ctx;
@@ -519,7 +530,7 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   return GDP_OK;
 }
 
-/* Sort key of a pair's fill inside its kind (22 bits): wider bands first,
+/* Sort key of a pair's fill inside its kind (14 bits): wider bands first,
    and inside one band width (lband + uband) more blocks first.  Threads
    that share the band width and run the same block in lock step are in the
    same column phase at the same step: the phase of the j-th swept column of
@@ -532,8 +543,10 @@ work_key (const gdp_pair_t &p, int W) {
   const int nb = std::min(63, g.X / W + 1);
   const int lb = (p.variant == GDP_FULL) ? p.lband : 0;
   const int band = std::min(255, lb + g.band_hi);
-  return (uint32_t) (255 - band) << 14 | (uint32_t) (63 - nb) << 8 | (uint32_t) std::min(255, lb);
+  return (uint32_t) (255 - band) << 6 | (uint32_t) (63 - nb);
 }
+#define KEY_KIND_SHIFT 14   /* sort key = kind << 14 | work key */
+#define KEY_GROUP_SHIFT 6   /* entries with equal key >> 6 share kind and band width */
 
 /* Kinds whose warps are padded to pairs of one band width: the 16-bit
    one-thread-per-pair fills, which run phase-specialised columns. */
@@ -542,22 +555,52 @@ padded_kind (int k) {
   return k < NTHREADKINDS && ((k >> 2) / 3) == 0;
 }
 
-/* LSD radix sort of (key, value) by the low `bits` bits of key, 10 bits
-   per pass. */
+/* Runs f(lo, hi, t) over [0, n) split into `nt` contiguous chunks, one
+   host thread per chunk. */
+template <class F>
 static void
-radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int bits) {
-  const size_t n = key.size();
+parallel_chunks (int64_t n, int nt, F f) {
+  if (nt <= 1) { f((int64_t) 0, n, 0); return; }
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 0; t < nt; t++) {
+    const int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
+    th.emplace_back([=, &f] { f(lo, hi, t); });
+  }
+  for (auto &x : th) x.join();
+}
+
+/* Stable LSD radix sort of (key, value) by the low 22 bits of key, 11 bits
+   per pass, `nt` host threads (per-thread histograms, then each thread
+   scatters its own chunk in order). */
+static void
+radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int nt) {
+  const int64_t n = (int64_t) key.size();
   std::vector<uint32_t> k2(n);
   std::vector<int32_t> v2(n);
-  for (int shift = 0; shift < bits; shift += 10) {
-    size_t cnt[1025] = {0};
-    for (size_t i = 0; i < n; i++) cnt[((key[i] >> shift) & 1023u) + 1]++;
-    for (int d = 0; d < 1024; d++) cnt[d + 1] += cnt[d];
-    for (size_t i = 0; i < n; i++) {
-      const size_t at = cnt[(key[i] >> shift) & 1023u]++;
-      k2[at] = key[i];
-      v2[at] = val[i];
-    }
+  constexpr int B = 2048;
+  std::vector<int64_t> hist((size_t) nt * B);
+  for (int shift = 0; shift < 22; shift += 11) {
+    std::fill(hist.begin(), hist.end(), 0);
+    parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+      int64_t *h = hist.data() + (size_t) t * B;
+      for (int64_t i = lo; i < hi; i++) h[(key[i] >> shift) & (B - 1)]++;
+    });
+    int64_t sum = 0;
+    for (int d = 0; d < B; d++)
+      for (int t = 0; t < nt; t++) {
+        const int64_t c = hist[(size_t) t * B + d];
+        hist[(size_t) t * B + d] = sum;
+        sum += c;
+      }
+    parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+      int64_t *h = hist.data() + (size_t) t * B;
+      for (int64_t i = lo; i < hi; i++) {
+        const int64_t at = h[(key[i] >> shift) & (B - 1)]++;
+        k2[at] = key[i];
+        v2[at] = val[i];
+      }
+    });
     key.swap(k2);
     val.swap(v2);
   }
@@ -572,91 +615,123 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   if (e == cudaSuccess) e = ph.meta.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_meta_t));
   if (e == cudaSuccess) e = ph.status.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
   if (e == cudaSuccess) e = ph.rec_off.ensure(std::max<int64_t>(n, 1) * sizeof(int64_t));
-  if (e == cudaSuccess) e = ph.lists.ensure(std::max<int64_t>(3 * n, 1) * sizeof(int32_t));
   if (e != cudaSuccess) return set_err(ctx, "pinned plan buffers", e);
   gdp_meta_t *meta = ph.meta.as<gdp_meta_t>();
   int32_t *status = ph.status.as<int32_t>();
   int64_t *rec_off = ph.rec_off.as<int64_t>();
-  /* fill entries (kind << 22 | work key, pair), sorted below */
-  std::vector<uint32_t> keys;
-  std::vector<int32_t> vals;
-  keys.reserve(n);
-  vals.reserve(n);
-  int64_t words = 0, recs = 0, ntb = 0, nwindow = 0;
-  int maxY[NKINDS] = {0};
-  for (int64_t i = 0; i < n; i++) {
-    const gdp_pair_t &p = pairs[i];
-    gdp_meta_t &m = meta[i];
-    m.dir16 = m.dir8 = -1;
-    m.maxh16 = -32768; m.status8 = 0; m.final8 = 0; m.final16 = 0;
-    rec_off[i] = 0;
-    const int st = validate(p, arena_bytes, ctx->genome_len);
-    if (st == GDP_OK && (p.flags & GDP_FLAG_GWINDOW)) nwindow++;
-    status[i] = st;
-    if (st != GDP_OK) continue;
-    const int late = (p.flags & GDP_FLAG_JUMP_LATE) ? 1 : 0;
-    const bool rerun = p.precision == 8 && (p.flags & GDP_FLAG_RERUN16);
-    const int Y = (p.variant == GDP_LOWER) ? p.rlength : p.glength;
-    if (p.precision == 16 || rerun) {
-      const int64_t w = gdp_pair_words(&p, 16);
-      gdp_geom_t g16;
-      gdp_geom_of(&p, 16, &g16);
-      const int sweep = 15 + g16.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
-      int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
-      if (!rerun && g16.X >= ctx->warp_min_x) {
-        if (sweep <= ctx->warp_max_sweep) {
-          /* the smallest lane group whose blocks do not overlap in time */
-          int kg = 2;
-          for (int q = 0; q < 2; q++)
-            if (sweep <= WARP_K[q] * 17 - 48) { kg = q; break; }
-          k = warp_kind_id(p.variant, late, kg);
-        } else {
-          /* enough lanes that a lane's next block starts after its last one ends */
-          for (int nwi = 0; nwi < 4; nwi++) {
-            if (sweep + 16 < CTA_NW[nwi] * 32 * 17 - 16) { k = cta_kind_id(p.variant, late, nwi); break; }
+  const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, n / 8192));
+  /* per chunk: sums of direction words, record slots, fill entries,
+     tracebacks, device windows, and the largest swept dimension per kind */
+  struct Chunk { int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0; int maxY[NKINDS] = {0}; };
+  std::vector<Chunk> ch(nt);
+  std::vector<uint32_t> k16(n), k8(n);   /* fill keys of each pair (~0u: none) */
+  const uint64_t glen = ctx->genome_len;
+  /* pass 1: validate, route, size (meta.dir16 / dir8 and rec_off hold sizes) */
+  parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+    Chunk &c = ch[t];
+    for (int64_t i = lo; i < hi; i++) {
+      const gdp_pair_t &p = pairs[i];
+      gdp_meta_t &m = meta[i];
+      m.dir16 = m.dir8 = -1;
+      m.maxh16 = -32768; m.status8 = 0; m.final8 = 0; m.final16 = 0;
+      rec_off[i] = 0;
+      k16[i] = k8[i] = ~0u;
+      const int st = validate(p, arena_bytes, glen);
+      status[i] = st;
+      if (st != GDP_OK) continue;
+      if (p.flags & GDP_FLAG_GWINDOW) c.nwindow++;
+      const int late = (p.flags & GDP_FLAG_JUMP_LATE) ? 1 : 0;
+      const bool rerun = p.precision == 8 && (p.flags & GDP_FLAG_RERUN16);
+      const int Y = (p.variant == GDP_LOWER) ? p.rlength : p.glength;
+      if (p.precision == 16 || rerun) {
+        gdp_geom_t g16;
+        gdp_geom_of(&p, 16, &g16);
+        const int sweep = 15 + g16.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
+        int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
+        if (!rerun && g16.X >= ctx->warp_min_x) {
+          if (sweep <= ctx->warp_max_sweep) {
+            /* the smallest lane group whose blocks do not overlap in time */
+            int kg = 2;
+            for (int q = 0; q < 2; q++)
+              if (sweep <= WARP_K[q] * 17 - ctx->group_slack) { kg = q; break; }
+            k = warp_kind_id(p.variant, late, kg);
+          } else {
+            /* enough lanes that a lane's next block starts after its last one ends */
+            for (int nwi = 0; nwi < 4; nwi++) {
+              if (sweep + 16 < CTA_NW[nwi] * 32 * 17 - 16) { k = cta_kind_id(p.variant, late, nwi); break; }
+            }
           }
         }
+        m.dir16 = (gdp_pair_words(&p, 16) + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
+        c.words += m.dir16;
+        k16[i] = (uint32_t) k << KEY_KIND_SHIFT | work_key(p, 16);
+        c.entries++;
+        c.maxY[k] = std::max(c.maxY[k], Y);
       }
-      m.dir16 = words;
-      words += (w + 3) & ~(int64_t) 3;   /* keep pairs 16-byte aligned */
-      keys.push_back((uint32_t) k << 22 | work_key(p, 16));
-      vals.push_back((int32_t) i);
-      maxY[k] = std::max(maxY[k], Y);
+      if (p.precision == 8) {
+        const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
+        m.dir8 = (gdp_pair_words(&p, 32) + 3) & ~(int64_t) 3;
+        c.words += m.dir8;
+        k8[i] = (uint32_t) k << KEY_KIND_SHIFT | work_key(p, 32);
+        c.entries++;
+        c.maxY[k] = std::max(c.maxY[k], Y);
+      }
+      if (p.flags & GDP_FLAG_TRACEBACK) {
+        rec_off[i] = (int64_t) p.rlength + p.glength + 2;
+        c.recs += rec_off[i];
+        c.ntb++;
+      }
     }
-    if (p.precision == 8) {
-      const int64_t w = gdp_pair_words(&p, 32);
-      const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
-      m.dir8 = words;
-      words += (w + 3) & ~(int64_t) 3;
-      keys.push_back((uint32_t) k << 22 | work_key(p, 32));
-      vals.push_back((int32_t) i);
-      maxY[k] = std::max(maxY[k], Y);
-    }
-    if (p.flags & GDP_FLAG_TRACEBACK) {
-      rec_off[i] = recs;
-      recs += (int64_t) p.rlength + p.glength + 2;
-      ntb++;
-    }
+  });
+  /* chunk bases */
+  std::vector<int64_t> wbase(nt), rbase(nt), ebase(nt), tbase(nt);
+  int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0;
+  int maxY[NKINDS] = {0};
+  for (int t = 0; t < nt; t++) {
+    wbase[t] = words; rbase[t] = recs; ebase[t] = entries; tbase[t] = ntb;
+    words += ch[t].words; recs += ch[t].recs; entries += ch[t].entries; ntb += ch[t].ntb;
+    nwindow += ch[t].nwindow;
+    for (int k = 0; k < NKINDS; k++) maxY[k] = std::max(maxY[k], ch[t].maxY[k]);
   }
-  static_assert(NKINDS < (1 << 9), "kind ids fit above the 22-bit work key");
-  radix_sort(keys, vals, 31);
+  /* pass 2: sizes to offsets, fill entries in pair order */
+  std::vector<uint32_t> keys(entries);
+  std::vector<int32_t> vals(entries);
+  std::vector<int32_t> tbl(ntb);
+  parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+    int64_t w = wbase[t], r = rbase[t], en = ebase[t], tb = tbase[t];
+    for (int64_t i = lo; i < hi; i++) {
+      if (status[i] != GDP_OK) continue;
+      gdp_meta_t &m = meta[i];
+      if (m.dir16 >= 0) { const int64_t sz = m.dir16; m.dir16 = w; w += sz; }
+      if (m.dir8 >= 0) { const int64_t sz = m.dir8; m.dir8 = w; w += sz; }
+      if (k16[i] != ~0u) { keys[en] = k16[i]; vals[en] = (int32_t) i; en++; }
+      if (k8[i] != ~0u) { keys[en] = k8[i]; vals[en] = (int32_t) i; en++; }
+      if (pairs[i].flags & GDP_FLAG_TRACEBACK) {
+        const int64_t sz = rec_off[i];
+        rec_off[i] = r;
+        r += sz;
+        tbl[tb++] = (int32_t) i;
+      }
+    }
+  });
+  static_assert(NKINDS < (1 << (22 - KEY_KIND_SHIFT)), "kind ids fit in the 22-bit sort key");
+  radix_sort(keys, vals, nt);
   /* padded kinds: every band-width group starts a warp (-1 = no pair) */
   int64_t groups = 0;
-  for (size_t i = 0; i < keys.size(); i++) {
-    const bool group_end = (i + 1 == keys.size()) || (keys[i + 1] >> 14) != (keys[i] >> 14);
-    if (group_end && padded_kind((int) (keys[i] >> 22))) groups++;
+  for (int64_t i = 0; i < entries; i++) {
+    const bool group_end = (i + 1 == entries) || (keys[i + 1] >> KEY_GROUP_SHIFT) != (keys[i] >> KEY_GROUP_SHIFT);
+    if (group_end && padded_kind((int) (keys[i] >> KEY_KIND_SHIFT))) groups++;
   }
-  e = ph.lists.ensure((size_t) std::max<int64_t>((int64_t) keys.size() + 31 * groups + ntb, 1) * sizeof(int32_t));
+  e = ph.lists.ensure((size_t) std::max<int64_t>(entries + 31 * groups + ntb, 1) * sizeof(int32_t));
   if (e != cudaSuccess) return set_err(ctx, "pinned plan lists", e);
   int32_t *lists = ph.lists.as<int32_t>();
-  int64_t pos = 0;
-  size_t ei = 0;
+  int64_t pos = 0, ei = 0;
   for (int k = 0; k < NKINDS; k++) {
     ph.start[k] = pos;
-    while (ei < keys.size() && (int) (keys[ei] >> 22) == k) {
+    const bool pad = padded_kind(k);
+    while (ei < entries && (int) (keys[ei] >> KEY_KIND_SHIFT) == k) {
       lists[pos++] = vals[ei];
-      const bool group_end = (ei + 1 == keys.size()) || (keys[ei + 1] >> 14) != (keys[ei] >> 14);
-      if (group_end && padded_kind(k))
+      if (pad && ((ei + 1 == entries) || (keys[ei + 1] >> KEY_GROUP_SHIFT) != (keys[ei] >> KEY_GROUP_SHIFT)))
         while ((pos - ph.start[k]) & 31) lists[pos++] = -1;
       ei++;
     }
@@ -665,8 +740,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   }
   ph.start[NKINDS] = pos;
   ph.counts[NKINDS] = (int32_t) ntb;
-  for (int64_t i = 0; i < n; i++)
-    if (status[i] == GDP_OK && (pairs[i].flags & GDP_FLAG_TRACEBACK)) lists[pos++] = (int32_t) i;
+  if (ntb > 0) memcpy(lists + pos, tbl.data(), ntb * sizeof(int32_t));
+  pos += ntb;
   ph.start[NKINDS + 1] = pos;
   ph.nlists = pos;
   ph.dir_words = words;
@@ -705,6 +780,7 @@ plan_upload (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, bool hdump, cudaStre
 extern "C" void
 gdp_plan_destroy (gdp_plan *pl) {
   if (!pl) return;
+  if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
   pl->d.release();
   pl->h.release();
   delete pl;
@@ -1007,7 +1083,145 @@ gdp_plan_execute (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *d_pairs, const c
                   gdp_result_t *d_results, gdp_rec_t *d_recs) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  return plan_run(ctx, pl->h, pl->d, d_pairs, d_arena, d_results, d_recs);
+  if (!pl->use_graph || ctx->profiling) return plan_run(ctx, pl->h, pl->d, d_pairs, d_arena, d_results, d_recs);
+  const void *key[4] = {d_pairs, d_arena, d_results, d_recs};
+  if (pl->gexec && memcmp(key, pl->gkey, sizeof(key)) == 0) {
+    CK(ctx, cudaGraphLaunch(pl->gexec, ctx->stream));
+    ctx->launches += pl->glaunches;
+    return GDP_OK;
+  }
+  /* run once (this call's work; it also sizes every buffer), then capture
+     the same launches for the next calls with these pointers */
+  const int64_t l0 = ctx->launches;
+  int rc = plan_run(ctx, pl->h, pl->d, d_pairs, d_arena, d_results, d_recs);
+  if (rc != GDP_OK) return rc;
+  const int64_t nl = ctx->launches - l0;
+  if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; }
+  cudaGraph_t g = nullptr;
+  CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  rc = plan_run(ctx, pl->h, pl->d, d_pairs, d_arena, d_results, d_recs);
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->launches -= nl;   /* captured, not launched */
+  if (rc != GDP_OK) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return set_err(ctx, "plan capture", e);
+  e = cudaGraphInstantiate(&pl->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { pl->gexec = nullptr; return set_err(ctx, "plan graph", e); }
+  memcpy(pl->gkey, key, sizeof(key));
+  pl->glaunches = nl;
+  return GDP_OK;
+}
+
+extern "C" int
+gdp_plan_use_graph (gdp_plan *pl, int on) {
+  if (pl == nullptr) return GDP_ERR_PARAM;
+  pl->use_graph = on != 0;
+  if (!pl->use_graph && pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; }
+  return GDP_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* Tunable routing parameters and the autotuner                        */
+/* ------------------------------------------------------------------ */
+
+extern "C" int
+gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
+  if (ctx == nullptr || name == nullptr) return GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!strcmp(name, "warp_min_x") && value >= 1) ctx->warp_min_x = (int) value;
+  else if (!strcmp(name, "warp_max_sweep") && value >= 1) ctx->warp_max_sweep = (int) std::min<int64_t>(value, 32 * 17 - 16);
+  else if (!strcmp(name, "group_slack") && value >= 16 && value <= 128) ctx->group_slack = (int) value;
+  else if (!strcmp(name, "tb_warp")) ctx->tb_warp = value != 0;
+  else if (!strcmp(name, "wave_pairs") && value >= 1) ctx->wave = value;
+  else return GDP_ERR_PARAM;
+  return GDP_OK;
+}
+
+extern "C" int
+gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
+  if (ctx == nullptr || name == nullptr || value == nullptr) return GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!strcmp(name, "warp_min_x")) *value = ctx->warp_min_x;
+  else if (!strcmp(name, "warp_max_sweep")) *value = ctx->warp_max_sweep;
+  else if (!strcmp(name, "group_slack")) *value = ctx->group_slack;
+  else if (!strcmp(name, "tb_warp")) *value = ctx->tb_warp ? 1 : 0;
+  else if (!strcmp(name, "wave_pairs")) *value = ctx->wave;
+  else return GDP_ERR_PARAM;
+  return GDP_OK;
+}
+
+/* Device time of one plan execution of a sample under the current routing
+   (best of `reps` after one warm-up), or a negative status. */
+static double
+tune_trial (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const gdp_pair_t *d_pairs, const char *d_arena,
+            gdp_result_t *d_res, DevBuf &recs, int reps) {
+  gdp_plan pl;
+  int rc = plan_build(ctx, pairs, n, -1, pl.h);
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl.h, pl.d, false, ctx->stream);
+  if (rc != GDP_OK) return -rc;
+  if (recs.ensure(std::max<int64_t>(pl.h.total_recs, 1) * sizeof(gdp_rec_t)) != cudaSuccess) return -GDP_ERR_CUDA;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 1e30;
+  for (int r = 0; r <= reps && rc == GDP_OK; r++) {
+    cudaEventRecord(a, ctx->stream);
+    rc = plan_run(ctx, pl.h, pl.d, d_pairs, d_arena, d_res, recs.as<gdp_rec_t>());
+    cudaEventRecord(b, ctx->stream);
+    if (cudaEventSynchronize(b) != cudaSuccess) rc = GDP_ERR_CUDA;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (r > 0) best = std::min(best, (double) ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  pl.d.release();
+  pl.h.release();
+  return rc == GDP_OK ? best : -rc;
+}
+
+extern "C" int
+gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char *arena, int64_t arena_bytes,
+              double *best_ms) {
+  if (ctx == nullptr || pairs == nullptr || npairs <= 0 || arena == nullptr || arena_bytes <= 0) return GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const bool prof = ctx->profiling;
+  ctx->profiling = false;
+  DevBuf dp, da, dr, drec;
+  CK(ctx, dp.ensure(npairs * sizeof(gdp_pair_t)));
+  CK(ctx, da.ensure(arena_bytes));
+  CK(ctx, dr.ensure(npairs * sizeof(gdp_result_t)));
+  CK(ctx, cudaMemcpyAsync(dp.p, pairs, npairs * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(da.p, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  /* coordinate descent over the routing knobs, each from a small set */
+  struct Knob { int *v; std::vector<int> cand; };
+  int tbw = ctx->tb_warp ? 1 : 0;
+  std::vector<Knob> knobs = {
+    {&ctx->warp_min_x, {128, 256, 512, 1024, 2048, 1 << 30}},
+    {&ctx->group_slack, {16, 32, 48, 80}},
+    {&ctx->warp_max_sweep, {272, 400, 496, 528}},
+    {&tbw, {1, 0}},
+  };
+  double best = tune_trial(ctx, pairs, npairs, dp.as<gdp_pair_t>(), da.as<char>(), dr.as<gdp_result_t>(), drec, 2);
+  int rc = best < 0 ? (int) -best : GDP_OK;
+  for (size_t k = 0; k < knobs.size() && rc == GDP_OK; k++) {
+    const int keep = *knobs[k].v;
+    int choice = keep;
+    for (int c : knobs[k].cand) {
+      if (c == keep) continue;
+      *knobs[k].v = c;
+      ctx->tb_warp = tbw != 0;
+      const double t = tune_trial(ctx, pairs, npairs, dp.as<gdp_pair_t>(), da.as<char>(), dr.as<gdp_result_t>(), drec, 2);
+      if (t < 0) { rc = (int) -t; break; }
+      if (t < best * 0.98) { best = t; choice = c; }
+    }
+    *knobs[k].v = choice;
+    ctx->tb_warp = tbw != 0;
+  }
+  ctx->profiling = prof;
+  if (best_ms) *best_ms = best;
+  return rc;
 }
 
 /* ------------------------------------------------------------------ */

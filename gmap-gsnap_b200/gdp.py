@@ -77,6 +77,10 @@ def load(path=LIB_PATH):
     lib.gdp_plan_dir_bytes.argtypes = [vp]
     lib.gdp_plan_dir_bytes.restype = i64
     lib.gdp_plan_destroy.argtypes = [vp]
+    lib.gdp_plan_use_graph.argtypes = [vp, i32]
+    lib.gdp_ctx_set_param.argtypes = [vp, ctypes.c_char_p, i64]
+    lib.gdp_ctx_get_param.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i64)]
+    lib.gdp_autotune.argtypes = [vp, vp, i64, vp, i64, ctypes.POINTER(ctypes.c_double)]
     lib.gdp_sync.argtypes = [vp]
     lib.gdp_debug_tables.argtypes = [i32, vp, vp, vp]
     lib.gdp_ctx_stream.argtypes = [vp]
@@ -255,6 +259,28 @@ class Context:
             if n.value:
                 out[name.value.decode()] = (ms.value, n.value)
         return out
+
+    def set_param(self, name, value):
+        rc = self.lib.gdp_ctx_set_param(self.h, name.encode(), int(value))
+        if rc != 0:
+            raise ValueError(f"gdp_ctx_set_param({name}, {value}): {STATUS.get(rc, rc)}")
+
+    def get_param(self, name):
+        v = ctypes.c_int64(0)
+        rc = self.lib.gdp_ctx_get_param(self.h, name.encode(), ctypes.byref(v))
+        if rc != 0:
+            raise ValueError(f"gdp_ctx_get_param({name}): {STATUS.get(rc, rc)}")
+        return v.value
+
+    def autotune(self, pairs, arena):
+        """Tunes the routing parameters on a sample batch; returns
+        (parameters, best device ms of the sample)."""
+        best = ctypes.c_double(0)
+        rc = self.lib.gdp_autotune(self.h, _ptr(pairs), pairs.size, _ptr(arena), arena.size, ctypes.byref(best))
+        if rc != 0:
+            raise RuntimeError(f"gdp_autotune: {STATUS.get(rc, rc)} {self.error()}")
+        names = ("warp_min_x", "warp_max_sweep", "group_slack", "tb_warp")
+        return {k: self.get_param(k) for k in names}, best.value
 
     def int_peak(self):
         return float(self.lib.gdp_measure_int_peak(self.h))

@@ -186,6 +186,34 @@ int64_t gdp_plan_rec_offset(const gdp_plan *plan, int64_t i);
 int64_t gdp_plan_dir_bytes(const gdp_plan *plan);
 void gdp_plan_destroy(gdp_plan *plan);
 
+/*
+ * With on != 0, gdp_plan_execute runs the plan's launches as one CUDA
+ * graph: the first call with a given set of device pointers runs the plan
+ * and captures its launches; later calls with the same pointers launch the
+ * graph.  Calls with profiling enabled run without the graph.
+ */
+int gdp_plan_use_graph(gdp_plan *plan, int on);
+
+/*
+ * Routing parameters of a context (they take effect in later plans):
+ *   "warp_min_x"     pairs with at least this many lanes (query rows; lower:
+ *                    genome columns) go to the lane-group / one-CTA fills
+ *   "warp_max_sweep" widest block sweep a lane group of 32 takes; wider
+ *                    sweeps go one CTA per pair
+ *   "group_slack"    a group of K lanes takes sweeps up to 17 K - slack
+ *   "tb_warp"        1: tracebacks with one warp per pair, 0: one thread
+ *   "wave_pairs"     pairs per wave of gdp_align_batch
+ * gdp_autotune times plan executions of a sample batch (device-resident
+ * copies, the caller's pairs and arena) under candidate values of the first
+ * four, one parameter at a time, and keeps the fastest; *best_ms gets the
+ * sample's device time with the chosen values.  Results never depend on
+ * these parameters.
+ */
+int gdp_ctx_set_param(gdp_ctx *ctx, const char *name, int64_t value);
+int gdp_ctx_get_param(gdp_ctx *ctx, const char *name, int64_t *value);
+int gdp_autotune(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char *arena, int64_t arena_bytes,
+                 double *best_ms);
+
 /* Waits for the context's stream. */
 int gdp_sync(gdp_ctx *ctx);
 
