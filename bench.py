@@ -239,15 +239,16 @@ def per_pair_vs_batched(lib, ctx, seed, npairs=20000, nsample=500):
             "results_identical": bool(same)}
 
 
-def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000):
+def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000,
+                  workers=4):
     """The serving loop under Poisson load: single-pair requests of the
     mixed distribution, genome windows extracted on the device from a
     resident 100 Mbp genome, admission by a 40 GB direction budget."""
     genome, blocks = gdp.make_genome(lib, 4242, 100_000_000)
     pool, arena = gdp.make_resident_pairs(lib, gdp.WL_MIX, seed, genome, pool_size)
     cells = gdp.band_cells(pool)
-    srv = gdp.Server(lib, device=device, workers=2, budget=40 << 30, blocks=blocks, length=genome.size)
-    srv.drive(pool, arena, 100_000, rate=1e6, seed=1)       # warm-up: buffers reach their working sizes
+    srv = gdp.Server(lib, device=device, workers=workers, budget=40 << 30, blocks=blocks, length=genome.size)
+    srv.drive(pool, arena, 300_000, rate=1e6, seed=1)       # warm-up: every worker's buffers reach working size
     rows = []
     for k, rate in enumerate(rates):
         n = int(min(max_requests, max(200, rate * seconds_per_rate)))
@@ -264,7 +265,7 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
                default=None)
     return {"genome": "100 Mbp seeded random, resident (genomecomp, 2-bit + N flags)",
             "requests": "single pairs of the 70/25/5 short/long/cDNA mix, device-extracted windows",
-            "workers": 2, "dir_budget_gb": 40, "sweep": rows, "knee_offered_per_s": knee,
+            "workers": workers, "dir_budget_gb": 40, "sweep": rows, "knee_offered_per_s": knee,
             "batches": st["batches"], "max_batch_pairs": st["max_batch_pairs"],
             "peak_admitted_dir_gb": round(st["peak_reserved_bytes"] / 2**30, 3)}
 

@@ -529,23 +529,26 @@ fill_thread_kernel (FillParams P) {
 }
 
 /*
- * One group of K lanes (K = 8, 16 or 32; 32 / K pairs per warp) per long
- * 16-bit pair (plain fills).  Lane l of a group owns the blocks b = l,
+ * One group of K lanes (K = 4 .. 32; 32 / K pairs per warp) per pair: long
+ * 16-bit pairs (plain fills), and the 8-bit pass of rerun pairs (W = 32,
+ * MODE 2), whose few pairs would leave most of the device idle with one
+ * thread each.  Lane l of a group owns the blocks b = l,
  * l + K, l + 2K, ... and processes column y of block b at step t = y + b:
  * block b needs the final column y (F carry, last lane H) and column y - 1
  * (diagonal) of block b - 1, which the previous lane of the group produced
  * one and two steps earlier, so one rotation shuffle inside the group per
  * step carries them.  A lane's next block starts after its previous one
- * ends as long as a block sweeps fewer than 17 K - 16 columns; the planner
+ * ends as long as a block sweeps fewer than (W + 1) K - 16 columns; the planner
  * picks the smallest K that allows the pair's sweep, so lanes idle between
  * blocks for at most a few steps.  Each lane runs block_column, the same
  * column step as the one-thread-per-pair kernel.
  */
-template <int VARIANT, bool LATE, int K>
-__global__ void __launch_bounds__(128, 4)
+template <int VARIANT, bool LATE, int K, int W = 16, int MODE = 0>
+__global__ void __launch_bounds__(128, (W == 16) ? 4 : 2)
 fill_warp_kernel (FillParams P) {
-  constexpr int W = 16, WORDS = 2, LO = -32768, G = 32 / K;
-  static_assert(K == 8 || K == 16 || K == 32, "group sizes divide the warp");
+  constexpr int WORDS = W / 8, LO = (W == 32) ? -128 : -32768, G = 32 / K;
+  static_assert(K == 4 || K == 8 || K == 16 || K == 32, "group sizes divide the warp");
+  static_assert(MODE == 0 || (MODE == 2 && W == 32), "plain fills, or the 8-bit pass of rerun pairs");
   __shared__ int8_t s_nt2int[128];
   for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
   __syncthreads();
@@ -569,7 +572,7 @@ fill_warp_kernel (FillParams P) {
     gdp_meta_t *mp = valid ? P.meta + pi : nullptr;
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
-    uint32_t *dir = valid ? P.dirs + mp->dir16 : nullptr;
+    uint32_t *dir = valid ? P.dirs + ((W == 16) ? mp->dir16 : mp->dir8) : nullptr;
     /* blocks that sweep something: 0 .. nb - 1 */
     int nb = 0, tend = -1;
     if (valid) {
@@ -618,8 +621,8 @@ fill_warp_kernel (FillParams P) {
           else diag = (b == 0) ? LO : bot_prev;
           uint32_t *dcol = dir + boff + (int64_t) (y - B.y0) * WORDS;
           int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
-          mine = block_column<W, VARIANT, LATE, 0>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
-                                                   final_score);
+          mine = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
+                                                      final_score);
           if (y == B.y1) {
             /* move to block b + K */
             for (int k = b; k < b + K && k < nb; k++) boff += gdp_block_words(&v.g, k * W);
@@ -630,9 +633,12 @@ fill_warp_kernel (FillParams P) {
       }
       bot_prev = rx;
     }
-    /* the lane that owned the final cell's block reports its score */
+    /* the lane that owned the final cell's block reports its score; the
+       8-bit pass also needs whether any lane saw an in-band 127 */
     const int fs = __shfl_sync(0xffffffffu, final_score, group * K + ((v.g.X / W) & (K - 1)));
-    if (valid && glane == 0) fill_finish<W, 0>(P, pi, mp, v.g, false, fs);
+    const unsigned gmask = (K == 32) ? 0xffffffffu : (((1u << K) - 1u) << (group * K));
+    const bool any_reached = (__ballot_sync(0xffffffffu, reached) & gmask) != 0;
+    if (valid && glane == 0) fill_finish<W, MODE>(P, pi, mp, v.g, any_reached, fs);
   }
 }
 

@@ -86,8 +86,12 @@ struct HostBuf {   /* pinned host memory */
 constexpr int NTHREADKINDS = 24;   /* one thread per pair: (W32, variant, late, pass) */
 constexpr int NWARPKINDS = 18;     /* K lanes per pair (16-bit plain): 24 + (variant * 2 + late) * 3 + log2(K) - 3 */
 constexpr int WARP_K[3] = {8, 16, 32};
-constexpr int NCTAKINDS = 24;      /* one CTA per pair (16-bit plain): 30 + (variant * 2 + late) * 4 + log2(NW) - 1 */
-constexpr int NKINDS = NTHREADKINDS + NWARPKINDS + NCTAKINDS;
+constexpr int NWARP8KINDS = 18;    /* K lanes per pair, 8-bit pass of rerun pairs: 42 + (variant * 2 + late) * 3 + log2(K) - 2 */
+constexpr int WARP8_K[3] = {4, 8, 16};
+constexpr int NCTAKINDS = 24;      /* one CTA per pair (16-bit plain): 60 + (variant * 2 + late) * 4 + log2(NW) - 1 */
+constexpr int FIRST_WARP8 = NTHREADKINDS + NWARPKINDS;
+constexpr int FIRST_CTA = FIRST_WARP8 + NWARP8KINDS;
+constexpr int NKINDS = FIRST_CTA + NCTAKINDS;
 constexpr int CTA_NW[4] = {2, 4, 8, 16};
 
 inline int kind_id (int w32, int variant, int late, int pass) {
@@ -98,8 +102,12 @@ inline int warp_kind_id (int variant, int late, int kg) {
   return NTHREADKINDS + (variant * 2 + late) * 3 + kg;
 }
 
+inline int warp8_kind_id (int variant, int late, int kg) {
+  return FIRST_WARP8 + (variant * 2 + late) * 3 + kg;
+}
+
 inline int cta_kind_id (int variant, int late, int nwi) {
-  return NTHREADKINDS + NWARPKINDS + (variant * 2 + late) * 4 + nwi;
+  return FIRST_CTA + (variant * 2 + late) * 4 + nwi;
 }
 
 }  // namespace
@@ -141,7 +149,21 @@ struct gdp_plan {
   int64_t glaunches = 0;
 };
 
-/* One in-flight wave of gdp_align_batch. */
+/* Host-side phase timing of the wave pipeline, compiled in only with
+   -DGDP_HOST_TRACE (a diagnostic build): one line per phase on stderr. */
+#ifdef GDP_HOST_TRACE
+#include <chrono>
+#define GDP_TRACE_BEGIN(v) const auto v = std::chrono::steady_clock::now()
+#define GDP_TRACE_END(v, what) \
+  fprintf(stderr, "gdp-trace %s %.3f ms\n", what, \
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - v).count())
+#else
+#define GDP_TRACE_BEGIN(v) (void) 0
+#define GDP_TRACE_END(v, what) (void) 0
+#endif
+
+/* One in-flight wave of gdp_align_batch; NSLOTS waves are in flight. */
+constexpr int NSLOTS = 3;
 struct Slot {
   PlanHost h;
   PlanDev d;
@@ -165,14 +187,15 @@ struct gdp_ctx {
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
-  int64_t wave = 131072;
+  int64_t wave = 262144;
   int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
   int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
   bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
   int group_slack = 48;     /* lane groups of K lanes take sweeps up to 17 K - group_slack columns */
   int plan_threads = 8;     /* host threads of the planner */
+  bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) */
   DevBuf arena, scratch;
-  Slot slot[2];
+  Slot slot[NSLOTS];
   std::atomic<int64_t> launches{0};
   std::string err;
   std::mutex mu;
@@ -202,10 +225,16 @@ kernel_name (int id) {
   if (id == PROF_RERUN) return "compact_rerun_kernel";
   if (id == PROF_RECS) return "compact_records_kernel";
   if (id == PROF_WINDOW) return "window_kernel";
-  if (id >= NTHREADKINDS + NWARPKINDS) {
-    const int c = id - NTHREADKINDS - NWARPKINDS, vl = c / 4, variant = vl / 2, late = vl & 1;
+  if (id >= FIRST_CTA) {
+    const int c = id - FIRST_CTA, vl = c / 4, variant = vl / 2, late = vl & 1;
     snprintf(buf[id], sizeof(buf[id]), "fill_cta<W16,%s,%s,%dwarps>",
              variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early", CTA_NW[c % 4]);
+    return buf[id];
+  }
+  if (id >= FIRST_WARP8) {
+    const int c = id - FIRST_WARP8, vl = c / 3, variant = vl / 2, late = vl & 1;
+    snprintf(buf[id], sizeof(buf[id]), "fill_warp<W32,%s,%s,%dlanes,8bit-check>",
+             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early", WARP8_K[c % 3]);
     return buf[id];
   }
   if (id >= NTHREADKINDS) {
@@ -272,7 +301,7 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
   if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
   for (auto &t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
-  for (int s = 0; s < 2; s++) slot_release(ctx->slot[s]);
+  for (int s = 0; s < NSLOTS; s++) slot_release(ctx->slot[s]);
   ctx->arena.release(); ctx->scratch.release();
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
@@ -309,7 +338,7 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
     gdp_ctx_destroy(ctx);
     return GDP_ERR_CUDA;
   }
-  for (int s = 0; s < 2; s++) {
+  for (int s = 0; s < NSLOTS; s++) {
     Slot &sl = ctx->slot[s];
     cudaEventCreateWithFlags(&sl.h2d_done, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&sl.comp_done, cudaEventDisableTiming);
@@ -669,7 +698,15 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
         c.maxY[k] = std::max(c.maxY[k], Y);
       }
       if (p.precision == 8) {
-        const int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
+        int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
+        if (rerun && ctx->check_groups) {
+          /* the 8-bit pass runs for few pairs: lane groups give it the whole device */
+          gdp_geom_t g8;
+          gdp_geom_of(&p, 32, &g8);
+          const int sweep8 = 31 + g8.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
+          for (int q = 0; q < 3; q++)
+            if (sweep8 <= WARP8_K[q] * 33 - ctx->group_slack) { k = warp8_kind_id(p.variant, late, q); break; }
+        }
         m.dir8 = (gdp_pair_words(&p, 32) + 3) & ~(int64_t) 3;
         c.words += m.dir8;
         k8[i] = (uint32_t) k << KEY_KIND_SHIFT | work_key(p, 32);
@@ -899,7 +936,7 @@ static void launch_cta (int nwi, FillParams P, int grid, cudaStream_t s) {
 
 static void
 launch_cta_kind (int k, FillParams P, int grid, cudaStream_t s) {
-  const int c = k - NTHREADKINDS - NWARPKINDS, vl = c / 4, variant = vl / 2, late = vl & 1, nwi = c % 4;
+  const int c = k - FIRST_CTA, vl = c / 4, variant = vl / 2, late = vl & 1, nwi = c % 4;
   if (variant == GDP_FULL) { if (late) launch_cta<GDP_FULL, true>(nwi, P, grid, s); else launch_cta<GDP_FULL, false>(nwi, P, grid, s); }
   else if (variant == GDP_UPPER) { if (late) launch_cta<GDP_UPPER, true>(nwi, P, grid, s); else launch_cta<GDP_UPPER, false>(nwi, P, grid, s); }
   else { if (late) launch_cta<GDP_LOWER, true>(nwi, P, grid, s); else launch_cta<GDP_LOWER, false>(nwi, P, grid, s); }
@@ -914,12 +951,57 @@ static void launch_warp (int kg, FillParams P, int grid, cudaStream_t s) {
   }
 }
 
+template <int V, bool L>
+static void launch_warp8 (int kg, FillParams P, int grid, cudaStream_t s) {
+  switch (WARP8_K[kg]) {
+  case 4: fill_warp_kernel<V, L, 4, 32, 2><<<grid, 128, 0, s>>>(P); break;
+  case 8: fill_warp_kernel<V, L, 8, 32, 2><<<grid, 128, 0, s>>>(P); break;
+  default: fill_warp_kernel<V, L, 16, 32, 2><<<grid, 128, 0, s>>>(P); break;
+  }
+}
+
+static void
+launch_warp8_kind (int k, FillParams P, int grid, cudaStream_t s) {
+  const int c = k - FIRST_WARP8, vl = c / 3, variant = vl / 2, late = vl & 1, kg = c % 3;
+  if (variant == GDP_FULL) { if (late) launch_warp8<GDP_FULL, true>(kg, P, grid, s); else launch_warp8<GDP_FULL, false>(kg, P, grid, s); }
+  else if (variant == GDP_UPPER) { if (late) launch_warp8<GDP_UPPER, true>(kg, P, grid, s); else launch_warp8<GDP_UPPER, false>(kg, P, grid, s); }
+  else { if (late) launch_warp8<GDP_LOWER, true>(kg, P, grid, s); else launch_warp8<GDP_LOWER, false>(kg, P, grid, s); }
+}
+
 static void
 launch_warp_kind (int k, FillParams P, int grid, cudaStream_t s) {
   const int c = k - NTHREADKINDS, vl = c / 3, variant = vl / 2, late = vl & 1, kg = c % 3;
   if (variant == GDP_FULL) { if (late) launch_warp<GDP_FULL, true>(kg, P, grid, s); else launch_warp<GDP_FULL, false>(kg, P, grid, s); }
   else if (variant == GDP_UPPER) { if (late) launch_warp<GDP_UPPER, true>(kg, P, grid, s); else launch_warp<GDP_UPPER, false>(kg, P, grid, s); }
   else { if (late) launch_warp<GDP_LOWER, true>(kg, P, grid, s); else launch_warp<GDP_LOWER, false>(kg, P, grid, s); }
+}
+
+/* The traceback launch over the plan's traceback list on stream ks. */
+static int
+launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
+                  gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t ks) {
+  TbParams T;
+  T.pairs = d_pairs; T.arena = d_arena;
+  T.list = pd.lists.as<int32_t>() + ph.start[NKINDS];
+  T.count = pd.counts.as<int32_t>() + NKINDS;
+  T.dirs = pd.dirs.as<uint32_t>(); T.meta = pd.meta.as<gdp_meta_t>(); T.res = d_res; T.recs = d_slots;
+  T.rec_off = pd.rec_off.as<int64_t>();
+  T.genome = ctx->d_genome; T.genomealt = ctx->d_genomealt;
+  T.genome_base = 0;
+  T.genome_len = ctx->genome_len;
+  T.tab = ctx->d_tab;
+  cudaEvent_t ev = nullptr;
+  prof_begin(ctx, &ev, ks);
+  if (ctx->tb_warp) {
+    const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, (int64_t) ctx->nsm * 16));
+    traceback_warp_kernel<<<g, 128, 0, ks>>>(T);
+  } else {
+    traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, ks>>>(T);
+  }
+  prof_end(ctx, PROF_TB, ev, ks);
+  ctx->launches++;
+  CK(ctx, cudaGetLastError());
+  return GDP_OK;
 }
 
 /* Enqueues fills and tracebacks of a planned batch on the compute stream.
@@ -962,16 +1044,25 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   int side = 0;
   CK(ctx, cudaEventRecord(ctx->fork_ev, s));
   for (int round = 0; round < 2; round++) {
+    if (round == 1 && forked) {
+      for (int q = 0; q < 2; q++) {
+        CK(ctx, cudaEventRecord(ctx->join_ev[q], ctx->side[q]));
+        CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
+      }
+    }
     for (int kk = 0; kk < NKINDS; kk++) {
       const int k = (round == 0) ? (kk + NTHREADKINDS) % NKINDS : kk;
-      const bool warp = k >= NTHREADKINDS && k < NTHREADKINDS + NWARPKINDS;
-      const bool cta = k >= NTHREADKINDS + NWARPKINDS;
-      const int w32 = (warp || cta) ? 0 : (k >> 2) / 3, pass = (warp || cta) ? 0 : (k & 1);
-      const bool second = (w32 == 1 && pass == 1);
+      const bool warp = k >= NTHREADKINDS && k < FIRST_WARP8;
+      const bool warp8 = k >= FIRST_WARP8 && k < FIRST_CTA;
+      const bool cta = k >= FIRST_CTA;
+      const bool thread = !warp && !warp8 && !cta;
+      const int w32 = thread ? (k >> 2) / 3 : 0, pass = thread ? (k & 1) : 0;
+      const bool second = (w32 == 1 && pass == 1) || warp8;
       if ((round == 0) == second || !ph.counts[k]) continue;
       const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], (int64_t) ctx->nsm * 8))
-                           : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
-                                  : fill_grid(ctx, ph.counts[k]);
+                     : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
+                     : warp8 ? warp_grid(ctx, ph.counts[k], WARP8_K[(k - FIRST_WARP8) % 3])
+                             : fill_grid(ctx, ph.counts[k]);
       FillParams P;
       P.pairs = d_pairs; P.arena = d_arena;
       P.list = pd.lists.as<int32_t>() + ph.start[k];
@@ -1012,41 +1103,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       prof_begin(ctx, &ev, ks);
       if (cta) launch_cta_kind(k, P, grid, ks);
       else if (warp) launch_warp_kind(k, P, grid, ks);
+      else if (warp8) launch_warp8_kind(k, P, grid, ks);
       else launch_kind(k, P, grid, ks);
       prof_end(ctx, k, ev, ks);
       ctx->launches++;
       CK(ctx, cudaGetLastError());
     }
   }
-  if (forked) {
-    for (int q = 0; q < 2; q++) {
-      CK(ctx, cudaEventRecord(ctx->join_ev[q], ctx->side[q]));
-      CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
-    }
-  }
-  if (ph.counts[NKINDS] > 0) {
-    TbParams T;
-    T.pairs = d_pairs; T.arena = d_arena;
-    T.list = pd.lists.as<int32_t>() + ph.start[NKINDS];
-    T.count = pd.counts.as<int32_t>() + NKINDS;
-    T.dirs = pd.dirs.as<uint32_t>(); T.meta = pd.meta.as<gdp_meta_t>(); T.res = d_res; T.recs = d_slots;
-    T.rec_off = pd.rec_off.as<int64_t>();
-    T.genome = ctx->d_genome; T.genomealt = ctx->d_genomealt;
-    T.genome_base = 0;
-    T.genome_len = ctx->genome_len;
-    T.tab = ctx->d_tab;
-    cudaEvent_t ev = nullptr;
-    prof_begin(ctx, &ev);
-    if (ctx->tb_warp) {
-      const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, (int64_t) ctx->nsm * 16));
-      traceback_warp_kernel<<<g, 128, 0, s>>>(T);
-    } else {
-      traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, s>>>(T);
-    }
-    prof_end(ctx, PROF_TB, ev);
-    ctx->launches++;
-    CK(ctx, cudaGetLastError());
-  }
+  if (ph.counts[NKINDS] > 0) return launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, s);
   return GDP_OK;
 }
 
@@ -1132,6 +1196,7 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "warp_max_sweep") && value >= 1) ctx->warp_max_sweep = (int) std::min<int64_t>(value, 32 * 17 - 16);
   else if (!strcmp(name, "group_slack") && value >= 16 && value <= 128) ctx->group_slack = (int) value;
   else if (!strcmp(name, "tb_warp")) ctx->tb_warp = value != 0;
+  else if (!strcmp(name, "check_groups")) ctx->check_groups = value != 0;
   else if (!strcmp(name, "wave_pairs") && value >= 1) ctx->wave = value;
   else return GDP_ERR_PARAM;
   return GDP_OK;
@@ -1145,6 +1210,7 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "warp_max_sweep")) *value = ctx->warp_max_sweep;
   else if (!strcmp(name, "group_slack")) *value = ctx->group_slack;
   else if (!strcmp(name, "tb_warp")) *value = ctx->tb_warp ? 1 : 0;
+  else if (!strcmp(name, "check_groups")) *value = ctx->check_groups ? 1 : 0;
   else if (!strcmp(name, "wave_pairs")) *value = ctx->wave;
   else return GDP_ERR_PARAM;
   return GDP_OK;
@@ -1196,12 +1262,13 @@ gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char 
   CK(ctx, cudaMemcpyAsync(da.p, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->stream));
   /* coordinate descent over the routing knobs, each from a small set */
   struct Knob { int *v; std::vector<int> cand; };
-  int tbw = ctx->tb_warp ? 1 : 0;
+  int tbw = ctx->tb_warp ? 1 : 0, cg = ctx->check_groups ? 1 : 0;
   std::vector<Knob> knobs = {
     {&ctx->warp_min_x, {128, 256, 512, 1024, 2048, 1 << 30}},
     {&ctx->group_slack, {16, 32, 48, 80}},
     {&ctx->warp_max_sweep, {272, 400, 496, 528}},
     {&tbw, {1, 0}},
+    {&cg, {1, 0}},
   };
   double best = tune_trial(ctx, pairs, npairs, dp.as<gdp_pair_t>(), da.as<char>(), dr.as<gdp_result_t>(), drec, 2);
   int rc = best < 0 ? (int) -best : GDP_OK;
@@ -1212,12 +1279,14 @@ gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char 
       if (c == keep) continue;
       *knobs[k].v = c;
       ctx->tb_warp = tbw != 0;
+      ctx->check_groups = cg != 0;
       const double t = tune_trial(ctx, pairs, npairs, dp.as<gdp_pair_t>(), da.as<char>(), dr.as<gdp_result_t>(), drec, 2);
       if (t < 0) { rc = (int) -t; break; }
       if (t < best * 0.98) { best = t; choice = c; }
     }
     *knobs[k].v = choice;
     ctx->tb_warp = tbw != 0;
+    ctx->check_groups = cg != 0;
   }
   ctx->profiling = prof;
   if (best_ms) *best_ms = best;
@@ -1234,10 +1303,19 @@ gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char 
 static int
 slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int64_t count,
              int64_t arena_bytes, gdp_result_t *results, cudaEvent_t arena_ready) {
+  /* the slot's host plan buffers are free once their last upload ended */
+  GDP_TRACE_BEGIN(t0);
+  CK(ctx, cudaEventSynchronize(sl.h2d_done));
+  GDP_TRACE_END(t0, "wait_h2d");
+  GDP_TRACE_BEGIN(t1);
   int rc = plan_build(ctx, pairs + first, count, arena_bytes, sl.h);
+  GDP_TRACE_END(t1, "plan");
   if (rc != GDP_OK) return rc;
   sl.first = first;
   sl.count = count;
+  /* the slot's device buffers are free once the last wave's copies out
+     ended: the copy-in stream waits for that on the device */
+  CK(ctx, cudaStreamWaitEvent(ctx->h2d, sl.out_done, 0));
   CK(ctx, sl.pairs.ensure(std::max<int64_t>(count, 1) * sizeof(gdp_pair_t)));
   CK(ctx, sl.results.ensure(std::max<int64_t>(count, 1) * sizeof(gdp_result_t)));
   CK(ctx, sl.d.slots.ensure(std::max<int64_t>(sl.h.total_recs, 1) * sizeof(gdp_rec_t)));
@@ -1269,7 +1347,9 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
 static int
 slot_finish (gdp_ctx *ctx, Slot &sl, gdp_rec_t *recs, int64_t max_recs, int64_t *base, bool *overflow) {
   if (!sl.busy) return GDP_OK;
+  GDP_TRACE_BEGIN(t0);
   CK(ctx, cudaEventSynchronize(sl.total_ready));
+  GDP_TRACE_END(t0, "wait_total");
   const int64_t total = sl.h.n > 0 ? *sl.total.as<int64_t>() : 0;
   if (total > 0) {
     if (recs == nullptr || *base + total > max_recs) {
@@ -1292,56 +1372,83 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   cudaSetDevice(ctx->device);
   if (nrecs_used) *nrecs_used = 0;
   if (n <= 0) return GDP_OK;
-  CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
-  cudaEvent_t arena_ready;
-  CK(ctx, cudaEventCreateWithFlags(&arena_ready, cudaEventDisableTiming));
   /* the previous batch may still be reading the arena */
-  for (int s = 0; s < 2; s++) CK(ctx, cudaEventSynchronize(ctx->slot[s].out_done));
+  for (int s = 0; s < NSLOTS; s++) CK(ctx, cudaEventSynchronize(ctx->slot[s].out_done));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
-  CK(ctx, cudaMemcpyAsync(ctx->arena.p, arena, arena_bytes, cudaMemcpyHostToDevice, ctx->h2d));
-  CK(ctx, cudaEventRecord(arena_ready, ctx->h2d));
+  CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
   const int64_t wave = std::max<int64_t>(1, ctx->wave);
+  /* The arena goes to the device as a growing prefix: before each wave, the
+     bytes up to the end of that wave's sequences that are not there yet.
+     With pairs in arena order the first wave starts after its own
+     sequences, not the whole arena. */
+  int64_t copied = 0;
+  auto arena_upto = [&](int64_t lo, int64_t count) -> int {
+    int64_t hi = 0;
+    for (int64_t i = lo; i < lo + count; i++) {
+      const gdp_pair_t &p = pairs[i];
+      const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
+      hi = std::max(hi, std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl)));
+    }
+    hi = std::min(std::max<int64_t>(hi, 0), arena_bytes);
+    if (hi > copied) {
+      CK(ctx, cudaMemcpyAsync(ctx->arena.as<char>() + copied, arena + copied, hi - copied, cudaMemcpyHostToDevice,
+                              ctx->h2d));
+      copied = hi;
+    }
+    return GDP_OK;
+  };
+  /* a short first wave gets the pipeline going */
+  const int64_t first_wave = std::min(wave, std::max<int64_t>(16384, wave / 8));
   std::vector<std::pair<int64_t, int64_t>> bases;   /* (first pair, record base) per wave */
+  int order[NSLOTS] = {0};                           /* slots in flight, oldest first */
+  int inflight = 0;
   int64_t base = 0;
   bool overflow = false;
   int rc = GDP_OK;
   int cur = 0;
-  for (int64_t first = 0; first < n && rc == GDP_OK; first += wave) {
-    Slot &sl = ctx->slot[cur];
-    if (sl.busy) {
-      rc = slot_finish(ctx, sl, recs, max_recs, &base, &overflow);
-      bases.push_back({sl.first, sl.rec_base});
+  /* Waves are launched NSLOTS deep.  The records of a wave leave as soon as
+     its count is known, oldest wave first; the host plans the next wave
+     while earlier ones compute and copy out. */
+  auto finish_oldest = [&](bool wait) -> bool {
+    if (inflight == 0) return false;
+    Slot &o = ctx->slot[order[0]];
+    if (!wait && cudaEventQuery(o.total_ready) != cudaSuccess) return false;
+    rc = slot_finish(ctx, o, recs, max_recs, &base, &overflow);
+    bases.push_back({o.first, o.rec_base});
+    for (int q = 1; q < inflight; q++) order[q - 1] = order[q];
+    inflight--;
+    return rc == GDP_OK;
+  };
+  std::vector<std::pair<int64_t, int64_t>> spans;   /* (first pair, count) per wave */
+  for (int64_t first = 0; first < n && rc == GDP_OK;) {
+    while (finish_oldest(false)) {}
+    if (rc != GDP_OK) break;
+    if (ctx->slot[cur].busy) {
+      /* every slot is in flight: the oldest must hand its records out first */
+      while (ctx->slot[cur].busy && rc == GDP_OK) finish_oldest(true);
       if (rc != GDP_OK) break;
     }
-    cudaEventSynchronize(sl.out_done);   /* the slot's buffers are free again */
-    const int64_t count = std::min(wave, n - first);
-    rc = slot_launch(ctx, sl, pairs, first, count, arena_bytes, results, first == 0 ? arena_ready : nullptr);
-    cur ^= 1;
-    /* while this wave runs, queue the previous wave's records out */
-    Slot &prev = ctx->slot[cur];
-    if (rc == GDP_OK && prev.busy) {
-      rc = slot_finish(ctx, prev, recs, max_recs, &base, &overflow);
-      bases.push_back({prev.first, prev.rec_base});
-    }
+    const int64_t count = std::min(first == 0 ? first_wave : wave, n - first);
+    rc = arena_upto(first, count);
+    if (rc != GDP_OK) break;
+    rc = slot_launch(ctx, ctx->slot[cur], pairs, first, count, arena_bytes, results, nullptr);
+    if (rc != GDP_OK) break;
+    spans.push_back({first, count});
+    first += count;
+    order[inflight++] = cur;
+    cur = (cur + 1) % NSLOTS;
   }
-  for (int s = 0; s < 2 && rc == GDP_OK; s++) {
-    Slot &sl = ctx->slot[cur];
-    if (sl.busy) {
-      rc = slot_finish(ctx, sl, recs, max_recs, &base, &overflow);
-      bases.push_back({sl.first, sl.rec_base});
-    }
-    cur ^= 1;
-  }
+  while (rc == GDP_OK && inflight > 0) finish_oldest(true);
   cudaError_t e = cudaStreamSynchronize(ctx->d2h);
   cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
-  cudaEventDestroy(arena_ready);
   if (rc == GDP_OK && e != cudaSuccess) rc = set_err(ctx, "batch copies", e);
   if (rc == GDP_OK && e2 != cudaSuccess) rc = set_err(ctx, "batch kernels", e2);
   if (rc == GDP_OK) {
+    /* record offsets of each wave are relative to the wave's first record */
     std::sort(bases.begin(), bases.end());
-    for (size_t w = 0; w < bases.size(); w++) {
-      const int64_t f = bases[w].first, b = bases[w].second;
-      const int64_t end = std::min(n, f + wave);
+    std::sort(spans.begin(), spans.end());
+    for (size_t w = 0; w < bases.size() && w < spans.size(); w++) {
+      const int64_t f = spans[w].first, end = f + spans[w].second, b = bases[w].second;
       if (b != 0)
         for (int64_t i = f; i < end; i++) results[i].rec_offset += b;
     }
@@ -1367,7 +1474,7 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
   int rc = plan_build(ctx, pp.data(), n, arena_bytes, pl.h);
   cudaStream_t s = ctx->stream;
   DevBuf dpairs, dres;
-  for (int k = 0; k < 2; k++) cudaEventSynchronize(ctx->slot[k].out_done);
+  for (int k = 0; k < NSLOTS; k++) cudaEventSynchronize(ctx->slot[k].out_done);
   if (rc == GDP_OK) rc = plan_upload(ctx, pl.h, pl.d, true, s);
   if (rc == GDP_OK) {
     cudaError_t e = ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16));

@@ -58,9 +58,9 @@ def test_traceback_random(env, seed):
 
 @pytest.mark.parametrize("seed,variants", [(301, (0,)), (302, (1,)), (303, (2,))])
 def test_long_pairs_one_warp_per_pair(env, seed, variants):
-    """Pairs with at least 512 lanes and a sweep of at most 496 columns per
-    block run one warp per pair (lane l owns blocks l, l+32, ...); they must
-    be bit-exact like the one-thread-per-pair fills."""
+    """Pairs with at least 512 lanes run on lane groups (lane l of a group
+    owns blocks l, l + K, ...); they must be bit-exact like the
+    one-thread-per-pair fills."""
     ctx, ref, rest = env
     pairs, arena = cases.random_cases(seed, 10, variants=variants, precisions=(16,), min_len=530,
                                       max_len=1400, extras=(0, 3, 10, 40, 90))
@@ -102,18 +102,31 @@ def test_wide_bands_one_cta_per_pair(env, seed, variants):
     assert any(k.startswith("fill_cta") for k in kernels), kernels
 
 
-def test_rerun_contract(env, gdplib):
+@pytest.mark.parametrize("check_groups", [0, 1])
+def test_rerun_contract(env, gdplib, check_groups):
     """8-bit pairs with the 16-bit rerun: the kept precision follows the
-    overflow rule, and the kept outputs are bit-exact with that precision."""
+    overflow rule, and the kept outputs are bit-exact with that precision,
+    whether the 8-bit pass runs one thread per pair or on lane groups."""
     ctx, ref, rest = env
     pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 31, GENOME['g'], 200)
-    fails = parity.check_fill(ctx, ref, pairs, arena)
-    assert not fails, "\n".join(fails)
-    res, _ = ctx.align(pairs, arena)
-    assert (res["status"] == 0).all()
-    assert (res["precision"] == 16).sum() > 0
-    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
-    assert not fails, "\n".join(fails)
+    keep = ctx.get_param("check_groups")
+    ctx.set_param("check_groups", check_groups)
+    try:
+        ctx.profile(True)
+        ctx.profile_reset()
+        fails = parity.check_fill(ctx, ref, pairs, arena)
+        assert not fails, "\n".join(fails)
+        res, _ = ctx.align(pairs, arena)
+        assert (res["status"] == 0).all()
+        assert (res["precision"] == 16).sum() > 0
+        fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+        assert not fails, "\n".join(fails)
+        kernels = ctx.profile_read()
+        ctx.profile(False)
+    finally:
+        ctx.set_param("check_groups", keep)
+    assert any("8bit-check" in k and k.startswith("fill_warp" if check_groups else "fill_thread")
+               for k in kernels), kernels
 
 
 @pytest.mark.parametrize("kind,n", [(gdp.WL_FIXED, 300), (gdp.WL_CDNA, 12), (gdp.WL_LONG, 4)])
