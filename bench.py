@@ -104,9 +104,10 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        backend = "nccl" if args.impl == "gdp" else "gloo"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
@@ -146,16 +147,20 @@ def make_workload(lib, name, npairs, seed, genome_len=1 << 24):
     return genome, blocks, pairs, arena
 
 
-def cpu_baseline(lib, name, seed, target_seconds, threads=None):
+def cpu_baseline(lib, name, seed, target_seconds, threads=None, genome=None):
     """The reference's own code (oracle/_ref) on a bounded sample of the same
-    workload, all host threads (or the port when the reference is absent)."""
+    workload, all host threads (or the port when the reference is absent).
+    `genome` = (sequence, genomecomp blocks) already set in the library."""
     import oracle
     kind = "reference" if oracle.reference_available() else "port"
     ref = oracle.reference() if kind == "reference" else oracle.restatement()
-    ref.init(0)
     threads = threads or os.cpu_count() or 1
-    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
-    ref.set_genome(blocks, None, genome.size)
+    if genome is None:
+        ref.init(0)
+        genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+        ref.set_genome(blocks, None, genome.size)
+    else:
+        genome, blocks = genome
     n = 200
     while True:
         pairs, arena = gdp.make_pairs(lib, WORKLOADS[name][0], seed + 99, genome, n)
@@ -271,9 +276,9 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
 
 
 def run_reference_arm(args):
-    world, rank, _ = dist_setup(args)
-    if rank != 0:
-        barrier(world)
+    # host cores only: rank 0 runs the sample, the other ranks exit at once
+    # (no process group, so nothing waits on rank 0's minutes of CPU work)
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     lib = gdp.load()
     name = args.workload
@@ -284,7 +289,7 @@ def run_reference_arm(args):
     threads = os.cpu_count() or 1
     genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
     ref.set_genome(blocks, None, genome.size)
-    cal = cpu_baseline(lib, name, args.seed, args.cpu_seconds / max(args.steps, 1), threads)
+    cal = cpu_baseline(lib, name, args.seed, args.cpu_seconds / max(args.steps, 1), threads, (genome, blocks))
     pairs, arena = gdp.make_pairs(lib, WORKLOADS[name][0], args.seed + 99, genome, cal["pairs"])
     cells = int(gdp.band_cells(pairs).sum())
     for _ in range(args.warmup):
@@ -307,7 +312,6 @@ def run_reference_arm(args):
                     "d2h_bytes_per_step": 0},
             "alignments_per_s": round(pairs.size * args.steps / t, 1)}
     print(json.dumps(line), flush=True)
-    barrier(world)
 
 
 def run_gdp(args):

@@ -1399,6 +1399,23 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   };
   /* a short first wave gets the pipeline going */
   const int64_t first_wave = std::min(wave, std::max<int64_t>(16384, wave / 8));
+  /* a wave also ends before its direction words would pass the context's
+     budget (an upper bound per pair: every block sweeps at most
+     W + lband + uband columns) */
+  auto wave_count = [&](int64_t first, int64_t cap) -> int64_t {
+    int64_t bytes = 0, k = 0;
+    for (; k < cap && first + k < n; k++) {
+      const gdp_pair_t &p = pairs[first + k];
+      const int64_t X = std::max(p.variant == GDP_LOWER ? p.glength : p.rlength, 0);
+      const int64_t band = std::max(p.lband, 0) + std::max(p.uband, 0);
+      int64_t b = 0;
+      if (p.precision == 16 || (p.flags & GDP_FLAG_RERUN16)) b += (X / 16 + 1) * (16 + band) * 8;
+      if (p.precision == 8) b += (X / 32 + 1) * (32 + band) * 16;
+      if (k > 0 && bytes + b > ctx->budget) break;
+      bytes += b;
+    }
+    return std::max<int64_t>(k, 1);
+  };
   std::vector<std::pair<int64_t, int64_t>> bases;   /* (first pair, record base) per wave */
   int order[NSLOTS] = {0};                           /* slots in flight, oldest first */
   int inflight = 0;
@@ -1428,7 +1445,7 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
       while (ctx->slot[cur].busy && rc == GDP_OK) finish_oldest(true);
       if (rc != GDP_OK) break;
     }
-    const int64_t count = std::min(first == 0 ? first_wave : wave, n - first);
+    const int64_t count = wave_count(first, std::min(first == 0 ? first_wave : wave, n - first));
     rc = arena_upto(first, count);
     if (rc != GDP_OK) break;
     rc = slot_launch(ctx, ctx->slot[cur], pairs, first, count, arena_bytes, results, nullptr);

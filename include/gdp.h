@@ -141,7 +141,9 @@ const char *gdp_version(void);
  * Mode_T (src/mode.h:4; 0 = STANDARD) and selects the substitution and
  * consistency tables built as Dynprog_init does (src/dynprog.c:1007-1196).
  * `dir_budget_bytes` bounds the device memory used for direction matrices
- * per submitted wave (0 = library default).
+ * per wave of gdp_align_batch (0 = 40 GB): a wave ends before its pairs'
+ * direction words would pass it (a pair larger than the budget runs in a
+ * wave of its own).
  */
 int gdp_ctx_create(gdp_ctx **ctx, int device, int mode, int64_t dir_budget_bytes);
 void gdp_ctx_destroy(gdp_ctx *ctx);

@@ -31,6 +31,12 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
 
 
+# Genomes handed to a library, by library path.  Every CpuOracle of one path
+# shares the library's single global genome pointer, so the arrays behind it
+# must live as long as the last set_genome of any of those instances.
+_GENOME_KEEP = {}
+
+
 class CpuOracle:
     """Wraps libgdpref.so (prefix 'ref_') or liboracle.so (prefix 'orc_')."""
 
@@ -54,7 +60,6 @@ class CpuOracle:
         self._pd.argtypes = [i32, i32, i32]
         self._cons = getattr(self.lib, prefix + "consistent")
         self._cons.argtypes = [i32, i32, i32]
-        self._genome_keep = None
 
     def init(self, mode=0):
         self._init(mode)
@@ -68,7 +73,7 @@ class CpuOracle:
     def set_genome(self, blocks, altblocks=None, length=None):
         if length is None:
             length = blocks.size // 3 * 32
-        self._genome_keep = (blocks, altblocks)
+        _GENOME_KEEP[self.path] = (blocks, altblocks)
         self._set_genome(_ptr(blocks), _ptr(altblocks), length)
 
     def align(self, pair_arr, i, arena, want_matrix=True, max_recs=None):

@@ -86,3 +86,23 @@ def test_autotuned_routing_gives_identical_results(gdplib):
     assert (ref["status"] == 0).all()
     assert _same(got, ref) and got_recs.tobytes() == ref_recs.tobytes()
     assert _same(thr, ref) and thr_recs.tobytes() == ref_recs.tobytes()
+
+
+def test_direction_budget_splits_waves(gdplib):
+    """A context whose direction-memory budget holds only a few pairs' words
+    cuts the host-buffer batch into many waves; the results and records are
+    the same bytes as one wave's."""
+    genome, blocks = gdp.make_genome(gdplib, 81, 1 << 22)
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_MIX, 82, genome, 800)
+    outs = []
+    for budget in (0, 1 << 20):
+        ctx = gdp.Context(gdplib, budget=budget)
+        ctx.set_genome(blocks, None, genome.size)
+        before = ctx.launches()
+        res, recs = ctx.align(pairs, arena)
+        outs.append((res, recs, ctx.launches() - before))
+        ctx.close()
+    (r0, c0, l0), (r1, c1, l1) = outs
+    assert (r0["status"] == 0).all()
+    assert _same(r0, r1) and c0.tobytes() == c1.tobytes()
+    assert l1 > 2 * l0          # many more waves ran
