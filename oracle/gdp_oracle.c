@@ -449,7 +449,7 @@ diag_pair (pool_t *P, const tbin_t *T, int r, int c, int *st) {
    reference reads stale scratch there, so such a traceback has no defined
    result.  Fgap is cleared by every full-band fill (:2203-2218), so only
    nogap/Egap reads can be stale. */
-static int tb_outside = 0, tb_stale = 0;
+static __thread int tb_outside = 0, tb_stale = 0;
 int orc_last_tb_outside (void) { return tb_outside; }
 int orc_last_tb_stale (void) { return tb_stale; }
 
@@ -609,8 +609,42 @@ orc_align (const gdp_pair_t *p, const char *arena,
   return n;
 }
 
+/* The precision whose outputs the rerun contract keeps for pair p
+   (GDP_FLAG_RERUN16 on an 8-bit pair): 8 unless the 8-bit fill reaches 127
+   inside the compare domain, ends at or below -98, or (with a traceback)
+   its 8-bit traceback reads a cell the 8-bit fill never wrote. */
+static int
+kept_precision (const gdp_pair_t *p, const char *arena) {
+  gdp_pair_t q = *p;
+  grid_t G;
+  int c, r, keep = 8;
+  if (p->precision != 8 || !(p->flags & GDP_FLAG_RERUN16)) return p->precision;
+  q.flags &= ~GDP_FLAG_RERUN16;
+  fill(&q, arena, &G);
+  for (c = 1; c <= q.glength && keep == 8; c++) {
+    int lo, hi;
+    if (q.variant == GDP_FULL) { lo = c - q.uband; hi = c + q.lband; }
+    else if (q.variant == GDP_UPPER) { lo = c - q.uband; hi = c; }
+    else { lo = c; hi = c + q.lband; }
+    if (lo < 1) lo = 1;
+    if (hi > q.rlength) hi = q.rlength;
+    for (r = lo; r <= hi; r++)
+      if (G.M[gidx(&G, c, r)] >= 127) { keep = 16; break; }
+  }
+  if (keep == 8 && G.M[gidx(&G, q.glength, q.rlength)] <= -98) keep = 16;
+  if (keep == 8 && (q.flags & GDP_FLAG_TRACEBACK)) {
+    int st[6];
+    traceback(&q, arena, &G, st, NULL, 0);
+    if (tb_stale) keep = 16;
+  }
+  grid_free(&G);
+  return keep;
+}
+
 typedef struct {
   const gdp_pair_t *pairs; const char *arena; int64_t n; int tid, nt; int64_t sum;
+  const int8_t *kept_in;
+  int8_t *kept_out;
 } job_t;
 
 static void *
@@ -618,31 +652,65 @@ worker (void *arg) {
   job_t *j = (job_t *) arg;
   int64_t i;
   for (i = j->tid; i < j->n; i += j->nt) {
+    const gdp_pair_t *p = &j->pairs[i];
     int32_t fs = 0, st[6] = {0};
-    orc_align(&j->pairs[i], j->arena, NULL, NULL, NULL, NULL, &fs, st, NULL, 0);
+    if (j->kept_out) {
+      j->kept_out[i] = (int8_t) kept_precision(p, j->arena);
+      continue;
+    }
+    if (p->precision == 8 && (p->flags & GDP_FLAG_RERUN16)) {
+      /* only the kept precision runs */
+      gdp_pair_t q = *p;
+      q.flags &= ~GDP_FLAG_RERUN16;
+      q.precision = j->kept_in ? j->kept_in[i] : 16;
+      orc_align(&q, j->arena, NULL, NULL, NULL, NULL, &fs, st, NULL, 0);
+    } else {
+      orc_align(p, j->arena, NULL, NULL, NULL, NULL, &fs, st, NULL, 0);
+    }
     j->sum += fs + st[0];
   }
   return NULL;
 }
 
-double
-orc_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int64_t *checksum) {
-  pthread_t th[256];
-  job_t jobs[256];
+static double
+run_jobs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int64_t *checksum,
+          const int8_t *kept_in, int8_t *kept_out) {
+  pthread_t *th;
+  job_t *jobs;
   struct timespec t0, t1;
   int t;
   int64_t sum = 0;
   if (tables_mode < 0) orc_init(0);
   if (nthreads < 1) nthreads = 1;
-  if (nthreads > 256) nthreads = 256;
+  th = (pthread_t *) calloc(nthreads, sizeof(pthread_t));
+  jobs = (job_t *) calloc(nthreads, sizeof(job_t));
   clock_gettime(CLOCK_MONOTONIC, &t0);
   for (t = 0; t < nthreads; t++) {
     jobs[t].pairs = pairs; jobs[t].arena = arena; jobs[t].n = npairs; jobs[t].tid = t;
-    jobs[t].nt = nthreads; jobs[t].sum = 0;
+    jobs[t].nt = nthreads; jobs[t].sum = 0; jobs[t].kept_in = kept_in; jobs[t].kept_out = kept_out;
     pthread_create(&th[t], NULL, worker, &jobs[t]);
   }
   for (t = 0; t < nthreads; t++) { pthread_join(th[t], NULL); sum += jobs[t].sum; }
   clock_gettime(CLOCK_MONOTONIC, &t1);
+  free(th);
+  free(jobs);
   if (checksum) *checksum = sum;
   return (double) (t1.tv_sec - t0.tv_sec) + 1e-9 * (double) (t1.tv_nsec - t0.tv_nsec);
+}
+
+/* Every pair once across nthreads threads (fill, and traceback when asked);
+   returns wall seconds.  An 8-bit pair flagged RERUN16 runs at the
+   precision kept[i] only (16 when kept is NULL): the least work that gives
+   the rerun contract's outputs. */
+double
+orc_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int64_t *checksum,
+           const int8_t *kept) {
+  return run_jobs(pairs, arena, npairs, nthreads, checksum, kept, NULL);
+}
+
+/* kept[i] = the precision the rerun contract keeps for pair i, computed on
+   nthreads threads. */
+void
+orc_kept_precision (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int8_t *kept) {
+  run_jobs(pairs, arena, npairs, nthreads, NULL, NULL, kept);
 }

@@ -16,5 +16,7 @@ int orc_align(const gdp_pair_t *p, const char *arena,
 int orc_last_tb_outside(void);
 int orc_last_tb_stale(void);
 double orc_bench(const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
-                 int64_t *checksum);
+                 int64_t *checksum, const int8_t *kept);
+void orc_kept_precision(const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
+                        int8_t *kept);
 #endif

@@ -54,7 +54,7 @@ class CpuOracle:
         self._align.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
         self._align.restype = i32
         self._bench = getattr(self.lib, prefix + "bench")
-        self._bench.argtypes = [vp, vp, i64, i32, ctypes.POINTER(i64)]
+        self._bench.argtypes = [vp, vp, i64, i32, ctypes.POINTER(i64), vp]
         self._bench.restype = ctypes.c_double
         self._pd = getattr(self.lib, prefix + "pairdistance")
         self._pd.argtypes = [i32, i32, i32]
@@ -95,10 +95,28 @@ class CpuOracle:
         return {"score": int(final[0]), "H": H, "dN": dN, "dE": dE, "dF": dF,
                 "stats": stats, "recs": recs[:min(nrec, max_recs)], "nrecs": nrec}
 
-    def bench(self, pairs, arena, nthreads):
+    def bench(self, pairs, arena, nthreads, kept=None):
+        """Wall seconds and a score checksum for every pair once on nthreads
+        threads.  `kept` (int8 per pair, from kept_precision) says which
+        precision an 8-bit pair flagged RERUN16 keeps; only that precision
+        runs (the least work giving the contract's outputs).  Without it such
+        pairs run in 16-bit."""
         cs = ctypes.c_int64(0)
-        secs = self._bench(_ptr(pairs), _ptr(arena), pairs.size, nthreads, ctypes.byref(cs))
+        if kept is not None:
+            kept = np.ascontiguousarray(kept, dtype=np.int8)
+            assert kept.size == pairs.size
+        secs = self._bench(_ptr(pairs), _ptr(arena), pairs.size, nthreads, ctypes.byref(cs), _ptr(kept))
         return secs, cs.value
+
+    def kept_precision(self, pairs, arena, nthreads):
+        """Per pair, the precision the rerun contract keeps (restatement only:
+        it needs to know whether an 8-bit traceback reads unwritten cells)."""
+        fn = self.lib.orc_kept_precision
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
+        fn.restype = None
+        kept = np.zeros(pairs.size, dtype=np.int8)
+        fn(_ptr(pairs), _ptr(arena), pairs.size, nthreads, _ptr(kept))
+        return kept
 
 
 def _rec_dtype():

@@ -369,6 +369,7 @@ ref_align (const gdp_pair_t *p, const char *arena,
 typedef struct {
   const gdp_pair_t *pairs;
   const char *arena;
+  const int8_t *kept;
   int64_t npairs;
   int tid, nthreads;
   int64_t checksum;
@@ -382,8 +383,15 @@ bench_worker (void *arg) {
   memset(&st, 0, sizeof(st));
   for (i = job->tid; i < job->npairs; i += job->nthreads) {
     const gdp_pair_t *p = &job->pairs[i];
+    gdp_pair_t q;
     fillout_t o;
     int stats[6];
+    if (p->precision == 8 && (p->flags & GDP_FLAG_RERUN16)) {
+      /* only the kept precision runs */
+      q = *p;
+      q.precision = job->kept ? job->kept[i] : 16;
+      p = &q;
+    }
     run_fill(&st, p, job->arena, &o);
     if (p->variant == GDP_LOWER) {
       sum += get_cell(o.matrix, o.prec, p->rlength, p->glength);
@@ -401,10 +409,13 @@ bench_worker (void *arg) {
 }
 
 /* Runs every pair once across nthreads threads; returns wall seconds and
-   writes a checksum of final and traceback scores. */
+   writes a checksum of final and traceback scores.  An 8-bit pair flagged
+   RERUN16 runs at the precision kept[i] only (16 when kept is NULL): the
+   least work that gives the rerun contract's outputs, and never an 8-bit
+   traceback that would read unwritten scratch. */
 double
 ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
-           int64_t *checksum) {
+           int64_t *checksum, const int8_t *kept) {
   pthread_t *th;
   benchjob_t *jobs;
   struct timespec t0, t1;
@@ -416,7 +427,7 @@ ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthre
   jobs = (benchjob_t *) calloc(nthreads, sizeof(benchjob_t));
   clock_gettime(CLOCK_MONOTONIC, &t0);
   for (t = 0; t < nthreads; t++) {
-    jobs[t].pairs = pairs; jobs[t].arena = arena; jobs[t].npairs = npairs;
+    jobs[t].pairs = pairs; jobs[t].arena = arena; jobs[t].npairs = npairs; jobs[t].kept = kept;
     jobs[t].tid = t; jobs[t].nthreads = nthreads;
     pthread_create(&th[t], NULL, bench_worker, &jobs[t]);
   }

@@ -120,3 +120,26 @@ def test_product_tables_standard_shape(gdplib):
     assert pd[0, A, ord("z")] == 0 and pd[0, ord("*"), A] == 0
     assert nt[A] == 0 and nt[ord("t")] == 3 and nt[N] == 4 and nt[ord("*")] == 4
     assert cons[0, ord("R"), G] == 1 and cons[0, A, C] == 0
+
+
+def test_kept_precision_and_cpu_bench(restatement, gdplib):
+    """The batched kept-precision resolver (used to time the CPU baselines)
+    agrees with the per-pair rerun rule, and the reference and the
+    restatement timed at those precisions give the same score checksum."""
+    genome, blocks = gdp.make_genome(gdplib, 93, 1 << 20)
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 94, genome, 400)
+    restatement.set_genome(blocks, None, genome.size)
+    kept = restatement.kept_precision(pairs, arena, 4)
+    assert set(np.unique(kept)) <= {8, 16}
+    for i in range(0, pairs.size, 7):
+        q = pairs[i:i + 1].copy()
+        q["precision"] = 8
+        q["flags"] = q["flags"] & ~gdp.FLAG_RERUN16
+        o8 = restatement.align(q.copy(), 0, arena)
+        assert kept[i] == _golden_precision(pairs, i, o8, restatement, arena), i
+    _, cs = restatement.bench(pairs, arena, 3, kept)
+    if orc.reference_available():
+        ref = orc.reference()
+        ref.set_genome(blocks, None, genome.size)
+        _, cs_ref = ref.bench(pairs, arena, 3, kept)
+        assert cs_ref == cs
