@@ -30,6 +30,9 @@
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <functional>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -75,7 +78,7 @@ struct HostBuf {   /* pinned host memory */
     bytes = 0;
     /* grow geometrically: a buffer that keeps growing is reallocated rarely */
     size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
-    cudaError_t e = cudaHostAlloc(&p, grow, cudaHostAllocDefault);
+    cudaError_t e = cudaHostAlloc(&p, grow, cudaHostAllocMapped);
     if (e == cudaSuccess) bytes = grow;
     return e;
   }
@@ -112,6 +115,62 @@ inline int cta_kind_id (int variant, int late, int nwi) {
 
 }  // namespace
 
+/* Persistent host worker threads for the planner.  run(nt, f) calls f(t)
+   for t = 0 .. nt-1, t = 0 on the caller, the rest on the pool's workers,
+   and returns when all are done.  A context owns one pool, so contexts
+   plan concurrently without sharing threads. */
+class WorkPool {
+ public:
+  WorkPool () = default;
+  WorkPool (const WorkPool &) = delete;
+  WorkPool &operator= (const WorkPool &) = delete;
+  ~WorkPool () {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  template <class F>
+  void run (int nt, F &&f) {
+    if (nt <= 1) { f(0); return; }
+    std::unique_lock<std::mutex> g(m_);
+    while ((int) th_.size() < nt - 1) th_.emplace_back([this] { work(); });
+    fn_ = [&f] (int t) { f(t); };
+    next_ = 1;
+    nt_ = nt;
+    left_ = nt - 1;
+    g.unlock();
+    cv_.notify_all();
+    f(0);
+    g.lock();
+    done_.wait(g, [this] { return left_ == 0; });
+    nt_ = next_ = 0;
+    fn_ = nullptr;
+  }
+ private:
+  void work () {
+    std::unique_lock<std::mutex> g(m_);
+    for (;;) {
+      cv_.wait(g, [this] { return stop_ || next_ < nt_; });
+      if (stop_) return;
+      const int t = next_++;
+      std::function<void(int)> fn = fn_;
+      g.unlock();
+      fn(t);
+      g.lock();
+      if (--left_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  std::function<void(int)> fn_;
+  int next_ = 0, nt_ = 0, left_ = 0;
+  bool stop_ = false;
+};
+
 /* Host side of a plan (pinned so its upload is asynchronous). */
 struct PlanHost {
   int64_t n = 0;
@@ -122,8 +181,17 @@ struct PlanHost {
   int maxY[NKINDS] = {0};
   int64_t dir_words = 0, total_recs = 0;
   int64_t nwindow = 0;   /* pairs whose genome window the device extracts */
+  /* planner scratch, kept from plan to plan (grown, never shrunk) */
+  std::vector<uint32_t> k16, k8, keys, keys2;
+  std::vector<int32_t> vals, vals2, tbl;
   void release () { lists.release(); meta.release(); status.release(); rec_off.release(); }
 };
+
+template <class T>
+static inline T *grow (std::vector<T> &v, int64_t n) {
+  if ((int64_t) v.size() < n) v.resize((size_t) n);
+  return v.data();
+}
 
 /* Device side of a plan. */
 struct PlanDev {
@@ -157,9 +225,19 @@ struct gdp_plan {
 #define GDP_TRACE_END(v, what) \
   fprintf(stderr, "gdp-trace %s %.3f ms\n", what, \
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - v).count())
+/* device-side timeline: an event recorded on a stream, printed at the end
+   of gdp_align_batch as milliseconds from the batch's first event */
+struct GdpTraceEv { char what[48]; cudaEvent_t ev; std::chrono::steady_clock::time_point host; };
+static std::vector<GdpTraceEv> gdp_tev;
+static std::mutex gdp_tev_mu;
+#define GDP_TEV(stream, fmt, arg) do { \
+    GdpTraceEv t_; snprintf(t_.what, sizeof(t_.what), fmt, (long long) (arg)); \
+    cudaEventCreate(&t_.ev); cudaEventRecord(t_.ev, stream); t_.host = std::chrono::steady_clock::now(); \
+    std::lock_guard<std::mutex> tg_(gdp_tev_mu); gdp_tev.push_back(t_); } while (0)
 #else
 #define GDP_TRACE_BEGIN(v) (void) 0
 #define GDP_TRACE_END(v, what) (void) 0
+#define GDP_TEV(stream, fmt, arg) (void) 0
 #endif
 
 /* One in-flight wave of gdp_align_batch; NSLOTS waves are in flight. */
@@ -196,6 +274,7 @@ struct gdp_ctx {
   bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) */
   DevBuf arena, scratch;
   Slot slot[NSLOTS];
+  WorkPool pool;            /* the planner's host threads */
   std::atomic<int64_t> launches{0};
   std::string err;
   std::mutex mu;
@@ -343,7 +422,8 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
     cudaEventCreateWithFlags(&sl.h2d_done, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&sl.comp_done, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&sl.out_done, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&sl.total_ready, cudaEventDisableTiming);
+    /* the copy-out thread sleeps on this one while the planner uses the cores */
+    cudaEventCreateWithFlags(&sl.total_ready, cudaEventDisableTiming | cudaEventBlockingSync);
   }
   ctx->h_tab = (gdp_tables_t *) malloc(sizeof(gdp_tables_t));
   gdp_build_tables(ctx->h_tab, mode);
@@ -585,33 +665,23 @@ padded_kind (int k) {
 }
 
 /* Runs f(lo, hi, t) over [0, n) split into `nt` contiguous chunks, one
-   host thread per chunk. */
+   pool thread per chunk. */
 template <class F>
 static void
-parallel_chunks (int64_t n, int nt, F f) {
-  if (nt <= 1) { f((int64_t) 0, n, 0); return; }
-  std::vector<std::thread> th;
-  th.reserve(nt);
-  for (int t = 0; t < nt; t++) {
-    const int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
-    th.emplace_back([=, &f] { f(lo, hi, t); });
-  }
-  for (auto &x : th) x.join();
+parallel_chunks (WorkPool &pool, int64_t n, int nt, F f) {
+  pool.run(nt, [&](int t) { f(n * t / nt, n * (t + 1) / nt, t); });
 }
 
-/* Stable LSD radix sort of (key, value) by the low 22 bits of key, 11 bits
-   per pass, `nt` host threads (per-thread histograms, then each thread
-   scatters its own chunk in order). */
+/* Stable LSD radix sort of (key, value)[0..n) by the low 22 bits of key,
+   11 bits per pass, `nt` pool threads (per-thread histograms, then each
+   thread scatters its own chunk in order).  k2/v2 are scratch of n. */
 static void
-radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int nt) {
-  const int64_t n = (int64_t) key.size();
-  std::vector<uint32_t> k2(n);
-  std::vector<int32_t> v2(n);
+radix_sort (WorkPool &pool, uint32_t *key, int32_t *val, uint32_t *k2, int32_t *v2, int64_t n, int nt) {
   constexpr int B = 2048;
   std::vector<int64_t> hist((size_t) nt * B);
   for (int shift = 0; shift < 22; shift += 11) {
     std::fill(hist.begin(), hist.end(), 0);
-    parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+    parallel_chunks(pool, n, nt, [&](int64_t lo, int64_t hi, int t) {
       int64_t *h = hist.data() + (size_t) t * B;
       for (int64_t i = lo; i < hi; i++) h[(key[i] >> shift) & (B - 1)]++;
     });
@@ -622,7 +692,7 @@ radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int nt) {
         hist[(size_t) t * B + d] = sum;
         sum += c;
       }
-    parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+    parallel_chunks(pool, n, nt, [&](int64_t lo, int64_t hi, int t) {
       int64_t *h = hist.data() + (size_t) t * B;
       for (int64_t i = lo; i < hi; i++) {
         const int64_t at = h[(key[i] >> shift) & (B - 1)]++;
@@ -630,9 +700,11 @@ radix_sort (std::vector<uint32_t> &key, std::vector<int32_t> &val, int nt) {
         v2[at] = val[i];
       }
     });
-    key.swap(k2);
-    val.swap(v2);
+    std::swap(key, k2);
+    std::swap(val, v2);
   }
+  /* an even number of passes leaves the sorted data in the caller's arrays */
+  static_assert((22 + 10) / 11 % 2 == 0, "radix passes are even");
 }
 
 /* Fills ph for pairs[0..n) (pinned host buffers).  arena_bytes < 0 skips the
@@ -653,10 +725,10 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
      tracebacks, device windows, and the largest swept dimension per kind */
   struct Chunk { int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0; int maxY[NKINDS] = {0}; };
   std::vector<Chunk> ch(nt);
-  std::vector<uint32_t> k16(n), k8(n);   /* fill keys of each pair (~0u: none) */
+  uint32_t *k16 = grow(ph.k16, n), *k8 = grow(ph.k8, n);   /* fill keys of each pair (~0u: none) */
   const uint64_t glen = ctx->genome_len;
   /* pass 1: validate, route, size (meta.dir16 / dir8 and rec_off hold sizes) */
-  parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+  parallel_chunks(ctx->pool, n, nt, [&](int64_t lo, int64_t hi, int t) {
     Chunk &c = ch[t];
     for (int64_t i = lo; i < hi; i++) {
       const gdp_pair_t &p = pairs[i];
@@ -731,10 +803,10 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     for (int k = 0; k < NKINDS; k++) maxY[k] = std::max(maxY[k], ch[t].maxY[k]);
   }
   /* pass 2: sizes to offsets, fill entries in pair order */
-  std::vector<uint32_t> keys(entries);
-  std::vector<int32_t> vals(entries);
-  std::vector<int32_t> tbl(ntb);
-  parallel_chunks(n, nt, [&](int64_t lo, int64_t hi, int t) {
+  uint32_t *keys = grow(ph.keys, entries);
+  int32_t *vals = grow(ph.vals, entries);
+  int32_t *tbl = grow(ph.tbl, ntb);
+  parallel_chunks(ctx->pool, n, nt, [&](int64_t lo, int64_t hi, int t) {
     int64_t w = wbase[t], r = rbase[t], en = ebase[t], tb = tbase[t];
     for (int64_t i = lo; i < hi; i++) {
       if (status[i] != GDP_OK) continue;
@@ -752,7 +824,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     }
   });
   static_assert(NKINDS < (1 << (22 - KEY_KIND_SHIFT)), "kind ids fit in the 22-bit sort key");
-  radix_sort(keys, vals, nt);
+  radix_sort(ctx->pool, keys, vals, grow(ph.keys2, entries), grow(ph.vals2, entries), entries, nt);
   /* padded kinds: every band-width group starts a warp (-1 = no pair) */
   int64_t groups = 0;
   for (int64_t i = 0; i < entries; i++) {
@@ -777,7 +849,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   }
   ph.start[NKINDS] = pos;
   ph.counts[NKINDS] = (int32_t) ntb;
-  if (ntb > 0) memcpy(lists + pos, tbl.data(), ntb * sizeof(int32_t));
+  if (ntb > 0) memcpy(lists + pos, tbl, ntb * sizeof(int32_t));
   pos += ntb;
   ph.start[NKINDS + 1] = pos;
   ph.nlists = pos;
@@ -850,9 +922,15 @@ extern "C" int64_t gdp_plan_dir_bytes (const gdp_plan *pl) { return pl->h.dir_wo
 /* Execution                                                           */
 /* ------------------------------------------------------------------ */
 
+/* Zeroed results, the planner's metadata copied to the working copy, and
+   the 8-bit pass counters cleared: all on the SMs, so that no copy engine
+   (busy with another wave's records) sits on the compute stream. */
 __global__ void
-init_results_kernel (gdp_result_t *res, const int32_t *status, const gdp_pair_t *pairs, int64_t n) {
+init_results_kernel (gdp_result_t *res, const int32_t *status, const gdp_pair_t *pairs, int64_t n,
+                     const gdp_meta_t *meta0, gdp_meta_t *meta, int32_t *work_counts, int nwork) {
+  if (blockIdx.x == 0 && (int) threadIdx.x < nwork) work_counts[threadIdx.x] = 0;
   for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+    meta[i] = meta0[i];
     gdp_result_t r;
     r.status = status[i];
     r.score = 0;
@@ -876,7 +954,7 @@ gather_nrecs_kernel (const gdp_result_t *res, int64_t n, int64_t *out) {
    result at it (offset relative to the batch), and writes the total. */
 __global__ void
 compact_records_kernel (gdp_result_t *res, const int64_t *slot_off, const gdp_rec_t *slots,
-                        const int64_t *scan, int64_t n, gdp_rec_t *out, int64_t *total) {
+                        const int64_t *scan, int64_t n, gdp_rec_t *out, int64_t *total, int64_t *total_host) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
@@ -887,7 +965,13 @@ compact_records_kernel (gdp_result_t *res, const int64_t *slot_off, const gdp_re
     for (int k = lane; k < nr; k += 32) out[dst + k] = src[k];
     if (lane == 0) {
       res[i].rec_offset = dst;
-      if (i == n - 1) *total = dst + nr;
+      if (i == n - 1) {
+        *total = dst + nr;
+        if (total_host) {
+          *(volatile int64_t *) total_host = dst + nr;
+          __threadfence_system();
+        }
+      }
     }
   }
 }
@@ -1014,12 +1098,13 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   if (n == 0) return GDP_OK;
   cudaEvent_t ev0 = nullptr;
   prof_begin(ctx, &ev0);
+  static_assert(NKINDS <= 256, "one block clears every 8-bit pass counter");
   init_results_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
-      d_res, pd.status.as<int32_t>(), d_pairs, n);
+      d_res, pd.status.as<int32_t>(), d_pairs, n, pd.meta0.as<gdp_meta_t>(), pd.meta.as<gdp_meta_t>(),
+      pd.work_counts.as<int32_t>(), NKINDS);
   prof_end(ctx, PROF_INIT, ev0);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
-  CK(ctx, cudaMemcpyAsync(pd.meta.p, pd.meta0.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToDevice, s));
   if (ph.nwindow > 0) {
     cudaEvent_t evw = nullptr;
     prof_begin(ctx, &evw);
@@ -1068,8 +1153,8 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.list = pd.lists.as<int32_t>() + ph.start[k];
       P.count = pd.counts.as<int32_t>() + k;
       if (second) {
-        /* only the pairs whose 16-bit maximum stayed below 127 run the 8-bit pass */
-        CK(ctx, cudaMemsetAsync(pd.work_counts.as<int32_t>() + k, 0, sizeof(int32_t), s));
+        /* only the pairs whose 16-bit maximum stayed below 127 run the 8-bit
+           pass (init_results_kernel cleared the counter) */
         const int cg = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
         cudaEvent_t evc = nullptr;
         prof_begin(ctx, &evc);
@@ -1118,7 +1203,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
    pd.total. */
 static int
 compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_res, const gdp_rec_t *d_slots,
-                 gdp_rec_t *out) {
+                 gdp_rec_t *out, int64_t *total_host = nullptr) {
   cudaStream_t s = ctx->stream;
   const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
@@ -1135,7 +1220,8 @@ compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_
   prof_begin(ctx, &ev);
   const int grid = (int) std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t) ctx->nsm * 16));
   compact_records_kernel<<<grid, 256, 0, s>>>(d_res, pd.rec_off.as<int64_t>(), d_slots,
-                                              pd.nrec_scan.as<int64_t>(), n, out, pd.total.as<int64_t>());
+                                              pd.nrec_scan.as<int64_t>(), n, out, pd.total.as<int64_t>(),
+                                              total_host);
   prof_end(ctx, PROF_RECS, ev);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
@@ -1321,47 +1407,58 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   CK(ctx, sl.d.slots.ensure(std::max<int64_t>(sl.h.total_recs, 1) * sizeof(gdp_rec_t)));
   CK(ctx, sl.recs.ensure(std::max<int64_t>(sl.h.total_recs, 1) * sizeof(gdp_rec_t)));
   CK(ctx, sl.total.ensure(sizeof(int64_t)));
+  GDP_TEV(ctx->h2d, "h2d_begin %lld", first);
   CK(ctx, cudaMemcpyAsync(sl.pairs.p, pairs + first, count * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, ctx->h2d));
   rc = plan_upload(ctx, sl.h, sl.d, false, ctx->h2d);
   if (rc != GDP_OK) return rc;
   CK(ctx, cudaEventRecord(sl.h2d_done, ctx->h2d));
+  GDP_TEV(ctx->h2d, "h2d_end %lld", first);
   CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.h2d_done, 0));
   if (arena_ready) CK(ctx, cudaStreamWaitEvent(ctx->stream, arena_ready, 0));
+  GDP_TEV(ctx->stream, "comp_begin %lld", first);
   rc = plan_run(ctx, sl.h, sl.d, sl.pairs.as<gdp_pair_t>(), ctx->arena.as<char>(), sl.results.as<gdp_result_t>(),
                 sl.d.slots.as<gdp_rec_t>());
   if (rc != GDP_OK) return rc;
+  /* the count reaches the host through a mapped pinned word written by the
+     compaction kernel, not a copy on the compute stream (a copy engine busy
+     with an earlier wave's records would hold the stream up) */
+  int64_t *total_dev = nullptr;
+  CK(ctx, cudaHostGetDevicePointer((void **) &total_dev, sl.total.p, 0));
+  *(volatile int64_t *) sl.total.p = 0;
   rc = compact_records(ctx, sl.h, sl.d, sl.results.as<gdp_result_t>(), sl.d.slots.as<gdp_rec_t>(),
-                       sl.recs.as<gdp_rec_t>());
+                       sl.recs.as<gdp_rec_t>(), total_dev);
   if (rc != GDP_OK) return rc;
-  CK(ctx, cudaMemcpyAsync(sl.total.p, sl.d.total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  GDP_TEV(ctx->stream, "comp_end %lld", first);
   CK(ctx, cudaEventRecord(sl.total_ready, ctx->stream));
   CK(ctx, cudaEventRecord(sl.comp_done, ctx->stream));
-  CK(ctx, cudaStreamWaitEvent(ctx->d2h, sl.comp_done, 0));
-  CK(ctx, cudaMemcpyAsync(results + first, sl.results.p, count * sizeof(gdp_result_t), cudaMemcpyDeviceToHost,
-                          ctx->d2h));
-  sl.busy = true;
   return GDP_OK;
 }
 
-/* Waits for the wave's record count and queues its records out at *base. */
+/* Waits for the wave's record count and queues its results and records
+   out (records at *base).  The copy stream takes waves in order, so a wave
+   still computing never holds up the copies of an earlier one. */
 static int
-slot_finish (gdp_ctx *ctx, Slot &sl, gdp_rec_t *recs, int64_t max_recs, int64_t *base, bool *overflow) {
-  if (!sl.busy) return GDP_OK;
+slot_finish (gdp_ctx *ctx, Slot &sl, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs, int64_t *base,
+             bool *overflow) {
   GDP_TRACE_BEGIN(t0);
   CK(ctx, cudaEventSynchronize(sl.total_ready));
   GDP_TRACE_END(t0, "wait_total");
-  const int64_t total = sl.h.n > 0 ? *sl.total.as<int64_t>() : 0;
+  CK(ctx, cudaStreamWaitEvent(ctx->d2h, sl.comp_done, 0));
+  CK(ctx, cudaMemcpyAsync(results + sl.first, sl.results.p, sl.count * sizeof(gdp_result_t), cudaMemcpyDeviceToHost,
+                          ctx->d2h));
+  const int64_t total = sl.h.n > 0 ? *(volatile int64_t *) sl.total.p : 0;
   if (total > 0) {
     if (recs == nullptr || *base + total > max_recs) {
       *overflow = true;
     } else {
+      GDP_TEV(ctx->d2h, "recs_begin %lld", sl.first);
       CK(ctx, cudaMemcpyAsync(recs + *base, sl.recs.p, total * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, ctx->d2h));
+      GDP_TEV(ctx->d2h, "recs_end %lld", sl.first);
     }
   }
   CK(ctx, cudaEventRecord(sl.out_done, ctx->d2h));
   sl.rec_base = *base;
   *base += total;
-  sl.busy = false;
   return GDP_OK;
 }
 
@@ -1377,33 +1474,38 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
   const int64_t wave = std::max<int64_t>(1, ctx->wave);
+#ifdef GDP_HOST_TRACE
+  for (auto &t : gdp_tev) cudaEventDestroy(t.ev);
+  gdp_tev.clear();
+  const auto host0 = std::chrono::steady_clock::now();
+  GDP_TEV(ctx->h2d, "batch_begin %lld", 0);
+#endif
   /* The arena goes to the device as a growing prefix: before each wave, the
      bytes up to the end of that wave's sequences that are not there yet.
      With pairs in arena order the first wave starts after its own
      sequences, not the whole arena. */
   int64_t copied = 0;
-  auto arena_upto = [&](int64_t lo, int64_t count) -> int {
-    int64_t hi = 0;
-    for (int64_t i = lo; i < lo + count; i++) {
-      const gdp_pair_t &p = pairs[i];
-      const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
-      hi = std::max(hi, std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl)));
-    }
+  auto arena_upto = [&](int64_t lo, int64_t hi) -> int {
     hi = std::min(std::max<int64_t>(hi, 0), arena_bytes);
     if (hi > copied) {
+      GDP_TEV(ctx->h2d, "arena_begin %lld", lo);
       CK(ctx, cudaMemcpyAsync(ctx->arena.as<char>() + copied, arena + copied, hi - copied, cudaMemcpyHostToDevice,
                               ctx->h2d));
+      GDP_TEV(ctx->h2d, "arena_end %lld", lo);
       copied = hi;
     }
     return GDP_OK;
   };
-  /* a short first wave gets the pipeline going */
-  const int64_t first_wave = std::min(wave, std::max<int64_t>(16384, wave / 8));
-  /* a wave also ends before its direction words would pass the context's
+  /* Short first waves get the pipeline going: the first holds 1/8 of a
+     wave and each next one twice the one before, up to a full wave, so the
+     copies out start early and never wait long for the next wave. */
+  int64_t wave_cap = std::min(wave, std::max<int64_t>(16384, wave / 8));
+  /* A wave also ends before its direction words would pass the context's
      budget (an upper bound per pair: every block sweeps at most
-     W + lband + uband columns) */
-  auto wave_count = [&](int64_t first, int64_t cap) -> int64_t {
-    int64_t bytes = 0, k = 0;
+     W + lband + uband columns).  One pass finds the count and the end of the
+     wave's sequences in the arena (*hi). */
+  auto wave_count = [&](int64_t first, int64_t cap, int64_t *hi) -> int64_t {
+    int64_t bytes = 0, k = 0, h = 0;
     for (; k < cap && first + k < n; k++) {
       const gdp_pair_t &p = pairs[first + k];
       const int64_t X = std::max(p.variant == GDP_LOWER ? p.glength : p.rlength, 0);
@@ -1413,51 +1515,103 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
       if (p.precision == 8) b += (X / 32 + 1) * (32 + band) * 16;
       if (k > 0 && bytes + b > ctx->budget) break;
       bytes += b;
+      const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
+      h = std::max(h, std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl)));
     }
+    *hi = h;
     return std::max<int64_t>(k, 1);
   };
   std::vector<std::pair<int64_t, int64_t>> bases;   /* (first pair, record base) per wave */
-  int order[NSLOTS] = {0};                           /* slots in flight, oldest first */
-  int inflight = 0;
+  std::vector<std::pair<int64_t, int64_t>> spans;   /* (first pair, count) per wave */
   int64_t base = 0;
   bool overflow = false;
   int rc = GDP_OK;
-  int cur = 0;
-  /* Waves are launched NSLOTS deep.  The records of a wave leave as soon as
-     its count is known, oldest wave first; the host plans the next wave
-     while earlier ones compute and copy out. */
-  auto finish_oldest = [&](bool wait) -> bool {
-    if (inflight == 0) return false;
-    Slot &o = ctx->slot[order[0]];
-    if (!wait && cudaEventQuery(o.total_ready) != cudaSuccess) return false;
-    rc = slot_finish(ctx, o, recs, max_recs, &base, &overflow);
+  /* Waves are launched NSLOTS deep by this thread, which plans the next
+     wave while earlier ones compute.  A copy-out thread takes the launched
+     waves in order: it waits for a wave's record count and at once queues
+     its results and records out, then frees the slot. */
+  std::mutex m;
+  std::condition_variable cv;
+  std::deque<int> launched;          /* slots launched, not yet handed out, oldest first */
+  bool all_launched = false;
+  int out_rc = GDP_OK;
+  auto hand_out = [&](int k) {
+    Slot &o = ctx->slot[k];
+    const int r = out_rc == GDP_OK ? slot_finish(ctx, o, results, recs, max_recs, &base, &overflow) : out_rc;
+    std::lock_guard<std::mutex> g(m);
+    if (r != GDP_OK) out_rc = r;
     bases.push_back({o.first, o.rec_base});
-    for (int q = 1; q < inflight; q++) order[q - 1] = order[q];
-    inflight--;
-    return rc == GDP_OK;
+    o.busy = false;
+    launched.pop_front();
+    cv.notify_all();
   };
-  std::vector<std::pair<int64_t, int64_t>> spans;   /* (first pair, count) per wave */
-  for (int64_t first = 0; first < n && rc == GDP_OK;) {
-    while (finish_oldest(false)) {}
-    if (rc != GDP_OK) break;
-    if (ctx->slot[cur].busy) {
-      /* every slot is in flight: the oldest must hand its records out first */
-      while (ctx->slot[cur].busy && rc == GDP_OK) finish_oldest(true);
-      if (rc != GDP_OK) break;
+  auto copy_out_loop = [&] {
+    cudaSetDevice(ctx->device);
+    for (;;) {
+      int k;
+      {
+        std::unique_lock<std::mutex> g(m);
+        cv.wait(g, [&] { return !launched.empty() || all_launched; });
+        if (launched.empty()) return;
+        k = launched.front();
+      }
+      hand_out(k);
     }
-    const int64_t count = wave_count(first, std::min(first == 0 ? first_wave : wave, n - first));
-    rc = arena_upto(first, count);
+  };
+  /* a batch of one wave hands out on this thread */
+  std::thread copy_out;
+  if (n > wave_cap) copy_out = std::thread(copy_out_loop);
+  int cur = 0;
+  for (int64_t first = 0; first < n;) {
+    if (copy_out.joinable()) {
+      /* every slot in flight: wait until the oldest has handed its records out */
+      std::unique_lock<std::mutex> g(m);
+      cv.wait(g, [&] { return !ctx->slot[cur].busy || out_rc != GDP_OK; });
+      if (out_rc != GDP_OK) break;
+    } else {
+      /* no copy-out thread (a batch meant for one wave, cut by the budget) */
+      while (ctx->slot[cur].busy && out_rc == GDP_OK) hand_out(launched.front());
+      if (out_rc != GDP_OK) break;
+    }
+    int64_t hi = 0;
+    const int64_t count = wave_count(first, std::min(wave_cap, n - first), &hi);
+    wave_cap = std::min(wave, 2 * wave_cap);
+    rc = arena_upto(first, hi);
     if (rc != GDP_OK) break;
     rc = slot_launch(ctx, ctx->slot[cur], pairs, first, count, arena_bytes, results, nullptr);
     if (rc != GDP_OK) break;
     spans.push_back({first, count});
     first += count;
-    order[inflight++] = cur;
+    {
+      std::lock_guard<std::mutex> g(m);
+      ctx->slot[cur].busy = true;
+      launched.push_back(cur);
+    }
+    cv.notify_all();
     cur = (cur + 1) % NSLOTS;
   }
-  while (rc == GDP_OK && inflight > 0) finish_oldest(true);
+  {
+    std::lock_guard<std::mutex> g(m);
+    all_launched = true;
+  }
+  cv.notify_all();
+  if (copy_out.joinable()) copy_out.join();
+  else copy_out_loop();
+  if (rc == GDP_OK) rc = out_rc;
+  GDP_TRACE_BEGIN(tdrain);
   cudaError_t e = cudaStreamSynchronize(ctx->d2h);
   cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  GDP_TRACE_END(tdrain, "drain");
+#ifdef GDP_HOST_TRACE
+  fprintf(stderr, "gdp-trace host_enqueue_done %.3f ms\n",
+          std::chrono::duration<double, std::milli>(tdrain - host0).count());
+  for (auto &t : gdp_tev) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, gdp_tev[0].ev, t.ev);
+    fprintf(stderr, "gdp-tev %8.3f %s (host %.3f)\n", ms, t.what,
+            std::chrono::duration<double, std::milli>(t.host - gdp_tev[0].host).count());
+  }
+#endif
   if (rc == GDP_OK && e != cudaSuccess) rc = set_err(ctx, "batch copies", e);
   if (rc == GDP_OK && e2 != cudaSuccess) rc = set_err(ctx, "batch kernels", e2);
   if (rc == GDP_OK) {
