@@ -435,8 +435,8 @@ traceback_entry (const char *name, int precision, int variant, List_T pairs, int
   const int64_t nrecs = std::min<int64_t>(res.nrecs, (int64_t) t.recs.size());
   for (int64_t k = 0; k < nrecs; k++) {
     const gdp_rec_t &x = t.recs[k];
-    if (x.genomejump != 0)
-      pairs = syms.gapholder(pairs, pool, 0, x.genomejump, nullptr, nullptr, 0);
+    if (x.comp == '\0')   /* gap holder: genomepos holds the skipped genome length */
+      pairs = syms.gapholder(pairs, pool, 0, x.genomepos, nullptr, nullptr, 0);
     else
       pairs = syms.push(pairs, pool, x.querypos, x.genomepos, x.cdna, x.comp, x.genome, x.genomealt,
                         dynprogindex);

@@ -961,8 +961,13 @@ compact_records_kernel (gdp_result_t *res, const int64_t *slot_off, const gdp_re
   for (int64_t i = warp; i < n; i += nwarps) {
     const int nr = res[i].nrecs;
     const int64_t dst = scan[i];
-    const gdp_rec_t *src = slots + slot_off[i];
-    for (int k = lane; k < nr; k += 32) out[dst + k] = src[k];
+    /* the pair's records as one run of 32-bit words, so a warp's stores
+       are contiguous */
+    static_assert(sizeof(gdp_rec_t) % 4 == 0, "records are whole words");
+    constexpr int RW = sizeof(gdp_rec_t) / 4;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(slots + slot_off[i]);
+    uint32_t *to = reinterpret_cast<uint32_t *>(out + dst);
+    for (int k = lane; k < nr * RW; k += 32) to[k] = src[k];
     if (lane == 0) {
       res[i].rec_offset = dst;
       if (i == n - 1) {

@@ -158,7 +158,7 @@ struct TbState {
     if (qpos < 0 || gpos < 0) return;   /* Pairpool_push drops these (:189-191) */
     if (n < cap) {
       gdp_rec_t r;
-      r.querypos = qpos; r.genomepos = gpos; r.genomejump = 0;
+      r.querypos = qpos; r.genomepos = gpos;
       r.cdna = cdna; r.comp = comp; r.genome = g; r.genomealt = ga;
       out[n] = r;
     } else {
@@ -169,8 +169,8 @@ struct TbState {
   __device__ void gapholder (int dist) {
     if (n < cap) {
       gdp_rec_t r;
-      r.querypos = -1; r.genomepos = -1; r.genomejump = dist;
-      r.cdna = ' '; r.comp = ' '; r.genome = ' '; r.genomealt = ' ';
+      r.querypos = -1; r.genomepos = dist;   /* gap holder: comp '\0' */
+      r.cdna = ' '; r.comp = '\0'; r.genome = ' '; r.genomealt = ' ';
       out[n] = r;
     } else {
       err = GDP_ERR_RECS;

@@ -45,7 +45,7 @@ struct WarpTb {
     if (keep) {
       if (idx < cap) {
         gdp_rec_t r;
-        r.querypos = qpos; r.genomepos = gpos; r.genomejump = 0;
+        r.querypos = qpos; r.genomepos = gpos;
         r.cdna = cdna; r.comp = comp; r.genome = g; r.genomealt = ga;
         out[idx] = r;
       } else {
@@ -59,8 +59,8 @@ struct WarpTb {
     if (n < cap) {
       if (lane == 0) {
         gdp_rec_t r;
-        r.querypos = -1; r.genomepos = -1; r.genomejump = dist;
-        r.cdna = ' '; r.comp = ' '; r.genome = ' '; r.genomealt = ' ';
+        r.querypos = -1; r.genomepos = dist;   /* gap holder: comp '\0' */
+        r.cdna = ' '; r.comp = '\0'; r.genome = ' '; r.genomealt = ' ';
         out[n] = r;
       }
     } else {

@@ -36,10 +36,10 @@ assert PAIR_DTYPE.itemsize == 88
 
 # struct gdp_rec, 16 bytes
 REC_DTYPE = np.dtype([
-    ("querypos", "<i4"), ("genomepos", "<i4"), ("genomejump", "<i4"),
+    ("querypos", "<i4"), ("genomepos", "<i4"),
     ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1"),
 ])
-assert REC_DTYPE.itemsize == 16
+assert REC_DTYPE.itemsize == 12
 
 # struct gdp_result, 48 bytes
 RESULT_DTYPE = np.dtype([

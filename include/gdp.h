@@ -105,19 +105,23 @@ typedef struct gdp_pair {
 } gdp_pair_t;
 
 /*
- * One traceback Pair record (the fields of the reference's struct Pair_T,
- * src/pairdef.h:10-50, that Dynprog_traceback_* sets).  Records of a pair
- * are stored in push order: the first record is the one the reference
- * pushes first (nearest the traceback start).  A gap holder
- * (Pairpool_push_gapholder, src/pairpool.c:374) has querypos = genomepos =
- * -1 and genomejump = the skipped genome length; all other records have
- * genomejump = 0 and dynprogindex = the pair's dynprogindex.
+ * One traceback Pair record, 12 bytes: the fields of the reference's struct
+ * Pair_T (src/pairdef.h:10-50) that Dynprog_traceback_* sets.  Records of a
+ * pair are stored in push order: the first record is the one the reference
+ * pushes first (nearest the traceback start).  Pairpool_push records
+ * (src/pairpool.c:169) carry querypos, genomepos and the four characters;
+ * their dynprogindex is the pair's and their genomejump 0.  A gap holder
+ * (Pairpool_push_gapholder, src/pairpool.c:374; the reference's Pair has
+ * querypos = genomepos = -1, blank characters and genomejump = the skipped
+ * genome length) is the record with comp == '\0': querypos = -1, genomepos =
+ * the skipped genome length, cdna = genome = genomealt = ' '.  No pushed
+ * record has comp == '\0' (comp is one of the reference's comparison
+ * characters).
  */
 typedef struct gdp_rec {
   int32_t querypos;
-  int32_t genomepos;
-  int32_t genomejump;
-  char cdna, comp, genome, genomealt;
+  int32_t genomepos;     /* gap holder: the skipped genome length */
+  char cdna, comp, genome, genomealt;   /* gap holder: comp == '\0' */
 } gdp_rec_t;
 
 /* Per-pair result. */

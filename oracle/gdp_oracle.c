@@ -373,7 +373,7 @@ push (pool_t *P, int querypos, int genomepos, char cdna, char comp, char g, char
   if (querypos < 0 || genomepos < 0) return;   /* Pairpool_push (:189-191) */
   if (P->recs && P->n < P->cap) {
     gdp_rec_t *d = &P->recs[P->n];
-    d->querypos = querypos; d->genomepos = genomepos; d->genomejump = 0;
+    d->querypos = querypos; d->genomepos = genomepos;
     d->cdna = cdna; d->comp = comp; d->genome = g; d->genomealt = galt;
   }
   P->n++;
@@ -383,8 +383,8 @@ static void
 push_gapholder (pool_t *P, int dist) {
   if (P->recs && P->n < P->cap) {
     gdp_rec_t *d = &P->recs[P->n];
-    d->querypos = -1; d->genomepos = -1; d->genomejump = dist;
-    d->cdna = ' '; d->comp = ' '; d->genome = ' '; d->genomealt = ' ';
+    d->querypos = -1; d->genomepos = dist;   /* gap holder: comp '\0' */
+    d->cdna = ' '; d->comp = '\0'; d->genome = ' '; d->genomealt = ' ';
   }
   P->n++;
 }

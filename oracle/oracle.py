@@ -120,7 +120,7 @@ class CpuOracle:
 
 
 def _rec_dtype():
-    return np.dtype([("querypos", "<i4"), ("genomepos", "<i4"), ("genomejump", "<i4"),
+    return np.dtype([("querypos", "<i4"), ("genomepos", "<i4"),
                      ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1")])
 
 

@@ -309,11 +309,18 @@ run_traceback (refstate_t *st, const gdp_pair_t *p, const char *arena, fillout_t
       Pair_T pr = (Pair_T) q->first;
       if (k < max_recs) {
         gdp_rec_t *d = &recs[k];
-        d->querypos = pr->querypos;
-        d->genomepos = (int32_t) pr->genomepos;
-        d->genomejump = pr->genomejump;
-        d->cdna = pr->cdna;
-        d->comp = pr->comp;
+        if (pr->gapp) {
+          /* a gap holder: comp '\0', genomepos = the skipped genome length */
+          d->querypos = pr->querypos;
+          d->genomepos = pr->genomejump;
+          d->cdna = pr->cdna;
+          d->comp = '\0';
+        } else {
+          d->querypos = pr->querypos;
+          d->genomepos = (int32_t) pr->genomepos;
+          d->cdna = pr->cdna;
+          d->comp = pr->comp;
+        }
         d->genome = pr->genome;
         d->genomealt = pr->genomealt;
       }
