@@ -48,15 +48,63 @@ DIR_BYTES_PER_CELL = 0.5  # 4 direction bits per cell
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+    """Samples the SM clock and the clock-event (throttle) reasons while the
+    timed region runs: NVML read-only queries every 5 ms from a thread, with
+    one sample at start and one at stop, so even a region of a few tens of
+    milliseconds has samples.  Falls back to `nvidia-smi -lms 200`."""
+
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []            # (sm_mhz, max_mhz, reason bits or names)
         self.proc = None
         self.thread = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _handle(self, pynvml):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            for u in (uuid, "GPU-" + uuid):
+                try:
+                    return pynvml.nvmlDeviceGetHandleByUUID(u)
+                except Exception:
+                    pass
+        except Exception:
+            pass
+        return pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_sample(self):
+        p, h = self.nvml
+        sm = p.nvmlDeviceGetClockInfo(h, p.NVML_CLOCK_SM)
+        mx = p.nvmlDeviceGetMaxClockInfo(h, p.NVML_CLOCK_SM)
+        try:
+            bits = p.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            bits = p.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append((float(sm), float(mx), int(bits)))
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = (pynvml, self._handle(pynvml))
+            self._nvml_sample()
+        except Exception:
+            self.nvml = None
+        if self.nvml:
+            def poll():
+                while not self.stop_flag.wait(0.005):
+                    try:
+                        self._nvml_sample()
+                    except Exception:
+                        return
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -71,29 +119,42 @@ class ClockSampler:
         self.thread.start()
 
     def _read(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            if len(r) > 2 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                active = {n for k, n in enumerate(names) if len(r) > 5 + k and r[5 + k].lower() == "active"}
+                self.rows.append((float(r[1]), float(r[2]), active))
 
     def stop(self):
+        self.stop_flag.set()
+        if self.nvml:
+            if self.thread:
+                self.thread.join(timeout=2)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        if self.thread:
-            self.thread.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+            if self.thread:
+                self.thread.join(timeout=2)
         reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            for k, name in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower() == "active":
-                    reasons.add(name)
+        for _, _, r in self.rows:
+            if isinstance(r, int):
+                reasons |= {n for n, b in self.REASONS.items() if r & b}
+            else:
+                reasons |= r
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows]
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def dist_setup(args):
