@@ -246,14 +246,22 @@ struct Slot {
   PlanHost h;
   PlanDev d;
   DevBuf pairs, results, recs;
+  /* the stream the wave's kernels run on (one of the context's wave
+     streams) and the slot's own scratch, so consecutive waves overlap on
+     the device (one wave's tail beside the next wave's start) */
+  cudaStream_t cs = nullptr;
+  DevBuf scratch;
   HostBuf total;           /* pinned int64: records of the wave */
   cudaEvent_t h2d_done = nullptr, comp_done = nullptr, out_done = nullptr, total_ready = nullptr;
   int64_t first = 0, count = 0, rec_base = 0;
   bool busy = false;
 };
 
+#define GDP_MAX_WAVE_STREAMS 6
 struct gdp_ctx {
   int device = 0;
+  cudaStream_t wave_stream[GDP_MAX_WAVE_STREAMS] = {};   /* gdp_align_batch's compute, highest priority first */
+  int nwave = 0;
   int nsm = 148;
   cudaStream_t stream = nullptr;        /* compute */
   cudaStream_t h2d = nullptr, d2h = nullptr;
@@ -362,6 +370,7 @@ gdp_version (void) {
 
 static void
 slot_release (Slot &sl) {
+  if (sl.cs) cudaStreamSynchronize(sl.cs);
   sl.d.release();
   sl.h.release();
   sl.pairs.release(); sl.results.release(); sl.recs.release(); sl.total.release();
@@ -370,6 +379,8 @@ slot_release (Slot &sl) {
   if (sl.out_done) cudaEventDestroy(sl.out_done);
   if (sl.total_ready) cudaEventDestroy(sl.total_ready);
   sl.h2d_done = sl.comp_done = sl.out_done = sl.total_ready = nullptr;
+  sl.cs = nullptr;
+  sl.scratch.release();
 }
 
 extern "C" void
@@ -381,6 +392,11 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
   for (auto &t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
   for (int s = 0; s < NSLOTS; s++) slot_release(ctx->slot[s]);
+  for (int k = 0; k < GDP_MAX_WAVE_STREAMS; k++)
+    if (ctx->wave_stream[k]) {
+      cudaStreamSynchronize(ctx->wave_stream[k]);
+      cudaStreamDestroy(ctx->wave_stream[k]);
+    }
   ctx->arena.release(); ctx->scratch.release();
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
@@ -416,6 +432,19 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
       cudaEventCreateWithFlags(&ctx->join_ev[1], cudaEventDisableTiming) != cudaSuccess) {
     gdp_ctx_destroy(ctx);
     return GDP_ERR_CUDA;
+  }
+  /* Wave streams, one per stream priority from the highest down: wave k of
+     a batch computes on stream min(k, last), so when waves overlap the
+     pending blocks of an older wave go before a younger wave's. */
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  ctx->nwave = std::max(1, std::min(GDP_MAX_WAVE_STREAMS, least - greatest + 1));
+  for (int k = 0; k < ctx->nwave; k++) {
+    if (cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
+      ctx->wave_stream[k] = nullptr;
+      gdp_ctx_destroy(ctx);
+      return GDP_ERR_CUDA;
+    }
   }
   for (int s = 0; s < NSLOTS; s++) {
     Slot &sl = ctx->slot[s];
@@ -1097,26 +1126,27 @@ launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_
    d_slots receives records at the plan's slot offsets. */
 static int
 plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
-          gdp_result_t *d_res, gdp_rec_t *d_slots) {
-  cudaStream_t s = ctx->stream;
+          gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t stream = nullptr, DevBuf *scratch_buf = nullptr) {
+  cudaStream_t s = stream ? stream : ctx->stream;
+  DevBuf &scratch = scratch_buf ? *scratch_buf : ctx->scratch;
   const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
   cudaEvent_t ev0 = nullptr;
-  prof_begin(ctx, &ev0);
+  prof_begin(ctx, &ev0, s);
   static_assert(NKINDS <= 256, "one block clears every 8-bit pass counter");
   init_results_kernel<<<(int) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
       d_res, pd.status.as<int32_t>(), d_pairs, n, pd.meta0.as<gdp_meta_t>(), pd.meta.as<gdp_meta_t>(),
       pd.work_counts.as<int32_t>(), NKINDS);
-  prof_end(ctx, PROF_INIT, ev0);
+  prof_end(ctx, PROF_INIT, ev0, s);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   if (ph.nwindow > 0) {
     cudaEvent_t evw = nullptr;
-    prof_begin(ctx, &evw);
+    prof_begin(ctx, &evw, s);
     window_kernel<<<(int) std::min<int64_t>(n, (int64_t) ctx->nsm * 16), 256, 0, s>>>(
         d_pairs, pd.status.as<int32_t>(), n, const_cast<char *>(d_arena), ctx->d_genome,
         ctx->d_genomealt ? ctx->d_genomealt : ctx->d_genome, ctx->genome_len);
-    prof_end(ctx, PROF_WINDOW, evw);
+    prof_end(ctx, PROF_WINDOW, evw, s);
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
@@ -1125,7 +1155,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     if (!ph.counts[k]) continue;
     need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
-  CK(ctx, ctx->scratch.ensure(std::max<size_t>(need, 64)));
+  CK(ctx, scratch.ensure(std::max<size_t>(need, 64)));
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs.
      The one-warp / one-CTA-per-pair kinds (no scratch) go first, on the
      two side streams, so that they run beside the one-thread-per-pair
@@ -1162,11 +1192,11 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
            pass (init_results_kernel cleared the counter) */
         const int cg = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
         cudaEvent_t evc = nullptr;
-        prof_begin(ctx, &evc);
+        prof_begin(ctx, &evc, s);
         compact_rerun_kernel<<<cg, 256, 0, s>>>(P.list, P.count, pd.meta.as<gdp_meta_t>(),
                                                 pd.work.as<int32_t>() + ph.start[k],
                                                 pd.work_counts.as<int32_t>() + k);
-        prof_end(ctx, PROF_RERUN, evc);
+        prof_end(ctx, PROF_RERUN, evc, s);
         ctx->launches++;
         CK(ctx, cudaGetLastError());
         P.list = pd.work.as<int32_t>() + ph.start[k];
@@ -1176,7 +1206,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.hdump = pd.hdump.as<int16_t>();
       P.meta = pd.meta.as<gdp_meta_t>();
       P.res = d_res;
-      P.scratch = ctx->scratch.as<int2>();
+      P.scratch = scratch.as<int2>();
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
@@ -1208,8 +1238,8 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
    pd.total. */
 static int
 compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_res, const gdp_rec_t *d_slots,
-                 gdp_rec_t *out, int64_t *total_host = nullptr) {
-  cudaStream_t s = ctx->stream;
+                 gdp_rec_t *out, int64_t *total_host = nullptr, cudaStream_t stream = nullptr) {
+  cudaStream_t s = stream ? stream : ctx->stream;
   const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
   CK(ctx, pd.nrec_scan.ensure((2 * n + 1) * sizeof(int64_t)));
@@ -1222,12 +1252,12 @@ compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_
   CK(ctx, cub::DeviceScan::ExclusiveSum(pd.cub_tmp.p, tmp, counts, pd.nrec_scan.as<int64_t>(), (int) n, s));
   ctx->launches++;
   cudaEvent_t ev = nullptr;
-  prof_begin(ctx, &ev);
+  prof_begin(ctx, &ev, s);
   const int grid = (int) std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, (int64_t) ctx->nsm * 16));
   compact_records_kernel<<<grid, 256, 0, s>>>(d_res, pd.rec_off.as<int64_t>(), d_slots,
                                               pd.nrec_scan.as<int64_t>(), n, out, pd.total.as<int64_t>(),
                                               total_host);
-  prof_end(ctx, PROF_RECS, ev);
+  prof_end(ctx, PROF_RECS, ev, s);
   ctx->launches++;
   CK(ctx, cudaGetLastError());
   return GDP_OK;
@@ -1393,7 +1423,7 @@ gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char 
    the host knows their count (slot_finish). */
 static int
 slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int64_t count,
-             int64_t arena_bytes, gdp_result_t *results, cudaEvent_t arena_ready) {
+             int64_t arena_bytes, gdp_result_t *results, cudaEvent_t arena_ready, int wave_index) {
   /* the slot's host plan buffers are free once their last upload ended */
   GDP_TRACE_BEGIN(t0);
   CK(ctx, cudaEventSynchronize(sl.h2d_done));
@@ -1418,11 +1448,12 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   if (rc != GDP_OK) return rc;
   CK(ctx, cudaEventRecord(sl.h2d_done, ctx->h2d));
   GDP_TEV(ctx->h2d, "h2d_end %lld", first);
-  CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.h2d_done, 0));
-  if (arena_ready) CK(ctx, cudaStreamWaitEvent(ctx->stream, arena_ready, 0));
-  GDP_TEV(ctx->stream, "comp_begin %lld", first);
+  sl.cs = ctx->wave_stream[std::min(wave_index, ctx->nwave - 1)];
+  CK(ctx, cudaStreamWaitEvent(sl.cs, sl.h2d_done, 0));
+  if (arena_ready) CK(ctx, cudaStreamWaitEvent(sl.cs, arena_ready, 0));
+  GDP_TEV(sl.cs, "comp_begin %lld", first);
   rc = plan_run(ctx, sl.h, sl.d, sl.pairs.as<gdp_pair_t>(), ctx->arena.as<char>(), sl.results.as<gdp_result_t>(),
-                sl.d.slots.as<gdp_rec_t>());
+                sl.d.slots.as<gdp_rec_t>(), sl.cs, &sl.scratch);
   if (rc != GDP_OK) return rc;
   /* the count reaches the host through a mapped pinned word written by the
      compaction kernel, not a copy on the compute stream (a copy engine busy
@@ -1431,12 +1462,20 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   CK(ctx, cudaHostGetDevicePointer((void **) &total_dev, sl.total.p, 0));
   *(volatile int64_t *) sl.total.p = 0;
   rc = compact_records(ctx, sl.h, sl.d, sl.results.as<gdp_result_t>(), sl.d.slots.as<gdp_rec_t>(),
-                       sl.recs.as<gdp_rec_t>(), total_dev);
+                       sl.recs.as<gdp_rec_t>(), total_dev, sl.cs);
   if (rc != GDP_OK) return rc;
-  GDP_TEV(ctx->stream, "comp_end %lld", first);
-  CK(ctx, cudaEventRecord(sl.total_ready, ctx->stream));
-  CK(ctx, cudaEventRecord(sl.comp_done, ctx->stream));
+  GDP_TEV(sl.cs, "comp_end %lld", first);
+  CK(ctx, cudaEventRecord(sl.total_ready, sl.cs));
+  CK(ctx, cudaEventRecord(sl.comp_done, sl.cs));
   return GDP_OK;
+}
+
+/* Adds the wave's first record (its base in the batch) to the record
+   offsets of the wave's results, on the copy-out stream before they leave. */
+__global__ void
+add_rec_base_kernel (gdp_result_t *res, int64_t n, int64_t base) {
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+    res[i].rec_offset += base;
 }
 
 /* Waits for the wave's record count and queues its results and records
@@ -1449,6 +1488,12 @@ slot_finish (gdp_ctx *ctx, Slot &sl, gdp_result_t *results, gdp_rec_t *recs, int
   CK(ctx, cudaEventSynchronize(sl.total_ready));
   GDP_TRACE_END(t0, "wait_total");
   CK(ctx, cudaStreamWaitEvent(ctx->d2h, sl.comp_done, 0));
+  if (*base != 0 && sl.count > 0) {
+    add_rec_base_kernel<<<(int) std::min<int64_t>((sl.count + 255) / 256, (int64_t) ctx->nsm * 4), 256, 0, ctx->d2h>>>(
+        sl.results.as<gdp_result_t>(), sl.count, *base);
+    ctx->launches++;
+    CK(ctx, cudaGetLastError());
+  }
   CK(ctx, cudaMemcpyAsync(results + sl.first, sl.results.p, sl.count * sizeof(gdp_result_t), cudaMemcpyDeviceToHost,
                           ctx->d2h));
   const int64_t total = sl.h.n > 0 ? *(volatile int64_t *) sl.total.p : 0;
@@ -1476,6 +1521,7 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   if (n <= 0) return GDP_OK;
   /* the previous batch may still be reading the arena */
   for (int s = 0; s < NSLOTS; s++) CK(ctx, cudaEventSynchronize(ctx->slot[s].out_done));
+  for (int k = 0; k < ctx->nwave; k++) CK(ctx, cudaStreamSynchronize(ctx->wave_stream[k]));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   CK(ctx, ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16)));
   const int64_t wave = std::max<int64_t>(1, ctx->wave);
@@ -1509,25 +1555,54 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
      budget (an upper bound per pair: every block sweeps at most
      W + lband + uband columns).  One pass finds the count and the end of the
      wave's sequences in the arena (*hi). */
+  auto pair_bytes = [&](const gdp_pair_t &p) -> int64_t {
+    const int64_t X = std::max(p.variant == GDP_LOWER ? p.glength : p.rlength, 0);
+    const int64_t band = std::max(p.lband, 0) + std::max(p.uband, 0);
+    int64_t b = 0;
+    if (p.precision == 16 || (p.flags & GDP_FLAG_RERUN16)) b += (X / 16 + 1) * (16 + band) * 8;
+    if (p.precision == 8) b += (X / 32 + 1) * (32 + band) * 16;
+    return b;
+  };
+  auto pair_end = [&](const gdp_pair_t &p) -> int64_t {
+    const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
+    return std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl));
+  };
+  /* The scan runs on the planner's threads, chunk by chunk; the first chunk
+     that would pass the budget is then walked pair by pair. */
   auto wave_count = [&](int64_t first, int64_t cap, int64_t *hi) -> int64_t {
-    int64_t bytes = 0, k = 0, h = 0;
-    for (; k < cap && first + k < n; k++) {
-      const gdp_pair_t &p = pairs[first + k];
-      const int64_t X = std::max(p.variant == GDP_LOWER ? p.glength : p.rlength, 0);
-      const int64_t band = std::max(p.lband, 0) + std::max(p.uband, 0);
-      int64_t b = 0;
-      if (p.precision == 16 || (p.flags & GDP_FLAG_RERUN16)) b += (X / 16 + 1) * (16 + band) * 8;
-      if (p.precision == 8) b += (X / 32 + 1) * (32 + band) * 16;
-      if (k > 0 && bytes + b > ctx->budget) break;
-      bytes += b;
-      const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
-      h = std::max(h, std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl)));
+    const int64_t m = std::min(cap, n - first);
+    const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, m / 16384));
+    std::vector<int64_t> cbytes(nt, 0), chi(nt, 0);
+    parallel_chunks(ctx->pool, m, nt, [&](int64_t lo, int64_t hi_, int t) {
+      int64_t b = 0, h = 0;
+      for (int64_t i = lo; i < hi_; i++) {
+        b += pair_bytes(pairs[first + i]);
+        h = std::max(h, pair_end(pairs[first + i]));
+      }
+      cbytes[t] = b;
+      chi[t] = h;
+    });
+    int64_t bytes = 0, h = 0, k = 0;
+    for (int t = 0; t < nt; t++) {
+      const int64_t lo = m * t / nt, hi_ = m * (t + 1) / nt;
+      if (bytes + cbytes[t] <= ctx->budget) {
+        bytes += cbytes[t];
+        h = std::max(h, chi[t]);
+        k = hi_;
+        continue;
+      }
+      for (int64_t i = lo; i < hi_; i++) {
+        const int64_t b = pair_bytes(pairs[first + i]);
+        if (i > 0 && bytes + b > ctx->budget) break;
+        bytes += b;
+        h = std::max(h, pair_end(pairs[first + i]));
+        k = i + 1;
+      }
+      break;
     }
     *hi = h;
     return std::max<int64_t>(k, 1);
   };
-  std::vector<std::pair<int64_t, int64_t>> bases;   /* (first pair, record base) per wave */
-  std::vector<std::pair<int64_t, int64_t>> spans;   /* (first pair, count) per wave */
   int64_t base = 0;
   bool overflow = false;
   int rc = GDP_OK;
@@ -1545,7 +1620,6 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
     const int r = out_rc == GDP_OK ? slot_finish(ctx, o, results, recs, max_recs, &base, &overflow) : out_rc;
     std::lock_guard<std::mutex> g(m);
     if (r != GDP_OK) out_rc = r;
-    bases.push_back({o.first, o.rec_base});
     o.busy = false;
     launched.pop_front();
     cv.notify_all();
@@ -1566,7 +1640,7 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   /* a batch of one wave hands out on this thread */
   std::thread copy_out;
   if (n > wave_cap) copy_out = std::thread(copy_out_loop);
-  int cur = 0;
+  int cur = 0, wave_index = 0;
   for (int64_t first = 0; first < n;) {
     if (copy_out.joinable()) {
       /* every slot in flight: wait until the oldest has handed its records out */
@@ -1583,9 +1657,8 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
     wave_cap = std::min(wave, 2 * wave_cap);
     rc = arena_upto(first, hi);
     if (rc != GDP_OK) break;
-    rc = slot_launch(ctx, ctx->slot[cur], pairs, first, count, arena_bytes, results, nullptr);
+    rc = slot_launch(ctx, ctx->slot[cur], pairs, first, count, arena_bytes, results, nullptr, wave_index++);
     if (rc != GDP_OK) break;
-    spans.push_back({first, count});
     first += count;
     {
       std::lock_guard<std::mutex> g(m);
@@ -1605,7 +1678,11 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   if (rc == GDP_OK) rc = out_rc;
   GDP_TRACE_BEGIN(tdrain);
   cudaError_t e = cudaStreamSynchronize(ctx->d2h);
-  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e2 = cudaSuccess;
+  for (int k = 0; k < ctx->nwave; k++) {
+    const cudaError_t ek = cudaStreamSynchronize(ctx->wave_stream[k]);
+    if (e2 == cudaSuccess) e2 = ek;
+  }
   GDP_TRACE_END(tdrain, "drain");
 #ifdef GDP_HOST_TRACE
   fprintf(stderr, "gdp-trace host_enqueue_done %.3f ms\n",
@@ -1619,17 +1696,8 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
 #endif
   if (rc == GDP_OK && e != cudaSuccess) rc = set_err(ctx, "batch copies", e);
   if (rc == GDP_OK && e2 != cudaSuccess) rc = set_err(ctx, "batch kernels", e2);
-  if (rc == GDP_OK) {
-    /* record offsets of each wave are relative to the wave's first record */
-    std::sort(bases.begin(), bases.end());
-    std::sort(spans.begin(), spans.end());
-    for (size_t w = 0; w < bases.size() && w < spans.size(); w++) {
-      const int64_t f = spans[w].first, end = f + spans[w].second, b = bases[w].second;
-      if (b != 0)
-        for (int64_t i = f; i < end; i++) results[i].rec_offset += b;
-    }
-    if (overflow) rc = GDP_ERR_RECS;
-  }
+  /* record offsets are batch-wide: add_rec_base_kernel moved each wave's */
+  if (rc == GDP_OK && overflow) rc = GDP_ERR_RECS;
   if (nrecs_used) *nrecs_used = base;
   return rc;
 }
