@@ -62,6 +62,12 @@ struct FillParams {
   int64_t nslots;
   int scratch_rows;        /* columns available per slot */
   const gdp_tables_t *tab;
+  /* Byte k: for mismatch type k, the smallest row and column index at which
+     an in-band score can reach 127 (at most 255).  Every score is the score
+     of a path from the matrix corner, so H(r, c) <= min(r, c) times the
+     table's largest entry.  The in-band 127 checks (MODE != 0) skip cells
+     below it; 0 checks every cell. */
+  uint32_t reach_from4;
 };
 
 /* Lanes lo..hi (0 <= lo <= hi <= 31) as a bit mask. */
@@ -89,6 +95,7 @@ struct PairView {
   bool revp;
   int open, ext, oe, mt, lband, uband;
   int dlo, dhi;                  /* in-band lanes of column y: y - dhi <= x <= y + dlo */
+  int reach_from;                /* FillParams::reach_from of the pair's mismatch type */
   const char *lseq, *lalt, *sseq, *salt;
   int llen, slen;
 };
@@ -285,7 +292,7 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
   } else {
     out = make_int2(B.H[W - 1], 0);
   }
-  if (MODE != 0 && !reached && y >= 1) {
+  if (MODE != 0 && !reached && y >= 1 && y >= v.reach_from && xlo + last >= v.reach_from) {
     const int dl = max(rel - v.dhi, (xlo == 0) ? 1 : 0), dh = min(rel + v.dlo, last);
     if (dh >= dl) {
       const uint32_t dom = lane_range(max(dl, 0), dh);
@@ -347,12 +354,13 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
  * diagonal fix).  Those columns need none of the lane masks of
  * block_column, and in the bands of long pairs they are most of the work.
  * The result equals block_column's for the same column.  `vmax` collects
- * the in-band scores (MODE != 0).
+ * the in-band scores (MODE != 0) when `track` says that the column and the
+ * block can hold a score of 127 (FillParams::reach_from).
  */
 template <int W, int VARIANT, bool LATE, int MODE>
 __device__ __forceinline__ int2
 block_column_steady (Block<W> &B, const PairView &v, int diag, int2 above, int ka, int kb, uint32_t *dcol,
-                     int &vmax) {
+                     int &vmax, bool track) {
   constexpr int LO = (W == 32) ? -128 : -32768;
   constexpr int HI = (W == 32) ? 127 : 32767;
   constexpr int WORDS = W / 8;
@@ -407,7 +415,7 @@ block_column_steady (Block<W> &B, const PairView &v, int diag, int2 above, int k
   } else {
     out = make_int2(B.H[W - 1], 0);
   }
-  if (MODE != 0) {
+  if (MODE != 0 && track) {
 #pragma unroll
     for (int i = 0; i < W; i++) vmax = max(vmax, B.H[i]);
   }
@@ -472,6 +480,7 @@ fill_thread_kernel (FillParams P) {
     }
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
+    v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
     uint32_t *dir = P.dirs + ((W == 16) ? mp->dir16 : mp->dir8);
     int2 *sc = P.scratch + slot;
     const int64_t scs = P.nslots;
@@ -507,7 +516,8 @@ fill_thread_kernel (FillParams P) {
         int2 out;
         if constexpr ((W == 16 && MODE != 2 && GDP_STEADY) || (W == 32 && GDP_STEADY8)) {
           if (hd == nullptr && B.last == W - 1 && y >= 1 && y != v.g.Y && column_steady<W, VARIANT, MODE>(v, xlo, y)) {
-            out = block_column_steady<W, VARIANT, LATE, MODE>(B, v, diag, above, ka, kb, dcol, vmax);
+            out = block_column_steady<W, VARIANT, LATE, MODE>(B, v, diag, above, ka, kb, dcol, vmax,
+                                                              y >= v.reach_from && xlo + W - 1 >= v.reach_from);
             if (MODE == 2 && vmax >= 127) reached = true;
           } else
             out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
@@ -572,6 +582,7 @@ fill_warp_kernel (FillParams P) {
     gdp_meta_t *mp = valid ? P.meta + pi : nullptr;
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
+    v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
     uint32_t *dir = valid ? P.dirs + ((W == 16) ? mp->dir16 : mp->dir8) : nullptr;
     /* blocks that sweep something: 0 .. nb - 1 */
     int nb = 0, tend = -1;
@@ -667,6 +678,7 @@ fill_cta_kernel (FillParams P) {
     gdp_meta_t *mp = P.meta + pi;
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
+    v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
     uint32_t *dir = P.dirs + mp->dir16;
     int nb = v.g.X / W + 1;
     while (nb > 0) {

@@ -190,6 +190,7 @@ gdp_fill16_noalloc (int device, int mode, const gdp_pair_t *d_pairs, int64_t npa
   P.nslots = GDP_NOALLOC_SLOTS;
   P.scratch_rows = GDP_NOALLOC_MAX_COLS;
   P.tab = tables;
+  P.reach_from4 = 0;
   P.list = list_late;
   P.count = counts;
   fill_thread_kernel<16, GDP_FULL, true, 0><<<GDP_NOALLOC_BLOCKS, GDP_NOALLOC_THREADS, 0, s>>>(P);

@@ -270,6 +270,7 @@ struct gdp_ctx {
   cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
+  int reach_from[4] = {0, 0, 0, 0};   /* FillParams::reach_from of h_tab */
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
@@ -351,6 +352,19 @@ prof_end (gdp_ctx *ctx, int id, cudaEvent_t a, cudaStream_t s = nullptr) {
   cudaEventCreate(&b);
   cudaEventRecord(b, s ? s : ctx->stream);
   ctx->timed.push_back({id, a, b});
+}
+
+/* Per mismatch type, the smallest row and column index at which a score
+   can reach 127 under h_tab: every score is a path score from the matrix
+   corner, at most min(r, c) times the table's largest entry. */
+static void
+update_reach (gdp_ctx *ctx) {
+  for (int mt = 0; mt < 4; mt++) {
+    int mx = -32768;
+    for (int a = 0; a < 128; a++)
+      for (int b = 0; b < 128; b++) mx = std::max(mx, (int) ctx->h_tab->pd[mt][a][b]);
+    ctx->reach_from[mt] = (mx <= 0) ? (1 << 30) : (127 + mx - 1) / mx;
+  }
 }
 
 static int
@@ -456,6 +470,7 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   }
   ctx->h_tab = (gdp_tables_t *) malloc(sizeof(gdp_tables_t));
   gdp_build_tables(ctx->h_tab, mode);
+  update_reach(ctx);
   if (cudaMalloc(&ctx->d_tab, sizeof(gdp_tables_t)) != cudaSuccess ||
       cudaMemcpy(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice) != cudaSuccess) {
     gdp_ctx_destroy(ctx);
@@ -1210,6 +1225,8 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
+      P.reach_from4 = 0;
+      for (int q = 0; q < 4; q++) P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
       cudaStream_t ks = s;
       if (warp || cta) {
         if (!forked) {
@@ -1922,6 +1939,7 @@ gdpi_set_tables (gdp_ctx *ctx, const gdp_tables_t *t) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
   memcpy(ctx->h_tab, t, sizeof(gdp_tables_t));
+  update_reach(ctx);
   CK(ctx, cudaMemcpyAsync(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GDP_OK;
