@@ -329,14 +329,11 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
     mp->final16 = final_score;
   }
   if (MODE == 2) {
+    /* the result takes the 8-bit outcome after both passes
+       (apply_rerun8_kernel): the two may run at the same time */
     const bool overflow = reached || final_score <= -128 + 30;
     mp->status8 = overflow ? 1 : 0;
     mp->final8 = final_score;
-    if (!overflow) {
-      P.res[pi].score = final_score;
-      P.res[pi].precision = 8;
-      P.res[pi].rerun = 0;
-    }
   } else {
     gdp_result_t *r = P.res + pi;
     r->score = final_score;
@@ -742,6 +739,25 @@ fill_cta_kernel (FillParams P) {
     }
     if (L == ((v.g.X / W) % NL)) fill_finish<W, 0>(P, pi, mp, v.g, false, final_score);
     __syncthreads();
+  }
+}
+
+/* After both passes of the rerun pairs in `list`: a pair whose 16-bit
+   scores stayed below 127 and whose 8-bit fill did not overflow keeps the
+   8-bit outcome (score, precision 8, no rerun); the others keep the 16-bit
+   outcome the 16-bit pass wrote. */
+static __global__ void
+apply_rerun8_kernel (const int32_t *list, const int32_t *count, const gdp_meta_t *meta, gdp_result_t *res) {
+  const int n = *count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int pi = list[i];
+    if (pi < 0) continue;
+    const gdp_meta_t m = meta[pi];
+    if (m.maxh16 < 127 && m.status8 == 0) {
+      res[pi].score = m.final8;
+      res[pi].precision = 8;
+      res[pi].rerun = 0;
+    }
   }
 }
 

@@ -92,9 +92,11 @@ constexpr int WARP_K[3] = {8, 16, 32};
 constexpr int NWARP8KINDS = 18;    /* K lanes per pair, 8-bit pass of rerun pairs: 42 + (variant * 2 + late) * 3 + log2(K) - 2 */
 constexpr int WARP8_K[3] = {4, 8, 16};
 constexpr int NCTAKINDS = 24;      /* one CTA per pair (16-bit plain): 60 + (variant * 2 + late) * 4 + log2(NW) - 1 */
+constexpr int NEARLY8KINDS = 6;    /* one thread per pair, 8-bit pass beside the 16-bit pass: 84 + variant * 2 + late */
 constexpr int FIRST_WARP8 = NTHREADKINDS + NWARPKINDS;
 constexpr int FIRST_CTA = FIRST_WARP8 + NWARP8KINDS;
-constexpr int NKINDS = FIRST_CTA + NCTAKINDS;
+constexpr int FIRST_EARLY8 = FIRST_CTA + NCTAKINDS;
+constexpr int NKINDS = FIRST_EARLY8 + NEARLY8KINDS;
 constexpr int CTA_NW[4] = {2, 4, 8, 16};
 
 inline int kind_id (int w32, int variant, int late, int pass) {
@@ -111,6 +113,10 @@ inline int warp8_kind_id (int variant, int late, int kg) {
 
 inline int cta_kind_id (int variant, int late, int nwi) {
   return FIRST_CTA + (variant * 2 + late) * 4 + nwi;
+}
+
+inline int early8_kind_id (int variant, int late) {
+  return FIRST_EARLY8 + variant * 2 + late;
 }
 
 }  // namespace
@@ -250,7 +256,7 @@ struct Slot {
      streams) and the slot's own scratch, so consecutive waves overlap on
      the device (one wave's tail beside the next wave's start) */
   cudaStream_t cs = nullptr;
-  DevBuf scratch;
+  DevBuf scratch, scratch8;
   HostBuf total;           /* pinned int64: records of the wave */
   cudaEvent_t h2d_done = nullptr, comp_done = nullptr, out_done = nullptr, total_ready = nullptr;
   int64_t first = 0, count = 0, rec_base = 0;
@@ -280,8 +286,9 @@ struct gdp_ctx {
   bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
   int group_slack = 48;     /* lane groups of K lanes take sweeps up to 17 K - group_slack columns */
   int plan_threads = 8;     /* host threads of the planner */
-  bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) */
-  DevBuf arena, scratch;
+  bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) ... */
+  int check_min_x = 1 << 30; /* ... or only for pairs with at least this many rows (lower: columns) */
+  DevBuf arena, scratch, scratch8;
   Slot slot[NSLOTS];
   WorkPool pool;            /* the planner's host threads */
   std::atomic<int64_t> launches{0};
@@ -313,6 +320,12 @@ kernel_name (int id) {
   if (id == PROF_RERUN) return "compact_rerun_kernel";
   if (id == PROF_RECS) return "compact_records_kernel";
   if (id == PROF_WINDOW) return "window_kernel";
+  if (id >= FIRST_EARLY8) {
+    const int c = id - FIRST_EARLY8, variant = c / 2, late = c & 1;
+    snprintf(buf[id], sizeof(buf[id]), "fill_thread<W32,%s,%s,8bit-check-early>",
+             variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early");
+    return buf[id];
+  }
   if (id >= FIRST_CTA) {
     const int c = id - FIRST_CTA, vl = c / 4, variant = vl / 2, late = vl & 1;
     snprintf(buf[id], sizeof(buf[id]), "fill_cta<W16,%s,%s,%dwarps>",
@@ -395,6 +408,7 @@ slot_release (Slot &sl) {
   sl.h2d_done = sl.comp_done = sl.out_done = sl.total_ready = nullptr;
   sl.cs = nullptr;
   sl.scratch.release();
+  sl.scratch8.release();
 }
 
 extern "C" void
@@ -411,7 +425,7 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
       cudaStreamSynchronize(ctx->wave_stream[k]);
       cudaStreamDestroy(ctx->wave_stream[k]);
     }
-  ctx->arena.release(); ctx->scratch.release();
+  ctx->arena.release(); ctx->scratch.release(); ctx->scratch8.release();
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
   if (ctx->d_genomealt) cudaFree(ctx->d_genomealt);
@@ -815,13 +829,19 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       }
       if (p.precision == 8) {
         int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
-        if (rerun && ctx->check_groups) {
-          /* the 8-bit pass runs for few pairs: lane groups give it the whole device */
-          gdp_geom_t g8;
-          gdp_geom_of(&p, 32, &g8);
+        gdp_geom_t g8;
+        gdp_geom_of(&p, 32, &g8);
+        if (rerun && (ctx->check_groups || g8.X >= ctx->check_min_x)) {
+          /* the 8-bit pass runs for few pairs, and its time is that of the
+             longest: lane groups give a long pair K lanes */
           const int sweep8 = 31 + g8.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
           for (int q = 0; q < 3; q++)
             if (sweep8 <= WARP8_K[q] * 33 - ctx->group_slack) { k = warp8_kind_id(p.variant, late, q); break; }
+        } else if (rerun && std::min(p.rlength, p.glength) < ctx->reach_from[p.mismatchtype & 3]) {
+          /* no score of this pair can reach 127 (a score is at most
+             min(r, c) times the largest table entry), so its 8-bit pass
+             does not wait for the 16-bit pass: it runs beside it */
+          k = early8_kind_id(p.variant, late);
         }
         m.dir8 = (gdp_pair_words(&p, 32) + 3) & ~(int64_t) 3;
         c.words += m.dir8;
@@ -1101,6 +1121,16 @@ launch_warp8_kind (int k, FillParams P, int grid, cudaStream_t s) {
   else { if (late) launch_warp8<GDP_LOWER, true>(kg, P, grid, s); else launch_warp8<GDP_LOWER, false>(kg, P, grid, s); }
 }
 
+/* the 8-bit pass of rerun pairs that cannot reach 127, one thread per pair,
+   beside the 16-bit pass */
+static void
+launch_early8_kind (int k, FillParams P, int grid, cudaStream_t s) {
+  const int c = k - FIRST_EARLY8, variant = c / 2, late = c & 1;
+  if (variant == GDP_FULL) { if (late) launch_fill<32, GDP_FULL, true, 2>(P, grid, s); else launch_fill<32, GDP_FULL, false, 2>(P, grid, s); }
+  else if (variant == GDP_UPPER) { if (late) launch_fill<32, GDP_UPPER, true, 2>(P, grid, s); else launch_fill<32, GDP_UPPER, false, 2>(P, grid, s); }
+  else { if (late) launch_fill<32, GDP_LOWER, true, 2>(P, grid, s); else launch_fill<32, GDP_LOWER, false, 2>(P, grid, s); }
+}
+
 static void
 launch_warp_kind (int k, FillParams P, int grid, cudaStream_t s) {
   const int c = k - NTHREADKINDS, vl = c / 3, variant = vl / 2, late = vl & 1, kg = c % 3;
@@ -1141,9 +1171,11 @@ launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_
    d_slots receives records at the plan's slot offsets. */
 static int
 plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
-          gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t stream = nullptr, DevBuf *scratch_buf = nullptr) {
+          gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t stream = nullptr, DevBuf *scratch_buf = nullptr,
+          DevBuf *scratch8_buf = nullptr) {
   cudaStream_t s = stream ? stream : ctx->stream;
   DevBuf &scratch = scratch_buf ? *scratch_buf : ctx->scratch;
+  DevBuf &scratch8 = scratch8_buf ? *scratch8_buf : ctx->scratch8;   /* the early 8-bit kinds' own */
   const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
   cudaEvent_t ev0 = nullptr;
@@ -1165,12 +1197,17 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
-  size_t need = 0;
+  size_t need = 0, need8 = 0;
   for (int k = 0; k < NTHREADKINDS; k++) {
     if (!ph.counts[k]) continue;
     need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
+  for (int k = FIRST_EARLY8; k < NKINDS; k++) {
+    if (!ph.counts[k]) continue;
+    need8 = std::max(need8, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
+  }
   CK(ctx, scratch.ensure(std::max<size_t>(need, 64)));
+  if (need8 > 0) CK(ctx, scratch8.ensure(need8));
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs.
      The one-warp / one-CTA-per-pair kinds (no scratch) go first, on the
      two side streams, so that they run beside the one-thread-per-pair
@@ -1189,8 +1226,9 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       const int k = (round == 0) ? (kk + NTHREADKINDS) % NKINDS : kk;
       const bool warp = k >= NTHREADKINDS && k < FIRST_WARP8;
       const bool warp8 = k >= FIRST_WARP8 && k < FIRST_CTA;
-      const bool cta = k >= FIRST_CTA;
-      const bool thread = !warp && !warp8 && !cta;
+      const bool cta = k >= FIRST_CTA && k < FIRST_EARLY8;
+      const bool early8 = k >= FIRST_EARLY8;
+      const bool thread = !warp && !warp8 && !cta && !early8;
       const int w32 = thread ? (k >> 2) / 3 : 0, pass = thread ? (k & 1) : 0;
       const bool second = (w32 == 1 && pass == 1) || warp8;
       if ((round == 0) == second || !ph.counts[k]) continue;
@@ -1221,14 +1259,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.hdump = pd.hdump.as<int16_t>();
       P.meta = pd.meta.as<gdp_meta_t>();
       P.res = d_res;
-      P.scratch = scratch.as<int2>();
+      P.scratch = early8 ? scratch8.as<int2>() : scratch.as<int2>();
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
       P.reach_from4 = 0;
       for (int q = 0; q < 4; q++) P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
       cudaStream_t ks = s;
-      if (warp || cta) {
+      if (warp || cta || early8) {
         if (!forked) {
           for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(ctx->side[q], ctx->fork_ev, 0));
           forked = true;
@@ -1241,11 +1279,23 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       if (cta) launch_cta_kind(k, P, grid, ks);
       else if (warp) launch_warp_kind(k, P, grid, ks);
       else if (warp8) launch_warp8_kind(k, P, grid, ks);
+      else if (early8) launch_early8_kind(k, P, grid, ks);
       else launch_kind(k, P, grid, ks);
       prof_end(ctx, k, ev, ks);
       ctx->launches++;
       CK(ctx, cudaGetLastError());
     }
+  }
+  /* the 8-bit outcome of rerun pairs, after both of their passes */
+  for (int k = 0; k < NKINDS; k++) {
+    const bool check8 = (k < NTHREADKINDS && (k >> 2) / 3 == 1 && (k & 1)) || (k >= FIRST_WARP8 && k < FIRST_CTA) ||
+                        k >= FIRST_EARLY8;
+    if (!check8 || !ph.counts[k]) continue;
+    const int ag = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
+    apply_rerun8_kernel<<<ag, 256, 0, s>>>(pd.lists.as<int32_t>() + ph.start[k], pd.counts.as<int32_t>() + k,
+                                           pd.meta.as<gdp_meta_t>(), d_res);
+    ctx->launches++;
+    CK(ctx, cudaGetLastError());
   }
   if (ph.counts[NKINDS] > 0) return launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, s);
   return GDP_OK;
@@ -1335,6 +1385,7 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "group_slack") && value >= 16 && value <= 128) ctx->group_slack = (int) value;
   else if (!strcmp(name, "tb_warp")) ctx->tb_warp = value != 0;
   else if (!strcmp(name, "check_groups")) ctx->check_groups = value != 0;
+  else if (!strcmp(name, "check_min_x") && value >= 1) ctx->check_min_x = (int) std::min<int64_t>(value, 1 << 30);
   else if (!strcmp(name, "wave_pairs") && value >= 1) ctx->wave = value;
   else return GDP_ERR_PARAM;
   return GDP_OK;
@@ -1349,6 +1400,7 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "group_slack")) *value = ctx->group_slack;
   else if (!strcmp(name, "tb_warp")) *value = ctx->tb_warp ? 1 : 0;
   else if (!strcmp(name, "check_groups")) *value = ctx->check_groups ? 1 : 0;
+  else if (!strcmp(name, "check_min_x")) *value = ctx->check_min_x;
   else if (!strcmp(name, "wave_pairs")) *value = ctx->wave;
   else return GDP_ERR_PARAM;
   return GDP_OK;
@@ -1407,6 +1459,7 @@ gdp_autotune (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs, const char 
     {&ctx->warp_max_sweep, {272, 400, 496, 528}},
     {&tbw, {1, 0}},
     {&cg, {1, 0}},
+    {&ctx->check_min_x, {96, 128, 160, 224, 1 << 30}},
   };
   double best = tune_trial(ctx, pairs, npairs, dp.as<gdp_pair_t>(), da.as<char>(), dr.as<gdp_result_t>(), drec, 2);
   int rc = best < 0 ? (int) -best : GDP_OK;
@@ -1470,7 +1523,7 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   if (arena_ready) CK(ctx, cudaStreamWaitEvent(sl.cs, arena_ready, 0));
   GDP_TEV(sl.cs, "comp_begin %lld", first);
   rc = plan_run(ctx, sl.h, sl.d, sl.pairs.as<gdp_pair_t>(), ctx->arena.as<char>(), sl.results.as<gdp_result_t>(),
-                sl.d.slots.as<gdp_rec_t>(), sl.cs, &sl.scratch);
+                sl.d.slots.as<gdp_rec_t>(), sl.cs, &sl.scratch, &sl.scratch8);
   if (rc != GDP_OK) return rc;
   /* the count reaches the host through a mapped pinned word written by the
      compaction kernel, not a copy on the compute stream (a copy engine busy

@@ -279,7 +279,7 @@ class Context:
         rc = self.lib.gdp_autotune(self.h, _ptr(pairs), pairs.size, _ptr(arena), arena.size, ctypes.byref(best))
         if rc != 0:
             raise RuntimeError(f"gdp_autotune: {STATUS.get(rc, rc)} {self.error()}")
-        names = ("warp_min_x", "warp_max_sweep", "group_slack", "tb_warp", "check_groups")
+        names = ("warp_min_x", "warp_max_sweep", "group_slack", "tb_warp", "check_groups", "check_min_x")
         return {k: self.get_param(k) for k in names}, best.value
 
     def int_peak(self):

@@ -209,11 +209,13 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *   "group_slack"    a group of K lanes takes sweeps up to 17 K - slack
  *   "tb_warp"        1: tracebacks with one warp per pair, 0: one thread
  *   "check_groups"   1: the 8-bit pass of rerun pairs on lane groups,
- *                    0: one thread per pair
+ *                    0: one thread per pair, except ...
+ *   "check_min_x"    ... pairs with at least this many lanes, whose 8-bit
+ *                    pass goes to lane groups all the same
  *   "wave_pairs"     pairs per wave of gdp_align_batch
  * gdp_autotune times plan executions of a sample batch (device-resident
  * copies, the caller's pairs and arena) under candidate values of the first
- * five, one parameter at a time, and keeps the fastest; *best_ms gets the
+ * six, one parameter at a time, and keeps the fastest; *best_ms gets the
  * sample's device time with the chosen values.  Results never depend on
  * these parameters.
  */

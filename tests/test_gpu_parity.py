@@ -109,8 +109,9 @@ def test_rerun_contract(env, gdplib, check_groups):
     whether the 8-bit pass runs one thread per pair or on lane groups."""
     ctx, ref, rest = env
     pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 31, GENOME['g'], 200)
-    keep = ctx.get_param("check_groups")
+    keep = ctx.get_param("check_groups"), ctx.get_param("check_min_x")
     ctx.set_param("check_groups", check_groups)
+    ctx.set_param("check_min_x", 1 << 30)
     try:
         ctx.profile(True)
         ctx.profile_reset()
@@ -124,7 +125,8 @@ def test_rerun_contract(env, gdplib, check_groups):
         kernels = ctx.profile_read()
         ctx.profile(False)
     finally:
-        ctx.set_param("check_groups", keep)
+        ctx.set_param("check_groups", keep[0])
+        ctx.set_param("check_min_x", keep[1])
     assert any("8bit-check" in k and k.startswith("fill_warp" if check_groups else "fill_thread")
                for k in kernels), kernels
 
@@ -221,3 +223,44 @@ def test_batch_determinism_and_launches(env, gdplib):
     r2, c2 = ctx.align(pairs, arena)
     assert mid > before
     assert r1.tobytes() == r2.tobytes() and c1.tobytes() == c2.tobytes()
+
+
+def test_rerun_long_pairs_on_lane_groups(env, gdplib):
+    """With check_min_x, the 8-bit pass of long rerun pairs runs on lane
+    groups and that of short ones one thread per pair, in one plan; both are
+    bit-exact under the rerun contract."""
+    ctx, ref, rest = env
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_SHORT, 33, GENOME['g'], 300)
+    keep = ctx.get_param("check_min_x")
+    ctx.set_param("check_min_x", 160)
+    try:
+        ctx.profile(True)
+        ctx.profile_reset()
+        fails = parity.check_fill(ctx, ref, pairs, arena)
+        assert not fails, "\n".join(fails)
+        fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+        assert not fails, "\n".join(fails)
+        kernels = ctx.profile_read()
+        ctx.profile(False)
+    finally:
+        ctx.set_param("check_min_x", keep)
+    assert any("8bit-check" in k and k.startswith("fill_warp") for k in kernels), kernels
+    assert any("8bit-check" in k and k.startswith("fill_thread") for k in kernels), kernels
+
+
+def test_rerun_short_pairs_beside_16bit_pass(env):
+    """Rerun pairs too short for any score to reach 127 run their 8-bit pass
+    beside the 16-bit pass (no wait for the 16-bit maximum); the kept
+    precision and every output follow the rerun contract bit for bit."""
+    ctx, ref, rest = env
+    pairs, arena = cases.random_cases(341, 300, precisions=(8,), min_len=1, max_len=42)
+    pairs["flags"] |= gdp.FLAG_RERUN16
+    ctx.profile(True)
+    ctx.profile_reset()
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+    kernels = ctx.profile_read()
+    ctx.profile(False)
+    assert any(k.endswith("8bit-check-early>") for k in kernels), kernels

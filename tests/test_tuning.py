@@ -73,12 +73,13 @@ def test_autotuned_routing_gives_identical_results(gdplib):
     ref, ref_recs = ctx.align(pairs, arena)
     params, best = ctx.autotune(pairs[:600], arena)
     assert best > 0
-    assert set(params) == {"warp_min_x", "warp_max_sweep", "group_slack", "tb_warp", "check_groups"}
+    assert set(params) == {"warp_min_x", "warp_max_sweep", "group_slack", "tb_warp", "check_groups", "check_min_x"}
     got, got_recs = ctx.align(pairs, arena)
     # a forced, very different routing gives the same results too
     ctx.set_param("warp_min_x", 1 << 30)
     ctx.set_param("tb_warp", 0)
     ctx.set_param("check_groups", 0)
+    ctx.set_param("check_min_x", 1 << 30)
     thr, thr_recs = ctx.align(pairs, arena)
     with pytest.raises(ValueError):
         ctx.set_param("no_such_parameter", 1)
