@@ -1271,8 +1271,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
           for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(ctx->side[q], ctx->fork_ev, 0));
           forked = true;
         }
-        ks = ctx->side[side];
-        side ^= 1;
+        if (early8) {
+          /* the early 8-bit kinds share one scratch: they stay in order on
+             one side stream */
+          ks = ctx->side[0];
+        } else {
+          ks = ctx->side[side];
+          side ^= 1;
+        }
       }
       cudaEvent_t ev = nullptr;
       prof_begin(ctx, &ev, ks);
