@@ -513,6 +513,16 @@ def run_gdp(args):
     hbm = None
     if os.path.exists(peaks_path):
         hbm = json.load(open(peaks_path)).get("hbm_gbs")
+    # DRAM bytes of the dominant kernel per launch: one ncu capture of the same
+    # kernel on 50,000 pairs of this workload (dram__bytes_read.sum +
+    # dram__bytes_write.sum = 123.70 + 266.46 MB over 300,657,762 in-band
+    # cells), scaled to this launch by its in-band cells; the kernel's bytes
+    # grow with the cells (directions and carries per swept cell)
+    traffic, traffic_src = None, None
+    if name == "short" and top_name.startswith("fill_thread<W16,full"):
+        traffic = int(round((123.696896e6 + 266.455296e6) / 300657762 * cells))
+        traffic_src = ("ncu capture of this kernel on 50,000 pairs (390.2 MB), scaled by in-band cells "
+                       "to this launch")
     if rank == 0:
         line = {
             "metric": "GCUPS (in-band cells, fill + traceback), batched",
@@ -533,7 +543,8 @@ def run_gdp(args):
                          "unit": "Tops/s (int32 lane-ops)", "frac": round(achieved_ops / int_peak, 4),
                          "peak_source": "measured int32 issue probe (gdp_measure_int_peak)",
                          "ops_per_cell": OPS_PER_CELL, "avg_launch_ms": round(avg_launch_ms, 3),
-                         "traffic": None,
+                         "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "dir_write_gbs": round(dir_bytes / (avg_launch_ms * 1e-3) / 1e9, 1),
                          "hbm_peak_gbs": hbm},
             "kernels": {k: {"ms_total": round(v[0], 3), "launches": v[1]} for k, v in prof.items()},
