@@ -251,6 +251,58 @@ def kept_precisions(lib, genome, blocks, pairs, arena, threads):
     return rest.kept_precision(pairs, arena, threads)
 
 
+def endpoint_search(lib, ctx, seed, ngaps=200000):
+    """End-gap endpoint search on the device: the short reads as end gaps
+    (an upper and a lower fill per gap, extraband 14 as Dynprog_compute_bands
+    gives end gaps), timed as one device-resident plan with and without the
+    search flags; the search's cost is the difference."""
+    import torch
+    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+    base, arena = gdp.make_pairs(lib, gdp.WL_SHORT, seed, genome, ngaps)
+    ctx.set_genome(blocks, None, genome.size)
+    rl, gl = base["rlength"].astype(np.int64), base["glength"].astype(np.int64)
+    pairs = np.repeat(base, 2)
+    up, lo = pairs[0::2], pairs[1::2]
+    up["variant"], lo["variant"] = gdp.UPPER, gdp.LOWER
+    up["uband"], up["lband"] = np.maximum(gl - rl, 0) + 14, 0
+    lo["lband"], lo["uband"] = np.maximum(rl - gl, 0) + 14, 0
+    pairs["precision"] = 16
+    keep = pairs["flags"] & gdp.FLAG_JUMP_LATE
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    d_arena = torch.from_numpy(arena).cuda()
+    d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    cells = int(gdp.band_cells(pairs).sum())
+    out = {"gaps": ngaps, "fills": int(pairs.size), "cells": cells}
+    for label, flags in (("plain", keep), ("endpoint", keep | gdp.FLAG_ENDPOINT)):
+        pairs["flags"] = flags
+        d_pairs.copy_(torch.from_numpy(pairs.view(np.uint8)))
+        plan = ctypes.c_void_p()
+        assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan)) == 0, ctx.error()
+        d_recs = torch.empty(16, dtype=torch.uint8, device="cuda")
+        run = lambda: lib.gdp_plan_execute(ctx.h, plan, ctypes.c_void_p(d_pairs.data_ptr()),
+                                           ctypes.c_void_p(d_arena.data_ptr()), ctypes.c_void_p(d_res.data_ptr()),
+                                           ctypes.c_void_p(d_recs.data_ptr()))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            run()
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b) / 5
+        lib.gdp_plan_destroy(plan)
+        res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+        out[label] = {"ms": round(ms, 3), "gcups": round(cells / (ms * 1e-3) / 1e9, 2),
+                      "bad_status": int((res["status"] != 0).sum())}
+        if label == "endpoint":
+            out[label]["halves_found"] = int(res["end_found"].sum())
+    out["search_overhead_pct"] = round(100 * (out["endpoint"]["ms"] / out["plain"]["ms"] - 1), 1)
+    return out
+
+
 def per_pair_vs_batched(lib, ctx, seed, npairs=20000, nsample=500):
     """The same mixed-length pairs (70/25/5 short/long/cDNA) aligned as one
     batch and as one plan per pair (every pair its own kernel launches),
@@ -506,6 +558,7 @@ def run_gdp(args):
     extra = {}
     if rank == 0 and world == 1 and not args.no_per_pair:
         extra["per_pair_vs_batched"] = per_pair_vs_batched(lib, ctx, args.seed + 7)
+        extra["endpoint_search"] = endpoint_search(lib, ctx, args.seed + 9)
     if rank == 0 and world == 1 and not args.no_serving:
         extra["serving"] = serving_sweep(lib, local, args.seed + 8,
                                          [1e3, 1e4, 5e4, 1e5, 2e5, 3e5, 5e5, 1e6])

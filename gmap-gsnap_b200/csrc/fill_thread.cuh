@@ -96,6 +96,7 @@ struct PairView {
   int open, ext, oe, mt, lband, uband;
   int dlo, dhi;                  /* in-band lanes of column y: y - dhi <= x <= y + dlo */
   int reach_from;                /* FillParams::reach_from of the pair's mismatch type */
+  int endmode;                   /* 0, or 1 (GDP_FLAG_ENDPOINT), or 2 (GDP_FLAG_ENDPOINT_QEND) */
   const char *lseq, *lalt, *sseq, *salt;
   int llen, slen;
 };
@@ -116,6 +117,69 @@ pair_view (const gdp_pair_t &p, const char *arena, PairView &v) {
   v.sseq = arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq);
   v.salt = arena + (VARIANT == GDP_LOWER ? p.rseq : p.gseq_alt);
   v.slen = (VARIANT == GDP_LOWER) ? p.rlength : p.glength;
+}
+
+/* One half of the end-gap endpoint search (GDP_FLAG_ENDPOINT*;
+   find_best_endpoint_{8,16}, src/dynprog_end.c:143-294, and
+   find_best_endpoint_to_queryend_indels_{8,16}, :358-508).  The reference
+   scans cells in row-then-column order and keeps the first best cell with
+   a score above the start (jump early) or the last one from the start up
+   (jump late).  That winner is the best score with the smallest (early) or
+   largest (late) (row, column) among the cells that pass, so the fill can
+   offer its cells in any order. */
+struct EndBest {
+  int score, r, c;
+  bool found;
+};
+
+template <bool LATE>
+__device__ __forceinline__ void
+end_offer (EndBest &b, int h, int r, int c, int start) {
+  if (LATE ? (h < start) : (h <= start)) return;
+  bool better;
+  if (!b.found || h > b.score) better = true;
+  else if (h < b.score) better = false;
+  else if (LATE) better = (r > b.r) || (r == b.r && c > b.c);
+  else better = (r < b.r) || (r == b.r && c < b.c);
+  if (better) { b.score = h; b.r = r; b.c = c; b.found = true; }
+}
+
+/* Offers the cells of swept column y of block xlo to the search: upper
+   fills their cells with c >= r (lanes are rows), lower fills their cells
+   with c < r (lanes are genome columns); the last-row search takes row
+   rlength only.  H holds the column's final scores. */
+template <int W, int VARIANT, bool LATE, class BlockT>
+__device__ __forceinline__ void
+end_column (EndBest &b, const BlockT &B, const PairView &v, int y, int start) {
+  const int xlo = B.xlo, last = B.last;
+  if (y < 1) return;
+  int lo, hi;
+  if (VARIANT == GDP_UPPER) {
+    lo = max(1, y - v.uband) - xlo;
+    hi = min(y, v.g.X) - xlo;
+    if (v.endmode == 2) lo = max(lo, v.g.X - xlo), hi = min(hi, v.g.X - xlo);
+  } else {
+    if (v.endmode == 2 && y != v.g.Y) return;
+    lo = max(1, y - v.lband) - xlo;
+    hi = min(y - 1, v.g.X) - xlo;
+  }
+  lo = max(lo, 0);
+  hi = min(hi, last);
+  if (lo > hi) return;
+  /* The column's own winner first: its cells share the column y, and the
+     lane order is the scan order among them (upper: rows; lower: genome
+     columns of one row), so the first lane with the column maximum (jump
+     early) or the last (jump late) is the one to offer. */
+  int cm = INT_MIN, ci = -1;
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    const int h = B.H[i];
+    const bool take = (i >= lo) & (i <= hi) & (LATE ? (h >= cm) : (h > cm));
+    cm = take ? h : cm;
+    ci = take ? i : ci;
+  }
+  if (VARIANT == GDP_UPPER) end_offer<LATE>(b, cm, xlo + ci, y, start);
+  else end_offer<LATE>(b, cm, y, xlo + ci, start);
 }
 
 /* Classes (0..4) of swept column y for the two genome strings (lower: the
@@ -320,7 +384,8 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
 /* Writes the per-pair outcome of a fill (see MODE). */
 template <int W, int MODE>
 __device__ __forceinline__ void
-fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, bool reached, int final_score) {
+fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, bool reached, int final_score,
+             const EndBest *eb = nullptr) {
   int y0l, y1l;
   gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
   const bool swept = (g.Y >= y0l && g.Y <= y1l);   /* the final cell was filled */
@@ -339,7 +404,15 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
     r->score = final_score;
     r->precision = W == 16 ? 16 : 8;
     r->rerun = (MODE == 1) ? 1 : 0;
-    if (!swept) r->status = GDP_ERR_BAND;
+    /* an end-gap half needs no final cell: the lower matrix of a gap with
+       glength > rlength, for one, holds none (score stays NEG_INFINITY) */
+    if (!swept && eb == nullptr) r->status = GDP_ERR_BAND;
+    if (eb != nullptr) {
+      r->end_score = eb->score;
+      r->end_r = eb->r;
+      r->end_c = eb->c;
+      r->end_found = eb->found ? 1 : 0;
+    }
   }
 }
 
@@ -478,6 +551,10 @@ fill_thread_kernel (FillParams P) {
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
     v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
+    v.endmode = (VARIANT == GDP_FULL) ? 0 : (p.flags & GDP_FLAG_ENDPOINT) ? 1 : (p.flags & GDP_FLAG_ENDPOINT_QEND) ? 2 : 0;
+    EndBest eb;
+    eb.score = 0; eb.r = 0; eb.c = 0; eb.found = false;
+    const int end_start = (v.endmode == 2) ? LO : 0;
     uint32_t *dir = P.dirs + ((W == 16) ? mp->dir16 : mp->dir8);
     int2 *sc = P.scratch + slot;
     const int64_t scs = P.nslots;
@@ -523,6 +600,7 @@ fill_thread_kernel (FillParams P) {
           out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached, final_score);
         }
         sc[(int64_t) y * scs] = out;
+        if (VARIANT != GDP_FULL && v.endmode != 0) end_column<W, VARIANT, LATE>(eb, B, v, y, end_start);
         dcol += WORDS;
         ka = ka2; kb = kb2; above = above2;
         if (MODE == 2 && reached) break;
@@ -531,7 +609,12 @@ fill_thread_kernel (FillParams P) {
       if (MODE == 2 && reached) break;
     }
     if (vmax >= 127) reached = true;
-    fill_finish<W, MODE>(P, pi, mp, v.g, reached, final_score);
+    if (v.endmode == 2 && !eb.found) {
+      /* the last-row search starts at (rlength, 0) */
+      eb.score = LO;
+      eb.r = (VARIANT == GDP_UPPER) ? v.g.X : v.g.Y;
+    }
+    fill_finish<W, MODE>(P, pi, mp, v.g, reached, final_score, v.endmode != 0 ? &eb : nullptr);
   }
 }
 

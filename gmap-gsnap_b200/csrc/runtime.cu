@@ -683,6 +683,13 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   if (p.flags & GDP_FLAG_TRACEBACK) {
     if (p.tb_r < 0 || p.tb_c < 0 || p.tb_r > p.rlength || p.tb_c > p.glength) return GDP_ERR_BAND;
   }
+  if (p.flags & (GDP_FLAG_ENDPOINT | GDP_FLAG_ENDPOINT_QEND)) {
+    /* the end-gap searches scan an upper and a lower fill at the pair's
+       own precision */
+    if (p.variant == GDP_FULL || (p.flags & GDP_FLAG_RERUN16) ||
+        ((p.flags & GDP_FLAG_ENDPOINT) && (p.flags & GDP_FLAG_ENDPOINT_QEND)))
+      return GDP_ERR_PARAM;
+  }
   if (p.flags & GDP_FLAG_GWINDOW) {
     /* the window's positions inside [chroffset, chrhigh) must be resident */
     const int64_t g0 = (p.flags & GDP_FLAG_REVP) ? (int64_t) p.genomeoffset - (p.glength - 1) : p.genomeoffset;
@@ -807,7 +814,8 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
         gdp_geom_of(&p, 16, &g16);
         const int sweep = 15 + g16.band_hi + (p.variant == GDP_FULL ? p.lband : 0);
         int k = kind_id(0, p.variant, late, rerun ? 1 : 0);
-        if (!rerun && g16.X >= ctx->warp_min_x) {
+        const bool endpoint = (p.flags & (GDP_FLAG_ENDPOINT | GDP_FLAG_ENDPOINT_QEND)) != 0;
+        if (!rerun && !endpoint && g16.X >= ctx->warp_min_x) {   /* endpoint searches: one thread per pair */
           if (sweep <= ctx->warp_max_sweep) {
             /* the smallest lane group whose blocks do not overlap in time */
             int kg = 2;
@@ -1003,6 +1011,7 @@ init_results_kernel (gdp_result_t *res, const int32_t *status, const gdp_pair_t 
     r.tb_score = r.nmatches = r.nmismatches = r.nopens = r.nindels = 0;
     r.nrecs = 0;
     r.rec_offset = 0;
+    r.end_score = r.end_r = r.end_c = r.end_found = 0;
     res[i] = r;
   }
 }
@@ -2001,5 +2010,40 @@ gdpi_set_tables (gdp_ctx *ctx, const gdp_tables_t *t) {
   update_reach(ctx);
   CK(ctx, cudaMemcpyAsync(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return GDP_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* End-gap endpoint search: merging the two halves                     */
+/* ------------------------------------------------------------------ */
+
+extern "C" int
+gdp_endpoint_combine (const gdp_result_t *upper, const gdp_result_t *lower, int jump_late, int qend, int precision,
+                      int rlength, int *finalscore, int *bestr, int *bestc) {
+  if (upper == nullptr || lower == nullptr || finalscore == nullptr || bestr == nullptr || bestc == nullptr)
+    return GDP_ERR_PARAM;
+  /* the reference scans each row's lower cells (c < r) before its upper
+     cells (c >= r): row-then-column order over both halves */
+  const gdp_result_t *best = nullptr;
+  for (const gdp_result_t *h : {lower, upper}) {
+    if (!h->end_found) continue;
+    if (best == nullptr || h->end_score > best->end_score) { best = h; continue; }
+    if (h->end_score < best->end_score) continue;
+    const bool later = (h->end_r > best->end_r) || (h->end_r == best->end_r && h->end_c > best->end_c);
+    if (jump_late ? later : !later) best = h;
+  }
+  if (best != nullptr) {
+    *finalscore = best->end_score;
+    *bestr = best->end_r;
+    *bestc = best->end_c;
+  } else if (qend) {
+    *finalscore = precision == 8 ? -128 : -32768;   /* NEG_INFINITY_8 / _16 */
+    *bestr = rlength;
+    *bestc = 0;
+  } else {
+    *finalscore = 0;
+    *bestr = 0;
+    *bestc = 0;
+  }
   return GDP_OK;
 }

@@ -15,6 +15,7 @@ LIB_PATH = os.environ.get("GDP_LIB") or os.path.join(HERE, "lib", "libgdp.so")
 
 FULL, UPPER, LOWER = 0, 1, 2
 FLAG_JUMP_LATE, FLAG_REVP, FLAG_TRACEBACK, FLAG_RERUN16, FLAG_GWINDOW = 1, 2, 4, 8, 16
+FLAG_ENDPOINT, FLAG_ENDPOINT_QEND = 32, 64
 HIGHQ, MEDQ, LOWQ, ENDQ = 0, 1, 2, 3
 STATUS = {0: "GDP_OK", 1: "GDP_ERR_LEN", 2: "GDP_ERR_BAND", 3: "GDP_ERR_PARAM",
           4: "GDP_ERR_BUDGET", 5: "GDP_ERR_TIMEOUT", 6: "GDP_ERR_CUDA",
@@ -34,21 +35,22 @@ PAIR_DTYPE = np.dtype([
 ])
 assert PAIR_DTYPE.itemsize == 88
 
-# struct gdp_rec, 16 bytes
+# struct gdp_rec, 12 bytes
 REC_DTYPE = np.dtype([
     ("querypos", "<i4"), ("genomepos", "<i4"),
     ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1"),
 ])
 assert REC_DTYPE.itemsize == 12
 
-# struct gdp_result, 48 bytes
+# struct gdp_result, 64 bytes
 RESULT_DTYPE = np.dtype([
     ("status", "<i4"), ("score", "<i4"), ("precision", "<i4"), ("rerun", "<i4"),
     ("tb_score", "<i4"), ("nmatches", "<i4"), ("nmismatches", "<i4"),
     ("nopens", "<i4"), ("nindels", "<i4"), ("nrecs", "<i4"),
     ("rec_offset", "<i8"),
+    ("end_score", "<i4"), ("end_r", "<i4"), ("end_c", "<i4"), ("end_found", "<i4"),
 ])
-assert RESULT_DTYPE.itemsize == 48
+assert RESULT_DTYPE.itemsize == 64
 
 WL_FIXED, WL_SHORT, WL_CDNA, WL_MIX, WL_LONG = 1, 2, 3, 4, 5
 
@@ -115,7 +117,22 @@ def load(path=LIB_PATH):
     lib.gdp_server_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
                                      ctypes.POINTER(i64), dp]
     lib.gdp_server_destroy.argtypes = [vp]
+    ip = ctypes.POINTER(i32)
+    lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
     return lib
+
+
+def endpoint_combine(lib, upper, lower, jump_late, qend, precision, rlength):
+    """The reference's (finalscore, bestr, bestc) of one end gap from the
+    results of its upper and lower halves (gdp_endpoint_combine)."""
+    u = np.ascontiguousarray(upper, dtype=RESULT_DTYPE).reshape(1)
+    lo = np.ascontiguousarray(lower, dtype=RESULT_DTYPE).reshape(1)
+    fs, br, bc = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    rc = lib.gdp_endpoint_combine(_ptr(u), _ptr(lo), int(jump_late), int(qend), int(precision), int(rlength),
+                                  ctypes.byref(fs), ctypes.byref(br), ctypes.byref(bc))
+    if rc != 0:
+        raise RuntimeError(f"gdp_endpoint_combine: {STATUS.get(rc, rc)}")
+    return fs.value, br.value, bc.value
 
 
 def tables(lib, mode=0):

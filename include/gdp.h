@@ -49,7 +49,9 @@ enum {
   GDP_FLAG_REVP = 2,        /* revp: sequences are read backwards from their last character */
   GDP_FLAG_TRACEBACK = 4,   /* run Dynprog_traceback_* from (tb_r, tb_c) */
   GDP_FLAG_RERUN16 = 8,     /* precision 8: rerun in 16-bit when the 8-bit fill overflows */
-  GDP_FLAG_GWINDOW = 16     /* the genome window comes from the resident genome (see below) */
+  GDP_FLAG_GWINDOW = 16,    /* the genome window comes from the resident genome (see below) */
+  GDP_FLAG_ENDPOINT = 32,   /* end-gap endpoint search over the band (see below) */
+  GDP_FLAG_ENDPOINT_QEND = 64  /* the same over the last query row only */
 };
 
 /* Mismatch types (src/dynprog.h:53) */
@@ -83,6 +85,23 @@ enum {
  * on the plus strand, the complement of chrhigh - gp on the minus strand,
  * '*' outside [chroffset, chrhigh) (get_genomic_nt, src/pairpool.c:1015).
  * A window that reaches past the resident genome gets GDP_ERR_NOGENOME.
+ *
+ * GDP_FLAG_ENDPOINT / GDP_FLAG_ENDPOINT_QEND (upper and lower fills, no
+ * GDP_FLAG_RERUN16): the fill also runs its half of the reference's
+ * end-gap endpoint search over the scores it computes.  Dynprog_end5_gap
+ * and Dynprog_end3_gap fill the upper and the lower matrix of one gap and
+ * scan both (src/dynprog_end.c:1415-1534): find_best_endpoint_{8,16}
+ * (:143-294) takes the best cell of the band, rows 1..rlength, with a score
+ * above 0 (jump early: the first such best cell in row-then-column order;
+ * jump late: the last, from score 0 up); find_best_endpoint_to_queryend_
+ * indels_{8,16} (:358-508) does the same on row rlength alone, from the
+ * most negative score.  The upper fill scans its cells with c >= r, the
+ * lower fill its cells with c < r, so one gap is two pairs (an upper and a
+ * lower pair with the same sequences and flags); the result's end_score,
+ * end_r and end_c hold each half's best, and gdp_endpoint_combine merges
+ * the two halves into the reference's finalscore, bestr and bestc.  A
+ * half whose final cell (rlength, glength) lies outside its triangle keeps
+ * GDP_OK (its score is then NEG_INFINITY_8/16: the cell is not computed).
  */
 typedef struct gdp_pair {
   int64_t rseq;          /* rsequence, rlength bytes */
@@ -133,7 +152,21 @@ typedef struct gdp_result {
   int32_t tb_score, nmatches, nmismatches, nopens, nindels;  /* traceback totals */
   int32_t nrecs;         /* number of Pair records */
   int64_t rec_offset;    /* index of the first record in the record buffer */
+  int32_t end_score, end_r, end_c;  /* GDP_FLAG_ENDPOINT*: this half's best cell (else 0) */
+  int32_t end_found;     /* 1 if a cell of this half passed the search's threshold */
 } gdp_result_t;
+
+/*
+ * Merges the endpoint-search halves of one end gap (the upper and the lower
+ * pair's results, GDP_FLAG_ENDPOINT or GDP_FLAG_ENDPOINT_QEND, the same
+ * jump_late_p) into the reference's finalscore, bestr and bestc
+ * (find_best_endpoint_{8,16}, src/dynprog_end.c:143-294, and
+ * find_best_endpoint_to_queryend_indels_{8,16}, :358-508).  `qend` selects
+ * the last-row search, `precision` its starting score (NEG_INFINITY_8 or
+ * _16) and `rlength` its default row.  Returns GDP_OK.
+ */
+int gdp_endpoint_combine(const gdp_result_t *upper, const gdp_result_t *lower, int jump_late, int qend,
+                         int precision, int rlength, int *finalscore, int *bestr, int *bestc);
 
 typedef struct gdp_ctx gdp_ctx;
 
