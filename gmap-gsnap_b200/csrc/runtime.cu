@@ -142,7 +142,12 @@ class WorkPool {
   void run (int nt, F &&f) {
     if (nt <= 1) { f(0); return; }
     std::unique_lock<std::mutex> g(m_);
-    while ((int) th_.size() < nt - 1) th_.emplace_back([this] { work(); });
+    try {
+      while ((int) th_.size() < nt - 1) th_.emplace_back([this] { work(); });
+    } catch (...) {
+      /* fewer threads than asked: the caller and the threads there are take
+         every index all the same */
+    }
     fn_ = [&f] (int t) { f(t); };
     next_ = 1;
     nt_ = nt;
@@ -151,6 +156,13 @@ class WorkPool {
     cv_.notify_all();
     f(0);
     g.lock();
+    while (next_ < nt_) {   /* indices no worker has taken yet */
+      const int t = next_++;
+      g.unlock();
+      f(t);
+      g.lock();
+      --left_;
+    }
     done_.wait(g, [this] { return left_ == 0; });
     nt_ = next_ = 0;
     fn_ = nullptr;
@@ -1722,9 +1734,15 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
       hand_out(k);
     }
   };
-  /* a batch of one wave hands out on this thread */
+  /* a batch of one wave hands out on this thread (and so does any batch
+     when no thread can be started) */
   std::thread copy_out;
-  if (n > wave_cap) copy_out = std::thread(copy_out_loop);
+  if (n > wave_cap) {
+    try {
+      copy_out = std::thread(copy_out_loop);
+    } catch (...) {
+    }
+  }
   int cur = 0, wave_index = 0;
   for (int64_t first = 0; first < n;) {
     if (copy_out.joinable()) {
