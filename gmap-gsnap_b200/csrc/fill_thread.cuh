@@ -522,6 +522,10 @@ column_steady (const PairView &v, int xlo, int y) {
 #ifndef GDP_FILL_MINB
 #define GDP_FILL_MINB 4
 #endif
+/* resident blocks of 128 threads per SM the 8-bit fills are built for */
+#ifndef GDP_FILL_MINB8
+#define GDP_FILL_MINB8 3
+#endif
 
 /* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records whether an
    in-band score reaches 127), 2 = 8-bit pass of a rerun pair (skipped when
@@ -529,7 +533,7 @@ column_steady (const PairView &v, int xlo, int y) {
    One thread per pair; the next column's characters and carry are fetched
    one column ahead. */
 template <int W, int VARIANT, bool LATE, int MODE>
-__global__ void __launch_bounds__(128, (W == 16) ? GDP_FILL_MINB : 1)
+__global__ void __launch_bounds__(128, (W == 16) ? GDP_FILL_MINB : GDP_FILL_MINB8)
 fill_thread_kernel (FillParams P) {
   constexpr int LO = (W == 32) ? -128 : -32768;
   constexpr int WORDS = W / 8;
