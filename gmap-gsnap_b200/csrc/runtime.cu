@@ -293,6 +293,7 @@ struct gdp_ctx {
   uint64_t genome_len = 0;
   int64_t budget = 0;
   int64_t wave = 262144;
+  int64_t first_wave = 0;   /* pairs of the first wave (0: wave / 16, at least 16,384) */
   int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
   int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
   bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
@@ -1414,6 +1415,7 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "check_groups")) ctx->check_groups = value != 0;
   else if (!strcmp(name, "check_min_x") && value >= 1) ctx->check_min_x = (int) std::min<int64_t>(value, 1 << 30);
   else if (!strcmp(name, "wave_pairs") && value >= 1) ctx->wave = value;
+  else if (!strcmp(name, "first_wave_pairs") && value >= 0) ctx->first_wave = value;
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1429,6 +1431,7 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "check_groups")) *value = ctx->check_groups ? 1 : 0;
   else if (!strcmp(name, "check_min_x")) *value = ctx->check_min_x;
   else if (!strcmp(name, "wave_pairs")) *value = ctx->wave;
+  else if (!strcmp(name, "first_wave_pairs")) *value = ctx->first_wave;
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1647,7 +1650,7 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   /* Short first waves get the pipeline going: the first holds 1/8 of a
      wave and each next one twice the one before, up to a full wave, so the
      copies out start early and never wait long for the next wave. */
-  int64_t wave_cap = std::min(wave, std::max<int64_t>(16384, wave / 8));
+  int64_t wave_cap = std::min(wave, ctx->first_wave > 0 ? ctx->first_wave : std::max<int64_t>(16384, wave / 16));
   /* A wave also ends before its direction words would pass the context's
      budget (an upper bound per pair: every block sweeps at most
      W + lband + uband columns).  One pass finds the count and the end of the

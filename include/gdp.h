@@ -246,6 +246,9 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *   "check_min_x"    ... pairs with at least this many lanes, whose 8-bit
  *                    pass goes to lane groups all the same
  *   "wave_pairs"     pairs per wave of gdp_align_batch
+ *   "first_wave_pairs" pairs of its first wave (0: wave_pairs / 16, at least
+ *                    16,384); each next wave holds twice the one before,
+ *                    up to wave_pairs
  * gdp_autotune times plan executions of a sample batch (device-resident
  * copies, the caller's pairs and arena) under candidate values of the first
  * six, one parameter at a time, and keeps the fastest; *best_ms gets the
