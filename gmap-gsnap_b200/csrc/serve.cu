@@ -278,6 +278,11 @@ gdp_server_create (int device, int mode, int nworkers, int64_t dir_budget_bytes,
   for (int w = 0; w < nworkers; w++) {
     gdp_ctx *c = nullptr;
     int rc = gdp_ctx_create(&c, device, mode, 0);
+    /* a worker's batch is one wave: the workers already overlap batches on
+       the device, and a one-wave call hands its records out on its own
+       thread */
+    if (rc == GDP_OK) rc = gdp_ctx_set_param(c, "wave_pairs", std::max<int64_t>(s->max_batch_pairs, 16384));
+    if (rc == GDP_OK) rc = gdp_ctx_set_param(c, "first_wave_pairs", std::max<int64_t>(s->max_batch_pairs, 16384));
     if (rc == GDP_OK && genome_blocks) rc = gdp_set_genome(c, genome_blocks, alt_blocks, genome_length);
     if (rc != GDP_OK) {
       if (c) gdp_ctx_destroy(c);
