@@ -102,12 +102,19 @@ struct WarpTb {
   }
   /* The diagonal steps (r - j, c - j), j < k: one match / ambiguous /
      mismatch Pair each, none where the genome character is '*'. */
-  __device__ void diagpairs (int r, int c, int k) {
+  /* The characters of lane j's cell (r - j, c - j) of a diagonal run, read
+     before the run's direction words arrive (the two loads overlap). */
+  __device__ void diagchars (int r, int c, bool valid, char &c1, char &c1uc, char &c2, char &c2a) const {
+    int qc = r - 1 - lane, gc = c - 1 - lane;
+    if (revp) { qc = -qc; gc = -gc; }
+    c1 = ' '; c1uc = ' '; c2 = '*'; c2a = '*';
+    if (valid) { c1 = rseq[qc]; c1uc = ruc[qc]; c2 = gseq[gc]; c2a = galt[gc]; }
+  }
+  __device__ void diagpairs (int r, int c, int k, char c1, char c1uc, char c2, char c2a) {
     const bool on = lane < k;
     int qc = r - 1 - lane, gc = c - 1 - lane;
     if (revp) { qc = -qc; gc = -gc; }
-    char c1 = ' ', c1uc = ' ', c2 = '*', c2a = '*';
-    if (on) { c1 = rseq[qc]; c1uc = ruc[qc]; c2 = gseq[gc]; c2a = galt[gc]; }
+    if (!on) { c1 = ' '; c1uc = ' '; c2 = '*'; c2a = '*'; }
     const bool pair = on && c2 != '*';
     char comp = ' ';
     bool match = false;
@@ -137,13 +144,15 @@ tb_walk_warp (const gdp_pair_t &p, DirCursor &dc, WarpTb &T) {
   while (r > 0 && c > 0 && !T.err) {
     /* the diagonal run: lane j looks at (r - j, c - j) */
     const bool valid = (r - lane > 0) && (c - lane > 0);
+    char c1, c1uc, c2, c2a;
+    T.diagchars(r, c, valid, c1, c1uc, c2, c2a);
     const int code = valid ? CELL(c - lane, r - lane) : -1;
     const bool bad = valid && (code < 0 || ABOVE(c - lane, r - lane));
     const bool gap = valid && !bad && (code & 3);
     const unsigned badm = __ballot_sync(GDP_FULL_MASK, bad);
     const unsigned stop = __ballot_sync(GDP_FULL_MASK, !valid || bad || gap);
     const int k = stop ? __ffs(stop) - 1 : 32;
-    if (k > 0) T.diagpairs(r, c, k);
+    if (k > 0) T.diagpairs(r, c, k, c1, c1uc, c2, c2a);
     r -= k; c -= k;
     if (T.err) break;
     if (k == 32 || r <= 0 || c <= 0) continue;
@@ -221,7 +230,7 @@ tb_walk_warp (const gdp_pair_t &p, DirCursor &dc, WarpTb &T) {
 #undef ABOVE
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 6)
 traceback_warp_kernel (TbParams P) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
