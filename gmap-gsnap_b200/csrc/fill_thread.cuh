@@ -261,11 +261,22 @@ block_start (Block<W> &B, const PairView &v, const gdp_tables_t *tab, int xlo) {
  *   above  (H[y][xlo-1], FF[y]) of the block above.
  * Writes the column's direction words to dcol (and scores to hd when not
  * NULL).  Returns (H of the last lane, F carry) for the block below.
+ *
+ * LS > 0 (full band only): lanes 0 .. LS-1 lie above the band's top lane
+ * and are skipped.  Such lanes have left the band for good: their H feeds
+ * only the diagonal of the lane below at the next column, which is above
+ * the band too, and their E only their own row, so no in-band cell reads
+ * them again.  Their scores keep the values of the last column computed
+ * and their direction bits are 0; a traceback reaching such a cell stops
+ * with GDP_ERR_BAND by position (the reference reads stale scratch there).
+ * The caller takes this body only when the column's top lane is at least
+ * LS, the column is not the last one, and no score dump is asked for.
  */
-template <int W, int VARIANT, bool LATE, int MODE>
+template <int W, int VARIANT, bool LATE, int MODE, int LS = 0>
 __device__ __forceinline__ int2
 block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int ka, int kb,
               uint32_t *dcol, int16_t *hd, bool &reached, int &final_score) {
+  static_assert(LS == 0 || VARIANT == GDP_FULL, "lanes above the band exist in full-band fills");
   constexpr int LO = (W == 32) ? -128 : -32768;
   constexpr int HI = (W == 32) ? 127 : 32767;
   constexpr int WORDS = W / 8;
@@ -297,8 +308,9 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
 #pragma unroll
   for (int j = 0; j < WORDS; j++) w[j] = 0;
 
+  if (LS > 0) diag = B.H[LS - 1];   /* the skipped lane above: its last computed score */
 #pragma unroll
-  for (int i = 0; i < W; i++) {
+  for (int i = LS; i < W; i++) {
     const uint32_t bit = 1u << i;
     const int Hold = B.H[i];
     int Eold = B.E[i];
@@ -336,7 +348,7 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
     if (xlo == 0 || y >= xlo + v.uband) { Fp = GDP_NEGINT; Hp = GDP_NEGINT; }
     else { Fp = above.y; Hp = above.x; }
 #pragma unroll
-    for (int i = 0; i < W; i++) {
+    for (int i = LS; i < W; i++) {
       const uint32_t bit = 1u << i;
       if (topmask & bit) {
         Fp = GDP_NEGINT + v.oe;
@@ -361,7 +373,7 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
     if (dh >= dl) {
       const uint32_t dom = lane_range(max(dl, 0), dh);
 #pragma unroll
-      for (int i = 0; i < W; i++)
+      for (int i = LS; i < W; i++)
         if ((dom & (1u << i)) && B.H[i] >= 127) reached = true;
     }
   }
@@ -536,6 +548,8 @@ template <int W, int VARIANT, bool LATE, int MODE>
 __global__ void __launch_bounds__(128, (W == 16) ? GDP_FILL_MINB : GDP_FILL_MINB8)
 fill_thread_kernel (FillParams P) {
   constexpr int LO = (W == 32) ? -128 : -32768;
+  /* lanes skipped in full-band columns whose top half left the band */
+  constexpr int HALF = (VARIANT == GDP_FULL && W == 16) ? W / 2 : 0;
   constexpr int WORDS = W / 8;
   __shared__ int8_t s_nt2int[128];
   for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
@@ -597,6 +611,10 @@ fill_thread_kernel (FillParams P) {
             out = block_column_steady<W, VARIANT, LATE, MODE>(B, v, diag, above, ka, kb, dcol, vmax,
                                                               y >= v.reach_from && xlo + W - 1 >= v.reach_from);
             if (MODE == 2 && vmax >= 127) reached = true;
+          } else if (HALF > 0 && hd == nullptr && y != v.g.Y && y - xlo - v.uband >= HALF) {
+            /* the top half of the block has left the band */
+            out = block_column<W, VARIANT, LATE, MODE, HALF>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
+                                                             final_score);
           } else
             out = block_column<W, VARIANT, LATE, MODE>(B, v, y, diag, above, ka, kb, dcol, hd, reached,
                                                        final_score);
