@@ -160,3 +160,37 @@ def domain_mask(variant, rlength, glength, lband, uband):
         lo, hi = c, c + lband
     m = (r >= np.maximum(lo, 1)) & (r <= np.minimum(hi, rlength)) & (c >= 1)
     return m
+
+
+def find_best_endpoint(Hu, Hl, rlength, glength, lband, uband, jump_late, qend, precision, half=None):
+    """The reference's end-gap endpoint scans over dense (c, r) score arrays
+    of an upper fill (Hu) and a lower fill (Hl): find_best_endpoint_{8,16}
+    (src/dynprog_end.c:143-294; rows 1..rlength, start score 0, bestr =
+    bestc = 0) and, with `qend`, find_best_endpoint_to_queryend_indels_{8,16}
+    (:358-508; row rlength only, start NEG_INFINITY_8/16, bestr = rlength,
+    bestc = 0).  Each row scans the lower cells c < r, then the upper cells
+    c >= r, keeping a cell with a score > (jump early) or >= (jump late) the
+    best so far.  `half` ("upper" / "lower") restricts the scan to one
+    matrix's cells.  Columns stop at glength: the reference's lower loop
+    runs to c = r - 1 even past glength, outside the lower matrix, which
+    only queries longer than glength + 1 reach.  Returns (finalscore,
+    bestr, bestc, found)."""
+    if qend:
+        best, br, bc, rows = (-128 if precision == 8 else -32768), rlength, 0, [rlength]
+    else:
+        best, br, bc, rows = 0, 0, 0, range(1, rlength + 1)
+    found = False
+    for r in rows:
+        clo, chigh = max(1, r - lband), min(glength, r + uband)
+        for c in range(clo, chigh + 1):
+            if c < r:
+                if half == "upper":
+                    continue
+                v = int(Hl[c, r])
+            else:
+                if half == "lower":
+                    continue
+                v = int(Hu[c, r])
+            if (v >= best) if jump_late else (v > best):
+                best, br, bc, found = v, r, c, True
+    return best, br, bc, found

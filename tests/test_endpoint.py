@@ -7,9 +7,9 @@ one gap and scan both for the endpoint of the alignment
 the band, find_best_endpoint_to_queryend_indels_{8,16} (:358-508) over the
 last query row.  Here each fill runs its half of the scan over the scores
 it computes, and gdp_endpoint_combine merges the halves.  The expected
-answer is that scan restated over the reference's own score matrices
-(oracle/_ref, or the pinned restatement): finalscore, bestr and bestc must
-be identical.
+answer is that scan (oracle.find_best_endpoint) over the reference's own
+score matrices (oracle/_ref, or the pinned restatement): finalscore, bestr
+and bestc must be identical.
 
 Cases keep rlength <= glength + 1: for longer queries the reference's
 lower-half scan (c < r) reads columns beyond glength, outside the lower
@@ -23,29 +23,6 @@ import gdp
 import oracle as orc
 
 pytestmark = pytest.mark.gpu
-
-
-def _scan(Hu, Hl, rl, gl, lband, uband, late, qend, prec):
-    """find_best_endpoint_* / ..._to_queryend_indels_* (src/dynprog_end.c)
-    over dense (c, r) score arrays of the upper and the lower fill."""
-    if qend:
-        best, br, bc, rows = (-128 if prec == 8 else -32768), rl, 0, [rl]
-    else:
-        best, br, bc, rows = 0, 0, 0, range(1, rl + 1)
-    for r in rows:
-        clo, chigh = max(1, r - lband), min(gl, r + uband)
-        c = clo
-        while c < r:
-            v = int(Hl[c, r])
-            if (v >= best) if late else (v > best):
-                best, br, bc = v, r, c
-            c += 1
-        while c <= chigh:
-            v = int(Hu[c, r])
-            if (v >= best) if late else (v > best):
-                best, br, bc = v, r, c
-            c += 1
-    return best, br, bc
 
 
 def _gap_cases(seed, n):
@@ -100,7 +77,7 @@ def test_endpoint_search_matches_reference_scan(env, gdplib, seed):
         ou, ol = ref.align(pairs, i, arena), ref.align(pairs, i + 1, arena)
         Hu = ou["H"].reshape(gl + 1, rl + 1)
         Hl = ol["H"].reshape(gl + 1, rl + 1)
-        want = _scan(Hu, Hl, rl, gl, int(lo["lband"]), int(up["uband"]), late, qend, prec)
+        want = orc.find_best_endpoint(Hu, Hl, rl, gl, int(lo["lband"]), int(up["uband"]), late, qend, prec)[:3]
         got = gdp.endpoint_combine(gdplib, res[i], res[i + 1], late, qend, prec, rl)
         if got != want:
             fails.append(f"gap {i // 2} r {rl} g {gl} late {late} qend {qend} prec {prec}: got {got} want {want}")
