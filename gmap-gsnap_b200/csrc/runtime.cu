@@ -717,12 +717,13 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   return GDP_OK;
 }
 
-/* Sort key of a pair's fill inside its kind (14 bits): wider bands first,
-   and inside one band width (lband + uband) more blocks first.  Threads
-   that share the band width and run the same block in lock step are in the
-   same column phase at the same step: the phase of the j-th swept column of
-   a block depends on j and lband + uband only (while the sweep is not cut
-   at column 0 or glength). */
+/* Sort key of a pair's fill inside its kind (22 bits): wider bands first,
+   inside one band width (lband + uband) by lband, and then more blocks
+   first.  Threads that share the band width and run the same block in lock
+   step are in the same column phase at the same step: the phase of the j-th
+   swept column of a block depends on j and lband + uband only, while the
+   sweep is not cut at column 0.  The sweeps of the first blocks are cut at
+   column 0 by lband, so pairs of one lband stay in phase there too. */
 static inline uint32_t
 work_key (const gdp_pair_t &p, int W) {
   gdp_geom_t g;
@@ -730,10 +731,11 @@ work_key (const gdp_pair_t &p, int W) {
   const int nb = std::min(63, g.X / W + 1);
   const int lb = (p.variant == GDP_FULL) ? p.lband : 0;
   const int band = std::min(255, lb + g.band_hi);
-  return (uint32_t) (255 - band) << 6 | (uint32_t) (63 - nb);
+  return (uint32_t) (255 - band) << 14 | (uint32_t) std::min(255, lb) << 6 | (uint32_t) (63 - nb);
 }
-#define KEY_KIND_SHIFT 14   /* sort key = kind << 14 | work key */
-#define KEY_GROUP_SHIFT 6   /* entries with equal key >> 6 share kind and band width */
+#define KEY_KIND_SHIFT 22   /* sort key = kind << 22 | work key */
+#define KEY_GROUP_SHIFT 6   /* entries with equal key >> 6 share kind, band width and lband */
+#define KEY_BITS 29         /* kinds below 128 */
 
 /* Kinds whose warps are padded to pairs of one band width: the 16-bit
    one-thread-per-pair fills, which run phase-specialised columns. */
@@ -750,14 +752,16 @@ parallel_chunks (WorkPool &pool, int64_t n, int nt, F f) {
   pool.run(nt, [&](int t) { f(n * t / nt, n * (t + 1) / nt, t); });
 }
 
-/* Stable LSD radix sort of (key, value)[0..n) by the low 22 bits of key,
+/* Stable LSD radix sort of (key, value)[0..n) by the low KEY_BITS bits of key,
    11 bits per pass, `nt` pool threads (per-thread histograms, then each
    thread scatters its own chunk in order).  k2/v2 are scratch of n. */
 static void
 radix_sort (WorkPool &pool, uint32_t *key, int32_t *val, uint32_t *k2, int32_t *v2, int64_t n, int nt) {
   constexpr int B = 2048;
+  uint32_t *const key0 = key;
+  int32_t *const val0 = val;
   std::vector<int64_t> hist((size_t) nt * B);
-  for (int shift = 0; shift < 22; shift += 11) {
+  for (int shift = 0; shift < KEY_BITS; shift += 11) {
     std::fill(hist.begin(), hist.end(), 0);
     parallel_chunks(pool, n, nt, [&](int64_t lo, int64_t hi, int t) {
       int64_t *h = hist.data() + (size_t) t * B;
@@ -781,8 +785,13 @@ radix_sort (WorkPool &pool, uint32_t *key, int32_t *val, uint32_t *k2, int32_t *
     std::swap(key, k2);
     std::swap(val, v2);
   }
-  /* an even number of passes leaves the sorted data in the caller's arrays */
-  static_assert((22 + 10) / 11 % 2 == 0, "radix passes are even");
+  /* an odd number of passes leaves the sorted data in the scratch arrays */
+  if (key != key0) {
+    parallel_chunks(pool, n, nt, [&](int64_t lo, int64_t hi, int) {
+      memcpy(key0 + lo, key + lo, (size_t) (hi - lo) * sizeof(uint32_t));
+      memcpy(val0 + lo, val + lo, (size_t) (hi - lo) * sizeof(int32_t));
+    });
+  }
 }
 
 /* Fills ph for pairs[0..n) (pinned host buffers).  arena_bytes < 0 skips the
@@ -908,7 +917,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
       }
     }
   });
-  static_assert(NKINDS < (1 << (22 - KEY_KIND_SHIFT)), "kind ids fit in the 22-bit sort key");
+  static_assert(NKINDS < (1 << (KEY_BITS - KEY_KIND_SHIFT)), "kind ids fit in the sort key");
   radix_sort(ctx->pool, keys, vals, grow(ph.keys2, entries), grow(ph.vals2, entries), entries, nt);
   /* padded kinds: every band-width group starts a warp (-1 = no pair) */
   int64_t groups = 0;
