@@ -717,9 +717,10 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   return GDP_OK;
 }
 
-/* Sort key of a pair's fill inside its kind (22 bits): wider bands first,
-   inside one band width (lband + uband) by lband, and then more blocks
-   first.  Threads that share the band width and run the same block in lock
+/* Sort key of a pair's fill inside its kind (25 bits): wider bands first,
+   inside one band width (lband + uband) by lband, and then longer pairs
+   first (more lanes, so more blocks, and with them about as many swept
+   columns).  Threads that share the band width and run the same block in lock
    step are in the same column phase at the same step: the phase of the j-th
    swept column of a block depends on j and lband + uband only, while the
    sweep is not cut at column 0.  The sweeps of the first blocks are cut at
@@ -728,14 +729,14 @@ static inline uint32_t
 work_key (const gdp_pair_t &p, int W) {
   gdp_geom_t g;
   gdp_geom_of(&p, W, &g);
-  const int nb = std::min(63, g.X / W + 1);
+  const int lanes = std::min(511, g.X);
   const int lb = (p.variant == GDP_FULL) ? p.lband : 0;
   const int band = std::min(255, lb + g.band_hi);
-  return (uint32_t) (255 - band) << 14 | (uint32_t) std::min(255, lb) << 6 | (uint32_t) (63 - nb);
+  return (uint32_t) (255 - band) << 17 | (uint32_t) std::min(255, lb) << 9 | (uint32_t) (511 - lanes);
 }
-#define KEY_KIND_SHIFT 22   /* sort key = kind << 22 | work key */
-#define KEY_GROUP_SHIFT 6   /* entries with equal key >> 6 share kind, band width and lband */
-#define KEY_BITS 29         /* kinds below 128 */
+#define KEY_KIND_SHIFT 25   /* sort key = kind << 25 | work key */
+#define KEY_GROUP_SHIFT 9   /* entries with equal key >> 9 share kind, band width and lband */
+#define KEY_BITS 32         /* kinds below 128 */
 
 /* Kinds whose warps are padded to pairs of one band width: the 16-bit
    one-thread-per-pair fills, which run phase-specialised columns. */
