@@ -866,21 +866,11 @@ apply_rerun8_kernel (const int32_t *list, const int32_t *count, const gdp_meta_t
   }
 }
 
-/* Keeps the rerun pairs whose 16-bit in-band maximum stays below 127: only
-   those need the 8-bit pass (the others provably overflow in 8 bits). */
-static __global__ void
-compact_rerun_kernel (const int32_t *list, const int32_t *count, const gdp_meta_t *meta,
-                      int32_t *out, int32_t *out_count) {
-  const int n = *count;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int pi = list[i];
-    const bool need = pi >= 0 && meta[pi].maxh16 < 127;
-    const unsigned mask = __ballot_sync(__activemask(), need);
-    const int lane = threadIdx.x & 31;
-    int base = 0;
-    const int leader = __ffs(mask) - 1;
-    if (mask && lane == leader) base = atomicAdd(out_count, __popc(mask));
-    base = __shfl_sync(__activemask(), base, leader < 0 ? 0 : leader);
-    if (need) out[base + __popc(mask & ((1u << lane) - 1))] = pi;
+/* The rerun pairs whose 16-bit in-band maximum stays below 127: only those
+   need the 8-bit pass (the others provably overflow in 8 bits). */
+struct NeedsPass8 {
+  const gdp_meta_t *meta;
+  __device__ __forceinline__ bool operator() (const int32_t &pi) const {
+    return pi >= 0 && meta[pi].maxh16 < 127;
   }
-}
+};

@@ -28,6 +28,7 @@
  */
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
@@ -218,10 +219,11 @@ struct PlanDev {
   DevBuf nrec_scan;    /* int64 exclusive scan of records per pair */
   DevBuf total;        /* int64 record total of the plan */
   DevBuf cub_tmp;
+  DevBuf sel_tmp;      /* temporary storage of the 8-bit pass selection */
   void release () {
     lists.release(); work.release(); counts.release(); work_counts.release(); status.release();
     meta0.release(); meta.release(); rec_off.release(); dirs.release(); hdump.release();
-    slots.release(); nrec_scan.release(); total.release(); cub_tmp.release();
+    slots.release(); nrec_scan.release(); total.release(); cub_tmp.release(); sel_tmp.release();
   }
 };
 
@@ -330,7 +332,7 @@ kernel_name (int id) {
   if (id == PROF_TB) return "traceback";
   if (id == PROF_INIT) return "init_results_kernel";
   if (id == PROF_PEAK) return "int_peak_kernel";
-  if (id == PROF_RERUN) return "compact_rerun_kernel";
+  if (id == PROF_RERUN) return "rerun_select";
   if (id == PROF_RECS) return "compact_records_kernel";
   if (id == PROF_WINDOW) return "window_kernel";
   if (id >= FIRST_EARLY8) {
@@ -1274,16 +1276,19 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.count = pd.counts.as<int32_t>() + k;
       if (second) {
         /* only the pairs whose 16-bit maximum stayed below 127 run the 8-bit
-           pass (init_results_kernel cleared the counter) */
-        const int cg = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
+           pass; the selection keeps the planner's order, so a warp's pairs
+           share band width and lband as in the other passes */
+        const NeedsPass8 need{pd.meta.as<gdp_meta_t>()};
+        size_t tmp = 0;
+        CK(ctx, cub::DeviceSelect::If(nullptr, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
+                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, s));
+        CK(ctx, pd.sel_tmp.ensure(std::max<size_t>(tmp, 16)));
         cudaEvent_t evc = nullptr;
         prof_begin(ctx, &evc, s);
-        compact_rerun_kernel<<<cg, 256, 0, s>>>(P.list, P.count, pd.meta.as<gdp_meta_t>(),
-                                                pd.work.as<int32_t>() + ph.start[k],
-                                                pd.work_counts.as<int32_t>() + k);
+        CK(ctx, cub::DeviceSelect::If(pd.sel_tmp.p, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
+                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, s));
         prof_end(ctx, PROF_RERUN, evc, s);
         ctx->launches++;
-        CK(ctx, cudaGetLastError());
         P.list = pd.work.as<int32_t>() + ph.start[k];
         P.count = pd.work_counts.as<int32_t>() + k;
       }
