@@ -737,7 +737,9 @@ work_key (const gdp_pair_t &p, int W) {
   return (uint32_t) (255 - band) << 17 | (uint32_t) std::min(255, lb) << 9 | (uint32_t) (511 - lanes);
 }
 #define KEY_KIND_SHIFT 25   /* sort key = kind << 25 | work key */
-#define KEY_GROUP_SHIFT 9   /* entries with equal key >> 9 share kind, band width and lband */
+#define KEY_GROUP_SHIFT 17  /* entries with equal key >> 17 share kind and band width: the padded groups
+                               (sorted by lband inside, so most warps hold one lband without the padding
+                               of a group per lband) */
 #define KEY_BITS 32         /* kinds below 128 */
 
 /* Kinds whose warps are padded to pairs of one band width: the 16-bit
