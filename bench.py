@@ -303,6 +303,103 @@ def endpoint_search(lib, ctx, seed, ngaps=200000):
     return out
 
 
+def stage3_gaps(genome, seed, ngaps, max_rlength, max_glength):
+    """Single gaps as stage 3 sends them to Dynprog_single_gap: a query
+    stretch between two aligned blocks (4..200 nt, log-uniform) against the
+    genome stretch between them, half of equal length (substitutions only)
+    and half with an indel of up to 10 nt; 1 % substitutions; plus strand;
+    extraband_single = max(3, |glength - rlength|), widebandp, HIGHQ."""
+    rng = np.random.default_rng(seed)
+    rl = np.exp(rng.uniform(np.log(4), np.log(201), ngaps)).astype(np.int64)
+    d = np.where(rng.random(ngaps) < 0.5, 0, rng.integers(-10, 11, ngaps))
+    gl = np.maximum(rl + d, 1)
+    goff = rng.integers(0, genome.size - 512, ngaps)
+    # query = the genome stretch (its first rlength characters, padded with
+    # random bases past glength), then 1 % substitutions
+    tot = int(rl.sum())
+    qoff = np.zeros(ngaps, np.int64)
+    qoff[1:] = np.cumsum(rl)[:-1]
+    idx = np.repeat(goff - qoff, rl) + np.arange(tot)
+    q = genome[idx].copy()
+    within = np.arange(tot) - np.repeat(qoff, rl) < np.repeat(gl, rl)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    q[~within] = rng.choice(acgt, size=int((~within).sum()))
+    sub = rng.random(tot) < 0.01
+    q[sub] = rng.choice(acgt, size=int(sub.sum()))
+    q[q == ord("N")] = ord("A")
+    arena = q   # rsequence and rsequenceuc are the same bytes
+    gaps = np.zeros(ngaps, dtype=gdp.SINGLE_GAP_DTYPE)
+    gaps["rseq"] = gaps["rseq_uc"] = qoff
+    gaps["rlength"], gaps["glength"] = rl, gl
+    gaps["roffset"] = rng.integers(0, 1000, ngaps)
+    gaps["goffset"] = goff
+    gaps["chroffset"], gaps["chrhigh"] = 0, genome.size
+    gaps["watsonp"] = 1
+    gaps["jump_late_p"] = rng.random(ngaps) < 0.5
+    gaps["widebandp"] = 1
+    gaps["extraband_single"] = np.maximum(3, np.abs(gl - rl))
+    gaps["max_rlength"], gaps["max_glength"] = max_rlength, max_glength
+    gaps["dynprogindex"] = 1
+    return gaps, arena
+
+
+def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=20000):
+    """Dynprog_single_gap over a batch of stage-3 single gaps, end to end
+    through gdp_single_gap_batch (host gaps and sequences in, host records
+    out), against the reference's own Dynprog_single_gap on the host (one
+    thread, a bounded sample of the same gaps)."""
+    import torch
+    genome, blocks = gdp.make_genome(lib, 778, 1 << 24)
+    ctx.set_genome(blocks, None, genome.size)
+    gaps, arena = stage3_gaps(genome, seed, ngaps, 500, 2000)
+    res, path, recs = ctx.single_gaps(gaps, arena)
+    dp = path == gdp.SINGLE_DP
+    rl, gl = gaps["rlength"].astype(np.int64), gaps["glength"].astype(np.int64)
+    xb = gaps["extraband_single"].astype(np.int64)
+    lb = np.where(gl >= rl, xb, rl - gl + xb)
+    ub = np.where(gl >= rl, gl - rl + xb, xb)
+    # in-band cells of the fills: rows max(1, c - uband)..min(r, c + lband) per column c
+    cells = 0
+    for i in np.nonzero(dp)[0]:
+        c = np.arange(1, gl[i] + 1)
+        cells += int(np.maximum(0, np.minimum(rl[i], c + lb[i]) - np.maximum(1, c - ub[i]) + 1).sum())
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    times = []
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.single_gaps(gaps, arena)
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = statistics.median(times)
+    out = {"gaps": ngaps, "simple": int((path == gdp.SINGLE_SIMPLE).sum()), "filled": int(dp.sum()),
+           "filled_8bit": int((res["precision"][dp] == 8).sum()), "fill_cells": cells,
+           "records": int(recs.size), "ms": round(ms, 3), "gaps_per_s": round(ngaps / (ms * 1e-3), 1),
+           "fill_gcups": round(cells / (ms * 1e-3) / 1e9, 3), "bad_status": int((res["status"] != 0).sum()),
+           "timing": "host gaps and sequences to host records (gdp_single_gap_batch), median of 3, "
+                     "CUDA events on the context stream"}
+    import oracle
+    if oracle.reference_available():
+        ref = oracle.reference()
+        ref.init(0)
+        ref.set_genome(blocks, None, genome.size)
+        rs = oracle.ReferenceSingleGap(ref, 200, 40)
+        sample = gaps[:cpu_gaps]
+        t0 = time.perf_counter()
+        st, off, rrecs = rs.run(sample, arena)
+        secs = time.perf_counter() - t0
+        same = (np.array_equal(st[:, 0], res["tb_score"][:cpu_gaps]) and
+                np.array_equal(st[:, 5], res["nrecs"][:cpu_gaps]) and
+                np.array_equal(rrecs, recs[:int(res["nrecs"][:cpu_gaps].sum())]))
+        out["cpu_baseline"] = {"value": round(cpu_gaps / secs, 1), "unit": "gaps/s", "cores": 1,
+                               "kind": "reference",
+                               "sample": f"the first {cpu_gaps} gaps, Dynprog_single_gap of oracle/_ref, "
+                                         f"{secs:.2f} s on 1 thread",
+                               "same_results": bool(same)}
+    return out
+
+
 def per_pair_vs_batched(lib, ctx, seed, npairs=20000, nsample=500):
     """The same mixed-length pairs (70/25/5 short/long/cDNA) aligned as one
     batch and as one plan per pair (every pair its own kernel launches),
@@ -559,6 +656,7 @@ def run_gdp(args):
     if rank == 0 and world == 1 and not args.no_per_pair:
         extra["per_pair_vs_batched"] = per_pair_vs_batched(lib, ctx, args.seed + 7)
         extra["endpoint_search"] = endpoint_search(lib, ctx, args.seed + 9)
+        extra["single_gap"] = single_gap_batch(lib, ctx, args.seed + 10)
     if rank == 0 and world == 1 and not args.no_serving:
         extra["serving"] = serving_sweep(lib, local, args.seed + 8,
                                          [1e3, 1e4, 5e4, 1e5, 2e5, 3e5, 5e5, 1e6])

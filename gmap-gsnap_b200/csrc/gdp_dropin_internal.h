@@ -1,8 +1,10 @@
-/* Internal single-pair interface between the runtime (runtime.cu) and the
-   reference-signature entry points (dropin.cu).  Not part of the C ABI. */
+/* Internal interfaces between the runtime (runtime.cu) and its host layers:
+   the reference-signature entry points (dropin.cu) and the single-gap
+   batch (single_gap.cu).  Not part of the C ABI. */
 #ifndef GDP_DROPIN_INTERNAL_H
 #define GDP_DROPIN_INTERNAL_H
 #include <vector>
+#include <cuda_runtime.h>
 #include "gdp_internal.h"
 
 struct gdpi_fill;
@@ -28,4 +30,24 @@ int gdpi_traceback_one(gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const ch
                        gdp_result_t *res, std::vector<gdp_rec_t> *recs);
 void gdpi_fill_free(gdpi_fill *f);
 int gdpi_set_tables(gdp_ctx *ctx, const gdp_tables_t *t);
+
+/* What the single-gap layer (single_gap.cu) reads of a context. */
+struct gdpi_single_cfg {
+  int user_open = 0, user_extend = 0;
+  bool user_p = false;   /* user_dynprog_p */
+};
+struct gdpi_view {
+  int device;
+  cudaStream_t stream;
+  const gdp_tables_t *d_tab;
+  const uint32_t *d_genome, *d_genomealt;   /* d_genomealt == d_genome without an alternate genome */
+  bool has_alt;
+  uint64_t genome_len;
+  int64_t budget;                           /* direction bytes per plan */
+  int nsm;
+  gdpi_single_cfg *single;
+};
+int gdpi_view_of(gdp_ctx *ctx, gdpi_view *v);
+void gdpi_count_launch(gdp_ctx *ctx);
+int gdpi_fail(gdp_ctx *ctx, const char *what, cudaError_t e);
 #endif

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "gdp_internal.h"
+#include "gdp_dropin_internal.h"
 #include "fill_thread.cuh"
 #include "traceback.cuh"
 #include "traceback_warp.cuh"
@@ -303,6 +304,7 @@ struct gdp_ctx {
   int plan_threads = 8;     /* host threads of the planner */
   bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) ... */
   int check_min_x = 1 << 30; /* ... or only for pairs with at least this many rows (lower: columns) */
+  gdpi_single_cfg single;   /* Dynprog_single_setup's user penalties */
   DevBuf arena, scratch, scratch8;
   Slot slot[NSLOTS];
   WorkPool pool;            /* the planner's host threads */
@@ -688,6 +690,7 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   if (p.mismatchtype < 0 || p.mismatchtype > 3) return GDP_ERR_PARAM;
   if (p.open < -127 || p.open > 0 || p.extend < -127 || p.extend > 0) return GDP_ERR_PARAM;
   if (p.genestrand < 0 || p.genestrand > 2) return GDP_ERR_PARAM;
+  if (p.xflags & ~GDP_XFLAG_SEGMENT) return GDP_ERR_PARAM;
   if (p.rlength <= 0 || p.glength <= 0 || p.rlength > (1 << 20) || p.glength > (1 << 20)) return GDP_ERR_LEN;
   if (p.lband < 0 || p.uband < 0) return GDP_ERR_BAND;
   if (arena_bytes >= 0) {
@@ -712,8 +715,16 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
     int64_t lo, hi;
     if (p.watsonp) { lo = (int64_t) p.chroffset + g0; hi = (int64_t) p.chroffset + g1; }
     else { lo = (int64_t) p.chrhigh - g1; hi = (int64_t) p.chrhigh - g0; }
-    lo = std::max<int64_t>(lo, p.chroffset);
-    hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
+    if (p.xflags & GDP_XFLAG_SEGMENT) {
+      /* Genome_get_segment_right stars positions at and above chrhigh,
+         Genome_get_segment_left those below chroffset */
+      if (p.watsonp) hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
+      else lo = std::max<int64_t>(lo, p.chroffset);
+    } else {
+      lo = std::max<int64_t>(lo, p.chroffset);
+      hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
+    }
+    if (lo <= hi && lo < 0) return GDP_ERR_NOGENOME;
     if (genome_len == 0 || (lo <= hi && (uint64_t) hi >= genome_len)) return GDP_ERR_NOGENOME;
   }
   return GDP_OK;
@@ -1912,7 +1923,6 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
 /* points (dropin.cu)                                                  */
 /* ------------------------------------------------------------------ */
 
-#include "gdp_dropin_internal.h"
 
 struct gdpi_fill {
   gdp_pair_t pair;
@@ -2049,6 +2059,32 @@ gdpi_set_tables (gdp_ctx *ctx, const gdp_tables_t *t) {
   CK(ctx, cudaMemcpyAsync(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GDP_OK;
+}
+
+int
+gdpi_view_of (gdp_ctx *ctx, gdpi_view *v) {
+  if (ctx == nullptr || v == nullptr) return GDP_ERR_PARAM;
+  v->device = ctx->device;
+  v->stream = ctx->stream;
+  v->d_tab = ctx->d_tab;
+  v->d_genome = ctx->d_genome;
+  v->d_genomealt = ctx->d_genomealt ? ctx->d_genomealt : ctx->d_genome;
+  v->has_alt = ctx->d_genomealt != nullptr;
+  v->genome_len = ctx->genome_len;
+  v->budget = ctx->budget;
+  v->nsm = ctx->nsm;
+  v->single = &ctx->single;
+  return GDP_OK;
+}
+
+void
+gdpi_count_launch (gdp_ctx *ctx) {
+  ctx->launches++;
+}
+
+int
+gdpi_fail (gdp_ctx *ctx, const char *what, cudaError_t e) {
+  return set_err(ctx, what, e);
 }
 
 /* ------------------------------------------------------------------ */

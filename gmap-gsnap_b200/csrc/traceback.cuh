@@ -18,6 +18,7 @@
  */
 #pragma once
 #include "gdp_internal.h"
+#include "genome_chars.cuh"
 
 struct TbParams {
   const gdp_pair_t *pairs;
@@ -77,49 +78,14 @@ struct DirCursor {
   }
 };
 
-__device__ __forceinline__ char
-gnt_decode (const uint32_t *b, uint32_t pos, bool flags) {
-  const uint32_t ptr = pos / 32u * 3u;
-  const int bit = (int) (pos % 32u);
-  if (flags && (__ldg(b + ptr + 2) & (1u << bit))) return 'N';
-  const uint32_t w = (bit < 16) ? __ldg(b + ptr + 1) : __ldg(b + ptr);
-  const int code = (int) ((w >> ((bit < 16) ? 2 * bit : 2 * bit - 32)) & 3u);
-  return "ACGT"[code];
-}
-
-__device__ __forceinline__ char
-gnt_compl (char c) {
-  return c == 'A' ? 'T' : c == 'C' ? 'G' : c == 'G' ? 'C' : c == 'T' ? 'A' : c;
-}
-
-/*
- * Genome character at genomic coordinate gp of a pair, as get_genomic_nt
- * reads it (src/pairpool.c:1015-1063): chroffset + gp on the plus strand,
- * the complement of chrhigh - gp on the minus strand, '*' outside
- * [chroffset, chrhigh); 32-bit unsigned coordinates.  `genome` holds
- * genomecomp blocks starting at absolute position `base` and covering `len`
- * nt.  Returns 0 when the position lies outside those blocks.
- */
-__device__ __forceinline__ char
-genomic_char (const gdp_pair_t &p, int gp, const uint32_t *genome, const uint32_t *genomealt, uint64_t base,
-              uint64_t len, char *alt) {
-  const uint32_t pos = p.watsonp ? p.chroffset + (uint32_t) gp : p.chrhigh - (uint32_t) gp;
-  if (pos < p.chroffset || pos >= p.chrhigh) { *alt = '*'; return '*'; }
-  if (genome == nullptr || pos < base || pos - base >= len) { *alt = 'N'; return 0; }
-  const uint32_t rp = (uint32_t) (pos - base);
-  const char c = gnt_decode(genome, rp, true);
-  const char ca = (c == 'N') ? c : gnt_decode(genomealt, rp, false);
-  if (p.watsonp) { *alt = ca; return c; }
-  *alt = gnt_compl(ca);
-  return gnt_compl(c);
-}
 
 /*
  * Genome windows of the pairs flagged GDP_FLAG_GWINDOW, read from the
  * resident genome into the arena at gseq (and gseq_alt when it differs):
  * window character j is the genome character at genomic coordinate
  * genomeoffset + j (revp: genomeoffset - (glength - 1) + j), the positions
- * the traceback's genome skips address.  One block per pair.
+ * the traceback's genome skips address (GDP_XFLAG_SEGMENT: as the single
+ * gap's genome segment holds them).  One block per pair.
  */
 __global__ void __launch_bounds__(256)
 window_kernel (const gdp_pair_t *pairs, const int32_t *status, int64_t n, char *arena, const uint32_t *genome,
@@ -131,10 +97,15 @@ window_kernel (const gdp_pair_t *pairs, const int32_t *status, int64_t n, char *
     const int g0 = (p.flags & GDP_FLAG_REVP) ? p.genomeoffset - (gl - 1) : p.genomeoffset;
     char *w = arena + p.gseq, *wa = arena + p.gseq_alt;
     const bool same = (p.gseq_alt == p.gseq);
+    const bool segment = (p.xflags & GDP_XFLAG_SEGMENT) != 0;
     for (int j = threadIdx.x; j < gl; j += blockDim.x) {
-      char a;
-      char c = genomic_char(p, g0 + j, genome, genomealt, 0, genome_len, &a);
-      if (c == 0) { c = 'N'; a = 'N'; }
+      char a, c;
+      if (segment) {
+        c = segment_char(p, g0 + j, genome, genomealt, genome_len, &a);
+      } else {
+        c = genomic_char(p, g0 + j, genome, genomealt, 0, genome_len, &a);
+        if (c == 0) { c = 'N'; a = 'N'; }
+      }
       w[j] = c;
       if (!same) wa[j] = a;
     }

@@ -30,7 +30,7 @@ PAIR_DTYPE = np.dtype([
     ("tb_r", "<i4"), ("tb_c", "<i4"),
     ("queryoffset", "<i4"), ("genomeoffset", "<i4"),
     ("chroffset", "<u4"), ("chrhigh", "<u4"),
-    ("watsonp", "i1"), ("genestrand", "i1"), ("reserved", "<i2"),
+    ("watsonp", "i1"), ("genestrand", "i1"), ("xflags", "<i2"),
     ("dynprogindex", "<i4"),
 ])
 assert PAIR_DTYPE.itemsize == 88
@@ -51,6 +51,20 @@ RESULT_DTYPE = np.dtype([
     ("end_score", "<i4"), ("end_r", "<i4"), ("end_c", "<i4"), ("end_found", "<i4"),
 ])
 assert RESULT_DTYPE.itemsize == 64
+
+XFLAG_SEGMENT = 1
+
+# struct gdp_single_gap, 72 bytes: the arguments of Dynprog_single_gap
+SINGLE_GAP_DTYPE = np.dtype([
+    ("rseq", "<i8"), ("rseq_uc", "<i8"),
+    ("rlength", "<i4"), ("glength", "<i4"), ("roffset", "<i4"), ("goffset", "<i4"),
+    ("chroffset", "<u4"), ("chrhigh", "<u4"),
+    ("watsonp", "i1"), ("genestrand", "i1"), ("jump_late_p", "i1"), ("widebandp", "i1"),
+    ("extraband_single", "<i4"), ("defect_rate", "<f8"),
+    ("max_rlength", "<i4"), ("max_glength", "<i4"), ("dynprogindex", "<i4"), ("pad", "<i4"),
+])
+assert SINGLE_GAP_DTYPE.itemsize == 72
+SINGLE_NULL, SINGLE_SIMPLE, SINGLE_DP = 0, 1, 2
 
 WL_FIXED, WL_SHORT, WL_CDNA, WL_MIX, WL_LONG = 1, 2, 3, 4, 5
 
@@ -119,6 +133,8 @@ def load(path=LIB_PATH):
     lib.gdp_server_destroy.argtypes = [vp]
     ip = ctypes.POINTER(i32)
     lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
+    lib.gdp_single_setup.argtypes = [vp, i32, i32, i32, i32]
+    lib.gdp_single_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, i64, ctypes.POINTER(i64)]
     return lib
 
 
@@ -321,6 +337,25 @@ class Context:
         if rc != 0:
             raise RuntimeError(f"gdp_align_batch: {STATUS.get(rc, rc)} {self.error()}")
         return results, recs[:used.value]
+
+    def single_setup(self, user_open=0, user_extend=0, user_dynprog_p=False, homopolymerp=False):
+        return self.lib.gdp_single_setup(self.h, user_open, user_extend, int(user_dynprog_p), int(homopolymerp))
+
+    def single_gaps(self, gaps, arena, max_recs=None):
+        """Dynprog_single_gap over a batch: (results, path, records)."""
+        n = gaps.size
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        path = np.zeros(n, dtype=np.int8)
+        if max_recs is None:
+            max_recs = int((np.maximum(gaps["rlength"], 0).astype(np.int64)
+                            + np.maximum(gaps["glength"], 0) + 2).sum())
+        recs = np.zeros(max(max_recs, 1), dtype=REC_DTYPE)
+        used = ctypes.c_int64(0)
+        rc = self.lib.gdp_single_gap_batch(self.h, _ptr(gaps), n, _ptr(arena), arena.size, _ptr(results),
+                                           _ptr(path), _ptr(recs), max_recs, ctypes.byref(used))
+        if rc != 0:
+            raise RuntimeError(f"gdp_single_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
+        return results, path, recs[:used.value]
 
     def fill_dump(self, pairs, arena):
         n = pairs.size

@@ -119,9 +119,21 @@ typedef struct gdp_pair {
   int32_t queryoffset, genomeoffset;
   uint32_t chroffset, chrhigh;
   int8_t watsonp, genestrand;
-  int16_t reserved;
+  int16_t xflags;        /* GDP_XFLAG_* (0 for the reference's fills and tracebacks) */
   int32_t dynprogindex;
 } gdp_pair_t;
+
+/* gdp_pair_t.xflags */
+enum {
+  /* GDP_FLAG_GWINDOW windows as Dynprog_single_gap reads its gsequence:
+     Genome_get_segment_right on the plus strand (positions from
+     chroffset + genomeoffset, '*' at and above chrhigh) and the reverse
+     complement of Genome_get_segment_left on the minus strand (positions
+     down from chrhigh - genomeoffset, '*' below chroffset), src/genome.c:
+     11022-11120.  The two differ from get_genomic_nt only on the minus
+     strand at genomic coordinate 0, which reads position chrhigh. */
+  GDP_XFLAG_SEGMENT = 1
+};
 
 /*
  * One traceback Pair record, 12 bytes: the fields of the reference's struct
@@ -367,6 +379,60 @@ int gdp_server_drive(gdp_server *server, const gdp_pair_t *pool, int64_t npool, 
 int gdp_server_stats(gdp_server *server, int64_t *batches, int64_t *pairs, int64_t *max_batch_pairs,
                      int64_t *peak_reserved_bytes, double *busy_s);
 void gdp_server_destroy(gdp_server *server);
+
+/*
+ * Dynprog_single_gap (src/dynprog_single.c:428-675) for a batch of gaps:
+ * the single-gap step of GMAP's stage 3 (src/stage3.c:9117), which fills
+ * the gap between two aligned blocks and traces it back.  Per gap, as the
+ * reference does:
+ *   - rlength <= 0, glength <= 0, or either above max_rlength / max_glength
+ *     (the caller's Dynprog_T sizes): no pairs, traceback score
+ *     NEG_INFINITY_32 (-32768), counts 0 (path GDP_SINGLE_NULL);
+ *   - the genome segment is read from the resident genome (gdp_set_genome)
+ *     as Genome_get_segment_right / _left read it (GDP_XFLAG_SEGMENT);
+ *   - glength == rlength: the ungapped diagonal (single_gap_simple, :345)
+ *     when it has at most one mismatch and at least one pair (path
+ *     GDP_SINGLE_SIMPLE, nopens = nindels = 0);
+ *   - otherwise Dynprog_compute_bands(extraband_single, widebandp), the
+ *     8-bit fill and traceback when rlength and glength are both below
+ *     use8p_size[mismatchtype] (41 HIGHQ, 63 MEDQ, 127 LOWQ), else the
+ *     16-bit ones, from (rlength, glength) (path GDP_SINGLE_DP).
+ * mismatchtype, open and extend follow defect_rate (DEFECT_HIGHQ 0.003,
+ * DEFECT_MEDQ 0.014) or gdp_single_setup's user penalties.
+ *
+ * results[i]: status, score (matrix[glength][rlength] of the DP path, else
+ * 0), precision (8 or 16 for the DP path, else 0), the traceback totals
+ * and the gap's records at rec_offset in `recs`.  Records come in the order
+ * of the List the reference returns, head first (the DP path's push order
+ * after its List_reverse; the simple path from its last query position
+ * down).  path[i] (may be NULL) gets the path taken.  The caller advances
+ * its dynprogindex by one per gap, as the reference does.
+ */
+typedef struct gdp_single_gap {
+  int64_t rseq;          /* rsequence (&queryseq_ptr[querydp5]), rlength bytes of the arena */
+  int64_t rseq_uc;       /* rsequenceuc (&queryuc_ptr[querydp5]) */
+  int32_t rlength, glength;       /* queryjump, genomejump */
+  int32_t roffset, goffset;       /* querydp5, genomedp5 */
+  uint32_t chroffset, chrhigh;
+  int8_t watsonp, genestrand, jump_late_p, widebandp;
+  int32_t extraband_single;
+  double defect_rate;
+  int32_t max_rlength, max_glength;   /* dynprog->max_rlength, dynprog->max_glength */
+  int32_t dynprogindex;
+  int32_t pad;
+} gdp_single_gap_t;
+
+enum { GDP_SINGLE_NULL = 0, GDP_SINGLE_SIMPLE = 1, GDP_SINGLE_DP = 2 };
+
+/* Dynprog_single_setup (src/dynprog_single.c:100): user gap penalties for
+   later gdp_single_gap_batch calls on the context.  homopolymerp != 0 is
+   rejected (GDP_ERR_PARAM): the reference's homopolymer branch fills with a
+   gsequence it never sets (src/dynprog_single.c:524-546). */
+int gdp_single_setup(gdp_ctx *ctx, int user_open, int user_extend, int user_dynprog_p, int homopolymerp);
+
+int gdp_single_gap_batch(gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t ngaps, const char *arena,
+                         int64_t arena_bytes, gdp_result_t *results, int8_t *path, gdp_rec_t *recs,
+                         int64_t max_recs, int64_t *nrecs_used);
 
 /* Kernel launches issued by the context since creation (one per kernel). */
 int64_t gdp_launch_count(gdp_ctx *ctx);

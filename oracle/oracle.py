@@ -119,6 +119,157 @@ class CpuOracle:
         return kept
 
 
+class ReferenceSingleGap:
+    """The reference's own Dynprog_single_gap (oracle/ref_single.c) over a
+    batch of gaps, in a reference library (shares its genome and tables)."""
+
+    def __init__(self, ref, maxlookback, extraquerygap):
+        lib = ref.lib
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        lib.ref_single_init.argtypes = [i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        lib.ref_single_setup.argtypes = [i32, i32, i32]
+        lib.ref_single_gap_batch.argtypes = [vp, i32, vp, vp, vp, i64, vp]
+        lib.ref_single_gap_batch.restype = i64
+        mr, mg = ctypes.c_int(0), ctypes.c_int(0)
+        lib.ref_single_init(maxlookback, extraquerygap, ctypes.byref(mr), ctypes.byref(mg))
+        self.lib = lib
+        self.max_rlength, self.max_glength = mr.value, mg.value
+
+    def setup(self, user_open=0, user_extend=0, user_dynprog_p=False):
+        self.lib.ref_single_setup(user_open, user_extend, int(user_dynprog_p))
+
+    def run(self, gaps, arena):
+        """Per gap: stats (traceback_score, nmatches, nmismatches, nopens,
+        nindels, npairs, list is NULL, dynprogindex after), record offsets,
+        and the records (the returned List, head first)."""
+        n = gaps.size
+        stats = np.zeros((n, 8), np.int32)
+        off = np.zeros(n, np.int64)
+        cap = int((np.maximum(gaps["rlength"], 0).astype(np.int64) + np.maximum(gaps["glength"], 0) + 2).sum()) + 1
+        recs = np.zeros(cap, dtype=_rec_dtype())
+        used = self.lib.ref_single_gap_batch(_ptr(gaps), n, _ptr(arena), _ptr(stats), _ptr(recs), cap, _ptr(off))
+        assert used <= cap
+        return stats, off, recs[:used]
+
+
+def _segment(g, galt, chroffset, chrhigh, goffset, glength, watsonp):
+    """Dynprog_single_gap's gsequence and gsequence_alt: Genome_get_segment_
+    right (plus) or the reverse complement of Genome_get_segment_left
+    (minus), src/genome.c:11022-11120; g and galt are uint8 genomes (ACGTN),
+    galt's characters at g's N positions read N."""
+    compl = {65: 84, 67: 71, 71: 67, 84: 65}
+    seg = np.empty(glength, np.uint8)
+    alt = np.empty(glength, np.uint8)
+    for j in range(glength):
+        pos = chroffset + goffset + j if watsonp else chrhigh - goffset - j
+        if (watsonp and pos >= chrhigh) or (not watsonp and pos < chroffset):
+            seg[j] = alt[j] = 42
+            continue
+        c = int(g[pos])
+        a = c if c == 78 else int(galt[pos])
+        seg[j], alt[j] = (c, a) if watsonp else (compl.get(c, c), compl.get(a, a))
+    return seg, alt
+
+
+def single_gap_restated(orc, gaps, arena, g, galt, user=None):
+    """Dynprog_single_gap (src/dynprog_single.c:428-675) restated over a CPU
+    oracle's fill and traceback (orc: restatement() or reference(), tables
+    and genome set).  Returns the same (stats, offsets, records) as
+    ReferenceSingleGap.run, without the dynprogindex column's update."""
+    n = gaps.size
+    stats = np.zeros((n, 8), np.int32)
+    off = np.zeros(n, np.int64)
+    out = []
+    used = 0
+    for i in range(n):
+        x = gaps[i]
+        rl, gl = int(x["rlength"]), int(x["glength"])
+        off[i] = used
+        stats[i, 7] = int(x["dynprogindex"])
+        if rl <= 0 or gl <= 0 or rl > int(x["max_rlength"]) or gl > int(x["max_glength"]):
+            stats[i, :7] = (-32768, 0, 0, 0, 0, 0, 1)
+            continue
+        seg, alt = _segment(g, galt, int(x["chroffset"]), int(x["chrhigh"]), int(x["goffset"]), gl,
+                            bool(x["watsonp"]))
+        rs = arena[int(x["rseq"]):int(x["rseq"]) + rl]
+        ru = arena[int(x["rseq_uc"]):int(x["rseq_uc"]) + rl]
+        q = 0 if x["defect_rate"] < 0.003 else 1 if x["defect_rate"] < 0.014 else 2
+        if gl == rl:
+            # single_gap_simple (:345-425): pushed left to right, so the List
+            # starts at the last position
+            score = nmatch = nmis = 0
+            recs = []
+            for k in range(rl):
+                c1, cu, c2, ca = int(rs[k]), int(ru[k]), int(seg[k]), int(alt[k])
+                if c2 == 42:
+                    continue
+                if cu == c2 or cu == ca:
+                    comp = b"*"
+                elif orc.consistent(int(x["genestrand"]), cu, c2) or orc.consistent(int(x["genestrand"]), cu, ca):
+                    comp = b":"
+                else:
+                    comp = b" "
+                if comp == b" ":
+                    score -= 3
+                    nmis += 1
+                else:
+                    score += 1
+                    nmatch += 1
+                qp, gp = int(x["roffset"]) + k, int(x["goffset"]) + k
+                if qp >= 0 and gp >= 0:
+                    recs.append((qp, gp, bytes([c1]), comp, bytes([c2]), bytes([ca])))
+            if nmis <= 1 and recs:
+                stats[i, :7] = (score, nmatch, nmis, 0, 0, len(recs), 0)
+                out.extend(reversed(recs))
+                used += len(recs)
+                continue
+        # the fill (:599-650): bands, precision by use8p_size, traceback from (rlength, glength)
+        xb = int(x["extraband_single"])
+        if not x["widebandp"]:
+            lb = ub = xb
+        elif gl >= rl:
+            lb, ub = xb, gl - rl + xb
+        else:
+            lb, ub = rl - gl + xb, xb
+        use8p = 128 // (3, 2, 1)[q] - 1
+        p = np.zeros(1, dtype=_pair_dtype())
+        local = np.concatenate([rs, ru, seg, alt])
+        p["rseq"], p["rseq_uc"], p["gseq"], p["gseq_alt"] = 0, rl, 2 * rl, 2 * rl + gl
+        p["rlength"], p["glength"], p["lband"], p["uband"] = rl, gl, lb, ub
+        p["variant"] = 0
+        p["precision"] = 8 if (rl < use8p and gl < use8p) else 16
+        p["mismatchtype"] = q
+        p["flags"] = 4 | (1 if x["jump_late_p"] else 0)
+        if user is not None:
+            p["open"], p["extend"] = user
+        else:
+            p["open"], p["extend"] = (-8, -7, -6)[q], (-3, -2, -1)[q]
+        p["tb_r"], p["tb_c"] = rl, gl
+        p["queryoffset"], p["genomeoffset"] = int(x["roffset"]), int(x["goffset"])
+        p["chroffset"], p["chrhigh"] = int(x["chroffset"]), int(x["chrhigh"])
+        p["watsonp"], p["genestrand"] = int(x["watsonp"]), int(x["genestrand"])
+        p["dynprogindex"] = int(x["dynprogindex"])
+        r = orc.align(p, 0, local, want_matrix=False)
+        st = r["stats"]
+        stats[i, :7] = (st[0], st[1], st[2], st[3], st[4], r["nrecs"], r["nrecs"] == 0)
+        for rec in r["recs"]:
+            out.append(tuple(rec))
+        used += len(r["recs"])
+    recs = np.array(out, dtype=_rec_dtype()) if out else np.zeros(0, dtype=_rec_dtype())
+    return stats, off, recs
+
+
+def _pair_dtype():
+    """struct gdp_pair (include/gdp.h), 88 bytes."""
+    return np.dtype([
+        ("rseq", "<i8"), ("rseq_uc", "<i8"), ("gseq", "<i8"), ("gseq_alt", "<i8"),
+        ("rlength", "<i4"), ("glength", "<i4"), ("lband", "<i4"), ("uband", "<i4"),
+        ("variant", "i1"), ("precision", "i1"), ("mismatchtype", "i1"), ("flags", "i1"),
+        ("open", "<i2"), ("extend", "<i2"), ("tb_r", "<i4"), ("tb_c", "<i4"),
+        ("queryoffset", "<i4"), ("genomeoffset", "<i4"), ("chroffset", "<u4"), ("chrhigh", "<u4"),
+        ("watsonp", "i1"), ("genestrand", "i1"), ("xflags", "<i2"), ("dynprogindex", "<i4")])
+
+
 def _rec_dtype():
     return np.dtype([("querypos", "<i4"), ("genomepos", "<i4"),
                      ("cdna", "S1"), ("comp", "S1"), ("genome", "S1"), ("genomealt", "S1")])

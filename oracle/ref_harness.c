@@ -61,6 +61,9 @@ ref_set_genome (const uint32_t *blocks, const uint32_t *altblocks, uint64_t geno
   genome_set = 1;
 }
 
+Genome_T ref_genome_main (void) { return &genome_main; }
+Genome_T ref_genome_alt (void) { return &genome_alt; }
+
 static const char ACGT[4] = {'A', 'C', 'G', 'T'};
 
 static char

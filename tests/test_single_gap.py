@@ -1,0 +1,126 @@
+"""Dynprog_single_gap over a batch (gdp_single_gap_batch).
+
+* CPU: the restated single gap (oracle.single_gap_restated: the host
+  decisions and single_gap_simple in Python, the fill and traceback of the
+  C restatement) equals the reference's own Dynprog_single_gap
+  (src/dynprog_single.c:428-675, compiled into oracle/_ref) on every gap:
+  traceback score and counts, NULL lists, and the returned List record by
+  record.
+* GPU: gdp_single_gap_batch equals the reference's Dynprog_single_gap on
+  the same gaps, with and without an alternate genome and with user
+  penalties (Dynprog_single_setup).
+"""
+import numpy as np
+import pytest
+
+import gdp
+import oracle
+import single_cases
+
+GENOME_LEN = 1 << 16
+MAXLOOKBACK, EXTRAQUERYGAP = 200, 40
+
+
+@pytest.fixture(scope="module")
+def genome():
+    return single_cases.genome_pair(77, GENOME_LEN)
+
+
+@pytest.fixture(scope="module")
+def ref_single(reference):
+    return oracle.ReferenceSingleGap(reference, MAXLOOKBACK, EXTRAQUERYGAP)
+
+
+def _gaps(seed, n, ref_single, genome):
+    return single_cases.single_gap_cases(seed, n, genome[0], ref_single.max_rlength, ref_single.max_glength)
+
+
+def _check_same(stats_a, off_a, recs_a, stats_b, off_b, recs_b, what):
+    bad = np.nonzero((stats_a[:, :7] != stats_b[:, :7]).any(axis=1))[0]
+    assert bad.size == 0, f"{what}: stats differ at gaps {bad[:8].tolist()}: {stats_a[bad[:3]]} vs {stats_b[bad[:3]]}"
+    for i in range(stats_a.shape[0]):
+        k = int(stats_a[i, 5])
+        a = recs_a[int(off_a[i]):int(off_a[i]) + k]
+        b = recs_b[int(off_b[i]):int(off_b[i]) + k]
+        assert np.array_equal(a, b), f"{what}: records of gap {i} differ"
+
+
+def test_restatement_matches_reference(reference, restatement, ref_single, genome):
+    g, alt, blocks, altblocks = genome
+    reference.set_genome(blocks, altblocks, GENOME_LEN)
+    restatement.set_genome(blocks, altblocks, GENOME_LEN)
+    ref_single.setup()
+    gaps, arena = _gaps(3, 400, ref_single, genome)
+    st_r, off_r, rec_r = ref_single.run(gaps, arena)
+    st_o, off_o, rec_o = oracle.single_gap_restated(restatement, gaps, arena, g, alt)
+    _check_same(st_r, off_r, rec_r, st_o, off_o, rec_o, "restatement")
+    # every branch of the single gap was taken
+    nulls = st_r[:, 6] == 1
+    simple = (gaps["rlength"] == gaps["glength"]) & ~nulls & (st_r[:, 3] == 0) & (st_r[:, 2] <= 1)
+    assert nulls.sum() >= 5 and simple.sum() >= 50 and (~nulls & ~simple).sum() >= 100
+    badlen = ((gaps["rlength"] <= 0) | (gaps["glength"] <= 0) | (gaps["rlength"] > ref_single.max_rlength)
+              | (gaps["glength"] > ref_single.max_glength))
+    assert badlen.sum() >= 5 and (st_r[badlen, 0] == -32768).all() and (st_r[badlen, 6] == 1).all()
+    # the reference advances dynprogindex away from zero by one per gap
+    dpi = gaps["dynprogindex"]
+    assert np.array_equal(st_r[:, 7], dpi + np.sign(dpi))
+
+
+def test_restatement_user_penalties(reference, restatement, ref_single, genome):
+    g, alt, blocks, altblocks = genome
+    reference.set_genome(blocks, None, GENOME_LEN)
+    restatement.set_genome(blocks, None, GENOME_LEN)
+    ref_single.setup(-11, -1, True)
+    try:
+        gaps, arena = _gaps(4, 150, ref_single, genome)
+        st_r, off_r, rec_r = ref_single.run(gaps, arena)
+        st_o, off_o, rec_o = oracle.single_gap_restated(restatement, gaps, arena, g, g, user=(-11, -1))
+        _check_same(st_r, off_r, rec_r, st_o, off_o, rec_o, "user penalties")
+    finally:
+        ref_single.setup()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("alt_genome", [True, False])
+def test_single_gap_batch_matches_reference(gdplib, reference, ref_single, genome, alt_genome):
+    g, alt, blocks, altblocks = genome
+    reference.set_genome(blocks, altblocks if alt_genome else None, GENOME_LEN)
+    ctx = gdp.Context(gdplib)
+    try:
+        ctx.set_genome(blocks, altblocks if alt_genome else None, GENOME_LEN)
+        gaps, arena = _gaps(11 + alt_genome, 3000, ref_single, genome)
+        res, path, recs = ctx.single_gaps(gaps, arena)
+        assert ctx.launches() > 0
+    finally:
+        ctx.close()
+    st_r, off_r, rec_r = ref_single.run(gaps, arena)
+    assert (res["status"] == 0).all(), np.unique(res["status"])
+    st_d = np.stack([res["tb_score"], res["nmatches"], res["nmismatches"], res["nopens"], res["nindels"],
+                     res["nrecs"], (res["nrecs"] == 0).astype(np.int32), st_r[:, 7]], axis=1)
+    _check_same(st_r, off_r, rec_r, st_d, res["rec_offset"], recs, "device")
+    assert (path == gdp.SINGLE_SIMPLE).sum() > 300 and (path == gdp.SINGLE_DP).sum() > 1000
+    dp = path == gdp.SINGLE_DP
+    assert set(np.unique(res["precision"][dp]).tolist()) == {8, 16}
+
+
+@pytest.mark.gpu
+def test_single_gap_batch_user_penalties(gdplib, reference, ref_single, genome):
+    g, alt, blocks, altblocks = genome
+    reference.set_genome(blocks, altblocks, GENOME_LEN)
+    ctx = gdp.Context(gdplib)
+    try:
+        ctx.set_genome(blocks, altblocks, GENOME_LEN)
+        assert ctx.single_setup(-11, -1, True) == 0
+        assert ctx.single_setup(0, 0, False, homopolymerp=True) == 3   # GDP_ERR_PARAM
+        gaps, arena = _gaps(21, 800, ref_single, genome)
+        res, path, recs = ctx.single_gaps(gaps, arena)
+    finally:
+        ctx.close()
+    ref_single.setup(-11, -1, True)
+    try:
+        st_r, off_r, rec_r = ref_single.run(gaps, arena)
+    finally:
+        ref_single.setup()
+    st_d = np.stack([res["tb_score"], res["nmatches"], res["nmismatches"], res["nopens"], res["nindels"],
+                     res["nrecs"], (res["nrecs"] == 0).astype(np.int32), st_r[:, 7]], axis=1)
+    _check_same(st_r, off_r, rec_r, st_d, res["rec_offset"], recs, "device, user penalties")
