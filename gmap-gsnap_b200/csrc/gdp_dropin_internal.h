@@ -31,11 +31,25 @@ int gdpi_traceback_one(gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const ch
 void gdpi_fill_free(gdpi_fill *f);
 int gdpi_set_tables(gdp_ctx *ctx, const gdp_tables_t *t);
 
-/* What the single-gap layer (single_gap.cu) reads of a context. */
+/* The single-gap layer's state in a context (single_gap.cu): the user
+   penalties of Dynprog_single_setup, and its working memory, kept between
+   calls: grow-only device buffers, pinned host staging and one plan whose
+   buffers are reused. */
+struct gdp_plan;
 struct gdpi_single_cfg {
   int user_open = 0, user_extend = 0;
   bool user_p = false;   /* user_dynprog_p */
+  static constexpr int NBUF = 16;
+  void *dbuf[NBUF] = {};
+  size_t dcap[NBUF] = {};
+  void *hbuf[NBUF] = {};
+  size_t hcap[NBUF] = {};
+  gdp_plan *plan = nullptr;
 };
+/* Plans pairs[0..n) into *plan (created on first use; its host and device
+   buffers only grow) and uploads the plan on the context stream. */
+int gdpi_plan_reuse(gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t n);
+void gdpi_single_release(gdpi_single_cfg *c);
 struct gdpi_view {
   int device;
   cudaStream_t stream;

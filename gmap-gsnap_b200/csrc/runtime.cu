@@ -443,6 +443,7 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
       cudaStreamDestroy(ctx->wave_stream[k]);
     }
   ctx->arena.release(); ctx->scratch.release(); ctx->scratch8.release();
+  gdpi_single_release(&ctx->single);
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
   if (ctx->d_genomealt) cudaFree(ctx->d_genomealt);
@@ -2059,6 +2060,29 @@ gdpi_set_tables (gdp_ctx *ctx, const gdp_tables_t *t) {
   CK(ctx, cudaMemcpyAsync(ctx->d_tab, ctx->h_tab, sizeof(gdp_tables_t), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return GDP_OK;
+}
+
+int
+gdpi_plan_reuse (gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t n) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (*plan == nullptr) *plan = new gdp_plan();
+  gdp_plan *pl = *plan;
+  int rc = plan_build(ctx, pairs, n, -1, pl->h);
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl->h, pl->d, false, ctx->stream);
+  return rc;
+}
+
+void
+gdpi_single_release (gdpi_single_cfg *c) {
+  for (int k = 0; k < gdpi_single_cfg::NBUF; k++) {
+    if (c->dbuf[k]) cudaFree(c->dbuf[k]);
+    if (c->hbuf[k]) cudaFreeHost(c->hbuf[k]);
+    c->dbuf[k] = c->hbuf[k] = nullptr;
+    c->dcap[k] = c->hcap[k] = 0;
+  }
+  if (c->plan) gdp_plan_destroy(c->plan);
+  c->plan = nullptr;
 }
 
 int

@@ -25,6 +25,7 @@
  * reference returns.
  */
 #include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -128,20 +129,112 @@ single_simple_kernel (const gdp_pair_t *cand, int64_t n, const char *arena, cons
   }
 }
 
-/* Stream-ordered device buffers of one call, freed on every return path. */
-struct CallBufs {
-  cudaStream_t s;
-  std::vector<void *> held;
-  explicit CallBufs (cudaStream_t st) : s(st) {}
-  template <class T> cudaError_t get (T **p, int64_t count) {
-    void *q = nullptr;
-    cudaError_t e = cudaMallocAsync(&q, (size_t) std::max<int64_t>(count, 1) * sizeof(T), s);
-    if (e == cudaSuccess) held.push_back(q);
-    *p = (T *) q;
-    return e;
-  }
-  ~CallBufs () { for (void *q : held) cudaFreeAsync(q, s); cudaStreamSynchronize(s); }
+/* Where a gap's outcome lives. */
+enum { SRC_NULL = 0, SRC_SIMPLE = 1, SRC_FILL = 2, SRC_ERROR = 3 };
+struct GapSrc {
+  int32_t kind;
+  int32_t idx;     /* SRC_SIMPLE: candidate index; SRC_FILL: fill index; SRC_ERROR: the status */
 };
+
+__global__ void __launch_bounds__(256)
+single_count_kernel (const GapSrc *src, int64_t n, const SimpleOut *sout, const gdp_result_t *fres, int64_t *count) {
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t) gridDim.x * blockDim.x) {
+    int64_t c = 0;
+    if (i < n) {
+      const GapSrc g = src[i];
+      if (g.kind == SRC_SIMPLE) c = sout[g.idx].nrecs;
+      else if (g.kind == SRC_FILL && fres[g.idx].status == GDP_OK) c = fres[g.idx].nrecs;
+    }
+    count[i] = c;   /* count[n] = 0: the scan's last entry is the total */
+  }
+}
+
+/*
+ * Final results and records in gap order, one warp per gap: the gap's
+ * records go to out[off[i] ..) (gaps whose records would pass max_recs get
+ * GDP_ERR_RECS and none), and *used gets the end of the records written.
+ */
+__global__ void __launch_bounds__(256)
+single_gather_kernel (const GapSrc *src, int64_t n, const int64_t *off, int64_t max_recs, const SimpleOut *sout,
+                      const gdp_rec_t *srecs, const int64_t *soff, const gdp_result_t *fres,
+                      const gdp_rec_t *const *fslots, gdp_result_t *res, gdp_rec_t *out,
+                      unsigned long long *used) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    const GapSrc g = src[i];
+    gdp_result_t r;
+    memset(&r, 0, sizeof(r));
+    const gdp_rec_t *from = nullptr;
+    int64_t cnt = 0;
+    if (g.kind == SRC_NULL) {
+      r.tb_score = NEG_INFINITY_32;
+    } else if (g.kind == SRC_ERROR) {
+      r.status = g.idx;
+    } else if (g.kind == SRC_SIMPLE) {
+      const SimpleOut o = sout[g.idx];
+      r.tb_score = o.score; r.nmatches = o.nmatch; r.nmismatches = o.nmismatch;
+      cnt = o.nrecs;
+      from = srecs + soff[g.idx];
+    } else {
+      r = fres[g.idx];
+      cnt = (r.status == GDP_OK) ? r.nrecs : 0;
+      from = fslots[g.idx] + r.rec_offset;
+    }
+    const int64_t o = off[i];
+    if (o + cnt > max_recs) {
+      r.status = GDP_ERR_RECS;
+      cnt = 0;
+    }
+    r.nrecs = (int32_t) cnt;
+    r.rec_offset = o;
+    /* a record is three 32-bit words */
+    const uint32_t *fw = reinterpret_cast<const uint32_t *>(from);
+    uint32_t *ow = reinterpret_cast<uint32_t *>(out + o);
+    for (int64_t w = lane; w < 3 * cnt; w += 32) ow[w] = fw[w];
+    if (lane == 0) {
+      res[i] = r;
+      if (cnt > 0) atomicMax(used, (unsigned long long) (o + cnt));
+    }
+  }
+}
+
+/* The context's grow-only working buffers: device slot k, pinned host slot k. */
+enum { D_ARENA, D_CAND, D_SOFF, D_SOUT, D_SRECS, D_FILL, D_FRES, D_SLOTS, D_SRC, D_COUNT, D_OFF, D_FSLOT, D_RES,
+       D_OUT, D_USED, D_TMP };
+enum { H_CAND, H_SOFF, H_SOUT, H_FILL, H_SRC, H_FSLOT, H_WORDS };
+
+template <class T> cudaError_t
+dev_slot (gdpi_single_cfg *c, int k, T **p, int64_t count) {
+  const size_t need = (size_t) std::max<int64_t>(count, 1) * sizeof(T);
+  if (c->dcap[k] < need) {
+    if (c->dbuf[k]) cudaFree(c->dbuf[k]);
+    c->dbuf[k] = nullptr;
+    c->dcap[k] = 0;
+    const size_t cap = need + need / 4;
+    cudaError_t e = cudaMalloc(&c->dbuf[k], cap);
+    if (e != cudaSuccess) return e;
+    c->dcap[k] = cap;
+  }
+  *p = (T *) c->dbuf[k];
+  return cudaSuccess;
+}
+
+template <class T> cudaError_t
+host_slot (gdpi_single_cfg *c, int k, T **p, int64_t count) {
+  const size_t need = (size_t) std::max<int64_t>(count, 1) * sizeof(T);
+  if (c->hcap[k] < need) {
+    if (c->hbuf[k]) cudaFreeHost(c->hbuf[k]);
+    c->hbuf[k] = nullptr;
+    c->hcap[k] = 0;
+    const size_t cap = need + need / 4;
+    cudaError_t e = cudaMallocHost(&c->hbuf[k], cap);
+    if (e != cudaSuccess) return e;
+    c->hcap[k] = cap;
+  }
+  *p = (T *) c->hbuf[k];
+  return cudaSuccess;
+}
 
 /* The reference's choices for one gap (src/dynprog_single.c:453-481, :612-617). */
 struct GapSetup {
@@ -257,43 +350,47 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
     if (g.glength == g.rlength) cand.push_back(i); else fill.push_back(i);
   }
 
-  CallBufs B(s);
+  gdpi_single_cfg *C = v.single;
   /* the arena, followed by the segments of the gaps that may need a fill */
   const int64_t seg_base = (arena_bytes + 15) / 16 * 16;
   int64_t seg_bytes = 0;
   for (int64_t i = 0; i < n; i++)
     if (kind[i] == GDP_SINGLE_DP) seg_bytes += (int64_t) gaps[i].glength * (v.has_alt ? 2 : 1);
   char *d_arena = nullptr;
-  SCK(B.get(&d_arena, seg_base + seg_bytes));
+  SCK(dev_slot(C, D_ARENA, &d_arena, seg_base + seg_bytes));
   if (arena_bytes > 0) SCK(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, s));
 
   /* phase 1: the ungapped diagonal of the equal-length gaps */
-  std::vector<SimpleOut> sout(cand.size());
-  std::vector<int64_t> soff(cand.size() + 1, 0);
+  const int64_t nc = (int64_t) cand.size();
   gdp_rec_t *d_srecs = nullptr;
-  if (!cand.empty()) {
-    std::vector<gdp_pair_t> cp(cand.size());
-    for (size_t k = 0; k < cand.size(); k++) {
+  int64_t *d_soff = nullptr;
+  SimpleOut *d_sout = nullptr;
+  if (nc > 0) {
+    gdp_pair_t *cp = nullptr, *d_cp = nullptr;
+    int64_t *soff = nullptr;
+    SimpleOut *sout = nullptr;
+    SCK(host_slot(C, H_CAND, &cp, nc));
+    SCK(host_slot(C, H_SOFF, &soff, nc + 1));
+    SCK(host_slot(C, H_SOUT, &sout, nc));
+    soff[0] = 0;
+    for (int64_t k = 0; k < nc; k++) {
       cp[k] = base_pair(gaps[cand[k]]);
       soff[k + 1] = soff[k] + gaps[cand[k]].rlength;
     }
-    gdp_pair_t *d_cp = nullptr;
-    int64_t *d_soff = nullptr;
-    SimpleOut *d_sout = nullptr;
-    SCK(B.get(&d_cp, (int64_t) cand.size()));
-    SCK(B.get(&d_soff, (int64_t) cand.size()));
-    SCK(B.get(&d_sout, (int64_t) cand.size()));
-    SCK(B.get(&d_srecs, soff.back()));
-    SCK(cudaMemcpyAsync(d_cp, cp.data(), cp.size() * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s));
-    SCK(cudaMemcpyAsync(d_soff, soff.data(), cand.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    const int64_t blocks = std::min<int64_t>(((int64_t) cand.size() + 7) / 8, (int64_t) v.nsm * 8);
-    single_simple_kernel<<<(int) blocks, 256, 0, s>>>(d_cp, (int64_t) cand.size(), d_arena, d_soff, d_srecs, d_sout,
-                                                       v.d_genome, v.d_genomealt, v.genome_len, v.d_tab);
+    SCK(dev_slot(C, D_CAND, &d_cp, nc));
+    SCK(dev_slot(C, D_SOFF, &d_soff, nc));
+    SCK(dev_slot(C, D_SOUT, &d_sout, nc));
+    SCK(dev_slot(C, D_SRECS, &d_srecs, soff[nc]));
+    SCK(cudaMemcpyAsync(d_cp, cp, nc * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s));
+    SCK(cudaMemcpyAsync(d_soff, soff, nc * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const int64_t blocks = std::min<int64_t>((nc + 7) / 8, (int64_t) v.nsm * 8);
+    single_simple_kernel<<<(int) blocks, 256, 0, s>>>(d_cp, nc, d_arena, d_soff, d_srecs, d_sout, v.d_genome,
+                                                       v.d_genomealt, v.genome_len, v.d_tab);
     gdpi_count_launch(ctx);
     SCK(cudaGetLastError());
-    SCK(cudaMemcpyAsync(sout.data(), d_sout, cand.size() * sizeof(SimpleOut), cudaMemcpyDeviceToHost, s));
+    SCK(cudaMemcpyAsync(sout, d_sout, nc * sizeof(SimpleOut), cudaMemcpyDeviceToHost, s));
     SCK(cudaStreamSynchronize(s));
-    for (size_t k = 0; k < cand.size(); k++) {
+    for (int64_t k = 0; k < nc; k++) {
       if (sout[k].simple) kind[cand[k]] = GDP_SINGLE_SIMPLE;
       else fill.push_back(cand[k]);
     }
@@ -301,12 +398,19 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
   }
 
   /* phase 2: fills and tracebacks of the rest, in plans within the budget */
-  std::vector<gdp_pair_t> fp(fill.size());
+  const int64_t nf = (int64_t) fill.size();
+  gdp_pair_t *fp = nullptr, *d_fp = nullptr;
+  gdp_result_t *d_fres = nullptr;
+  gdp_rec_t *d_slots = nullptr;
+  const gdp_rec_t **fslot = nullptr, **d_fslot = nullptr;
+  SCK(host_slot(C, H_FILL, &fp, nf));
+  SCK(host_slot(C, H_FSLOT, &fslot, nf));
+  int64_t slot_total = 0;   /* record slots of all fills: rlength + glength + 2 each */
   {
     int64_t seg = seg_base;
-    for (size_t k = 0; k < fill.size(); k++) {
+    for (int64_t k = 0; k < nf; k++) {
       const gdp_single_gap_t &g = gaps[fill[k]];
-      const GapSetup st = gap_setup(g, *v.single);
+      const GapSetup st = gap_setup(g, *C);
       gdp_pair_t p = base_pair(g);
       p.lband = st.lband; p.uband = st.uband;
       p.precision = (int8_t) st.precision;
@@ -317,87 +421,94 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
       p.gseq_alt = v.has_alt ? seg + g.glength : seg;
       seg += (int64_t) g.glength * (v.has_alt ? 2 : 1);
       fp[k] = p;
+      slot_total += (int64_t) g.rlength + g.glength + 2;
     }
   }
-  std::vector<gdp_result_t> fres(fill.size());
-  std::vector<gdp_rec_t> frecs;
-  std::vector<int64_t> frec_base(fill.size(), 0);
-  for (size_t k0 = 0; k0 < fill.size();) {
+  SCK(dev_slot(C, D_FILL, &d_fp, nf));
+  SCK(dev_slot(C, D_FRES, &d_fres, nf));
+  SCK(dev_slot(C, D_SLOTS, &d_slots, slot_total));
+  if (nf > 0) SCK(cudaMemcpyAsync(d_fp, fp, nf * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s));
+  int64_t slot_used = 0;
+  for (int64_t k0 = 0; k0 < nf;) {
     /* one plan: gaps k0..k1 while their direction bytes stay in the budget */
-    size_t k1 = k0;
-    int64_t bytes = 0;
-    while (k1 < fill.size()) {
+    int64_t k1 = k0, bytes = 0;
+    while (k1 < nf) {
       const int64_t b = gdp_pair_words(&fp[k1], fp[k1].precision == 8 ? 32 : 16) * 4;
       if (k1 > k0 && bytes + b > v.budget) break;
       bytes += b;
       k1++;
     }
-    const int64_t m = (int64_t) (k1 - k0);
-    gdp_plan *pl = nullptr;
-    int rc = gdp_plan_create(ctx, fp.data() + k0, m, &pl);
+    int rc = gdpi_plan_reuse(ctx, &C->plan, fp + k0, k1 - k0);
     if (rc != GDP_OK) return rc;
-    const int64_t nr = gdp_plan_total_recs(pl);
-    gdp_pair_t *d_fp = nullptr;
-    gdp_result_t *d_fres = nullptr;
-    gdp_rec_t *d_frecs = nullptr;
-    cudaError_t e = B.get(&d_fp, m);
-    if (e == cudaSuccess) e = B.get(&d_fres, m);
-    if (e == cudaSuccess) e = B.get(&d_frecs, nr);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_fp, fp.data() + k0, m * sizeof(gdp_pair_t), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) { gdp_plan_destroy(pl); return gdpi_fail(ctx, "single-gap fill buffers", e); }
-    rc = gdp_plan_execute(ctx, pl, d_fp, d_arena, d_fres, d_frecs);
-    if (rc != GDP_OK) { gdp_plan_destroy(pl); return rc; }
-    const size_t base = frecs.size();
-    frecs.resize(base + (size_t) nr);
-    e = cudaMemcpyAsync(fres.data() + k0, d_fres, m * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess && nr > 0)
-      e = cudaMemcpyAsync(frecs.data() + base, d_frecs, nr * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    gdp_plan_destroy(pl);
-    if (e != cudaSuccess) return gdpi_fail(ctx, "single-gap fill results", e);
-    for (int64_t k = 0; k < m; k++) frec_base[k0 + k] = (int64_t) base;
+    const int64_t nr = gdp_plan_total_recs(C->plan);
+    if (slot_used + nr > slot_total) return GDP_ERR_RECS;   /* the planner's bound is the one above */
+    rc = gdp_plan_execute(ctx, C->plan, d_fp + k0, d_arena, d_fres + k0, d_slots + slot_used);
+    if (rc != GDP_OK) return rc;
+    for (int64_t k = k0; k < k1; k++) fslot[k] = d_slots + slot_used;
+    slot_used += nr;
+    if (k1 < nf) SCK(cudaStreamSynchronize(s));   /* the plan's buffers are reused by the next plan */
     k0 = k1;
   }
 
-  /* simple records */
-  std::vector<gdp_rec_t> srecs((size_t) soff.back());
-  if (!cand.empty() && soff.back() > 0) {
-    SCK(cudaMemcpyAsync(srecs.data(), d_srecs, soff.back() * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, s));
-    SCK(cudaStreamSynchronize(s));
-  }
-
-  /* assemble per gap, in gap order */
-  std::vector<int64_t> cand_of((size_t) n, -1), fill_of((size_t) n, -1);
-  for (size_t k = 0; k < cand.size(); k++) cand_of[cand[k]] = (int64_t) k;
-  for (size_t k = 0; k < fill.size(); k++) fill_of[fill[k]] = (int64_t) k;
-  int64_t used = 0;
-  for (int64_t i = 0; i < n; i++) {
-    gdp_result_t &r = results[i];
-    const gdp_rec_t *src = nullptr;
-    int32_t cnt = 0;
-    if (kind[i] == GDP_SINGLE_SIMPLE) {
-      const SimpleOut &o = sout[cand_of[i]];
-      r.tb_score = o.score; r.nmatches = o.nmatch; r.nmismatches = o.nmismatch;
-      cnt = o.nrecs;
-      src = srecs.data() + soff[cand_of[i]];
-    } else if (kind[i] == GDP_SINGLE_DP) {
-      const int64_t k = fill_of[i];
-      r = fres[k];
-      cnt = (r.status == GDP_OK) ? r.nrecs : 0;
-      src = frecs.data() + frec_base[k] + r.rec_offset;
-    }
-    r.rec_offset = used;
-    r.nrecs = cnt;
-    if (cnt > 0) {
-      if (used + cnt > max_recs) {
-        r.status = GDP_ERR_RECS;
-        r.nrecs = 0;
+  /* results and records in gap order, on the device */
+  GapSrc *src = nullptr, *d_src = nullptr;
+  SCK(host_slot(C, H_SRC, &src, n));
+  {
+    int64_t ci = 0, fi = 0;
+    for (int64_t i = 0; i < n; i++) {
+      GapSrc g{SRC_NULL, 0};
+      if (kind[i] == GDP_SINGLE_NULL) {
+        if (results[i].status != GDP_OK) g = GapSrc{SRC_ERROR, results[i].status};
+      } else if (kind[i] == GDP_SINGLE_SIMPLE) {
+        while (cand[ci] < i) ci++;
+        g = GapSrc{SRC_SIMPLE, (int32_t) ci};
       } else {
-        memcpy(recs + used, src, (size_t) cnt * sizeof(gdp_rec_t));
-        used += cnt;
+        while (fill[fi] < i) fi++;
+        g = GapSrc{SRC_FILL, (int32_t) fi};
       }
+      src[i] = g;
+      if (path) path[i] = kind[i];
     }
-    if (path) path[i] = kind[i];
+  }
+  int64_t *d_count = nullptr, *d_off = nullptr, *words = nullptr;
+  gdp_result_t *d_res = nullptr;
+  gdp_rec_t *d_out = nullptr;
+  unsigned long long *d_used = nullptr;
+  SCK(host_slot(C, H_WORDS, &words, 2));
+  SCK(dev_slot(C, D_SRC, &d_src, n));
+  SCK(dev_slot(C, D_COUNT, &d_count, n + 1));
+  SCK(dev_slot(C, D_OFF, &d_off, n + 1));
+  SCK(dev_slot(C, D_FSLOT, &d_fslot, nf));
+  SCK(dev_slot(C, D_RES, &d_res, n));
+  SCK(dev_slot(C, D_USED, &d_used, 1));
+  SCK(cudaMemcpyAsync(d_src, src, n * sizeof(GapSrc), cudaMemcpyHostToDevice, s));
+  if (nf > 0) SCK(cudaMemcpyAsync(d_fslot, fslot, nf * sizeof(gdp_rec_t *), cudaMemcpyHostToDevice, s));
+  SCK(cudaMemsetAsync(d_used, 0, sizeof(unsigned long long), s));
+  const int cblocks = (int) std::min<int64_t>((n + 256) / 256, (int64_t) v.nsm * 8);
+  single_count_kernel<<<cblocks, 256, 0, s>>>(d_src, n, d_sout, d_fres, d_count);
+  gdpi_count_launch(ctx);
+  SCK(cudaGetLastError());
+  size_t tmp_bytes = 0;
+  SCK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_count, d_off, n + 1, s));
+  char *d_tmp = nullptr;
+  SCK(dev_slot(C, D_TMP, &d_tmp, (int64_t) tmp_bytes));
+  SCK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_count, d_off, n + 1, s));
+  /* the records end where the scan does, or earlier when max_recs cuts them */
+  SCK(cudaMemcpyAsync(&words[0], d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SCK(cudaStreamSynchronize(s));
+  SCK(dev_slot(C, D_OUT, &d_out, std::min(words[0], max_recs)));
+  const int gblocks = (int) std::min<int64_t>((n + 7) / 8, (int64_t) v.nsm * 8);
+  single_gather_kernel<<<gblocks, 256, 0, s>>>(d_src, n, d_off, max_recs, d_sout, d_srecs, d_soff, d_fres, d_fslot,
+                                                d_res, d_out, d_used);
+  gdpi_count_launch(ctx);
+  SCK(cudaGetLastError());
+  SCK(cudaMemcpyAsync(results, d_res, n * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s));
+  SCK(cudaMemcpyAsync(&words[1], d_used, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SCK(cudaStreamSynchronize(s));
+  const int64_t used = words[1];
+  if (used > 0) {
+    SCK(cudaMemcpyAsync(recs, d_out, used * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, s));
+    SCK(cudaStreamSynchronize(s));
   }
   if (nrecs_used) *nrecs_used = used;
   return GDP_OK;
