@@ -135,6 +135,12 @@ def load(path=LIB_PATH):
     lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
     lib.gdp_single_setup.argtypes = [vp, i32, i32, i32, i32]
     lib.gdp_single_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_gap_queue_create.argtypes = [i32, i32, i64, i64, vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+    lib.gdp_gap_queue_setup.argtypes = [vp, i32, i32, i32, i32]
+    lib.gdp_gap_queue_align.argtypes = [vp, vp, vp, vp, vp, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_gap_queue_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    lib.gdp_gap_queue_destroy.argtypes = [vp]
+    lib.gdp_gap_queue_destroy.restype = None
     return lib
 
 
@@ -437,3 +443,52 @@ class Server:
                                   ctypes.byref(busy))
         return {"batches": b.value, "pairs": p.value, "max_batch_pairs": m.value,
                 "peak_reserved_bytes": pk.value, "busy_s": busy.value}
+
+
+class GapQueue:
+    """gdp_gap_queue: Dynprog_single_gap calls from many threads, aligned together."""
+
+    def __init__(self, lib, blocks, altblocks=None, length=None, device=0, mode=0, max_batch=0, max_wait_us=200):
+        self.lib = lib
+        self.h = ctypes.c_void_p()
+        if length is None:
+            length = blocks.size // 3 * 32
+        self._keep = (blocks, altblocks)
+        rc = lib.gdp_gap_queue_create(device, mode, max_batch, max_wait_us, _ptr(blocks), _ptr(altblocks), length,
+                                      ctypes.byref(self.h))
+        if rc != 0:
+            raise RuntimeError(f"gdp_gap_queue_create: {STATUS.get(rc, rc)}")
+
+    def setup(self, user_open=0, user_extend=0, user_dynprog_p=False, homopolymerp=False):
+        return self.lib.gdp_gap_queue_setup(self.h, user_open, user_extend, int(user_dynprog_p), int(homopolymerp))
+
+    def align(self, gap, rsequence, rsequenceuc):
+        """One gap (a SINGLE_GAP_DTYPE record; rseq offsets ignored) with its
+        query strings (uint8 arrays); blocks until done."""
+        g = np.array(gap, dtype=SINGLE_GAP_DTYPE).reshape(1)
+        res = np.zeros(1, dtype=RESULT_DTYPE)
+        path = np.zeros(1, dtype=np.int8)
+        cap = max(int(g["rlength"][0]), 0) + max(int(g["glength"][0]), 0) + 2
+        recs = np.zeros(cap, dtype=REC_DTYPE)
+        n = ctypes.c_int64(0)
+        rc = self.lib.gdp_gap_queue_align(self.h, _ptr(g), _ptr(rsequence), _ptr(rsequenceuc), _ptr(res),
+                                          _ptr(path), _ptr(recs), cap, ctypes.byref(n))
+        if rc != 0:
+            raise RuntimeError(f"gdp_gap_queue_align: {STATUS.get(rc, rc)}")
+        return res[0], int(path[0]), recs[:n.value]
+
+    def stats(self):
+        b, g, m = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        self.lib.gdp_gap_queue_stats(self.h, ctypes.byref(b), ctypes.byref(g), ctypes.byref(m))
+        return {"batches": b.value, "gaps": g.value, "max_batch": m.value}
+
+    def close(self):
+        if self.h:
+            self.lib.gdp_gap_queue_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -434,6 +434,32 @@ int gdp_single_gap_batch(gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t nga
                          int64_t arena_bytes, gdp_result_t *results, int8_t *path, gdp_rec_t *recs,
                          int64_t max_recs, int64_t *nrecs_used);
 
+/*
+ * Stage-3 batching adapter.  GMAP's stage 3 calls Dynprog_single_gap once
+ * per gap from each worker thread (src/stage3.c:9117).  A gap queue keeps
+ * that call shape -- one gap, its rsequence / rsequenceuc by pointer, a
+ * blocking call -- and aligns the gaps of all calling threads together: a
+ * worker thread owning a context on `device` (tables of `mode`, the genome
+ * resident) runs every waiting gap (up to max_batch, 0: 4,096) as one
+ * gdp_single_gap_batch once max_batch gaps wait or the oldest has waited
+ * max_wait_us.  gdp_gap_queue_align ignores gap->rseq / rseq_uc, returns
+ * when the gap is done, with its result (rec_offset 0), path and records
+ * (GDP_ERR_RECS when more than max_recs), and the batch call's return code.
+ * Results do not depend on the batching.  gdp_gap_queue_setup is
+ * Dynprog_single_setup and must come before the first gdp_gap_queue_align;
+ * gdp_gap_queue_destroy must come after the last one has returned.
+ */
+typedef struct gdp_gap_queue gdp_gap_queue;
+int gdp_gap_queue_create(int device, int mode, int64_t max_batch, int64_t max_wait_us,
+                         const uint32_t *genome_blocks, const uint32_t *alt_blocks, uint64_t genome_length,
+                         gdp_gap_queue **queue);
+int gdp_gap_queue_setup(gdp_gap_queue *queue, int user_open, int user_extend, int user_dynprog_p, int homopolymerp);
+int gdp_gap_queue_align(gdp_gap_queue *queue, const gdp_single_gap_t *gap, const char *rsequence,
+                        const char *rsequenceuc, gdp_result_t *result, int8_t *path, gdp_rec_t *recs,
+                        int64_t max_recs, int64_t *nrecs);
+int gdp_gap_queue_stats(gdp_gap_queue *queue, int64_t *batches, int64_t *gaps, int64_t *max_batch);
+void gdp_gap_queue_destroy(gdp_gap_queue *queue);
+
 /* Kernel launches issued by the context since creation (one per kernel). */
 int64_t gdp_launch_count(gdp_ctx *ctx);
 

@@ -9,7 +9,12 @@
 * GPU: gdp_single_gap_batch equals the reference's Dynprog_single_gap on
   the same gaps, with and without an alternate genome and with user
   penalties (Dynprog_single_setup).
+* GPU: the stage-3 batching adapter (gdp_gap_queue) called one gap at a
+  time from eight threads gives each gap the result and records of the
+  batch call, and batches the threads' gaps together.
 """
+import threading
+
 import numpy as np
 import pytest
 
@@ -124,3 +129,46 @@ def test_single_gap_batch_user_penalties(gdplib, reference, ref_single, genome):
     st_d = np.stack([res["tb_score"], res["nmatches"], res["nmismatches"], res["nopens"], res["nindels"],
                      res["nrecs"], (res["nrecs"] == 0).astype(np.int32), st_r[:, 7]], axis=1)
     _check_same(st_r, off_r, rec_r, st_d, res["rec_offset"], recs, "device, user penalties")
+
+
+@pytest.mark.gpu
+def test_gap_queue_from_threads_equals_batch(gdplib, genome):
+    g, alt, blocks, altblocks = genome
+    gaps, arena = single_cases.single_gap_cases(31, 1600, g, 500, 2000)
+    ctx = gdp.Context(gdplib)
+    try:
+        ctx.set_genome(blocks, altblocks, GENOME_LEN)
+        res_b, path_b, recs_b = ctx.single_gaps(gaps, arena)
+    finally:
+        ctx.close()
+    q = gdp.GapQueue(gdplib, blocks, altblocks, GENOME_LEN, max_batch=256, max_wait_us=500)
+    out = [None] * gaps.size
+    errors = []
+
+    def worker(t):
+        try:
+            for i in range(t, gaps.size, 8):
+                x = gaps[i]
+                rl = max(int(x["rlength"]), 0)
+                rs = np.ascontiguousarray(arena[int(x["rseq"]):int(x["rseq"]) + rl])
+                ru = np.ascontiguousarray(arena[int(x["rseq_uc"]):int(x["rseq_uc"]) + rl])
+                out[i] = q.align(x, rs, ru)
+        except Exception as e:   # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    stats = q.stats()
+    q.close()
+    assert not errors, errors
+    keys = ("status", "score", "precision", "tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs")
+    for i in range(gaps.size):
+        r, p, recs = out[i]
+        assert all(r[k] == res_b[i][k] for k in keys), (i, r, res_b[i])
+        assert p == path_b[i]
+        o = int(res_b["rec_offset"][i])
+        assert np.array_equal(recs, recs_b[o:o + int(res_b["nrecs"][i])]), i
+    assert stats["gaps"] == gaps.size and stats["batches"] < gaps.size and stats["max_batch"] > 1
