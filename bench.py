@@ -397,7 +397,7 @@ def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=20000):
            "timing": "host gaps and sequences to host records (gdp_single_gap_batch, pinned host "
                      "buffers), median of 3 after one warm-up, CUDA events on the context stream"}
     import oracle
-    if oracle.reference_available():
+    if cpu_gaps > 0 and oracle.reference_available():
         ref = oracle.reference()
         ref.init(0)
         ref.set_genome(blocks, None, genome.size)
