@@ -28,6 +28,7 @@
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include "gdp.h"
 #include "gdp_internal.h"
@@ -202,7 +203,7 @@ single_gather_kernel (const GapSrc *src, int64_t n, const int64_t *off, int64_t 
 /* The context's grow-only working buffers: device slot k, pinned host slot k. */
 enum { D_ARENA, D_CAND, D_SOFF, D_SOUT, D_SRECS, D_FILL, D_FRES, D_SLOTS, D_SRC, D_COUNT, D_OFF, D_FSLOT, D_RES,
        D_OUT, D_USED, D_TMP };
-enum { H_CAND, H_SOFF, H_SOUT, H_FILL, H_SRC, H_FSLOT, H_WORDS };
+enum { H_CAND, H_SOFF, H_SOUT, H_FILL, H_FSEG, H_SRC, H_FSLOT, H_WORDS };
 
 template <class T> cudaError_t
 dev_slot (gdpi_single_cfg *c, int k, T **p, int64_t count) {
@@ -234,6 +235,21 @@ host_slot (gdpi_single_cfg *c, int k, T **p, int64_t count) {
   }
   *p = (T *) c->hbuf[k];
   return cudaSuccess;
+}
+
+/* f(lo, hi) over [0, n) on up to 16 host threads (one below 8,192 items). */
+template <class F> void
+par_for (int64_t n, F f) {
+  const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = (int) std::min<int64_t>(std::min<int64_t>(hw, 16), std::max<int64_t>(1, n / 8192));
+  if (nt <= 1) { f((int64_t) 0, n); return; }
+  std::vector<std::thread> th;
+  const int64_t chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const int64_t lo = t * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi) th.emplace_back([=, &f] { f(lo, hi); });
+  }
+  for (auto &x : th) x.join();
 }
 
 /* The reference's choices for one gap (src/dynprog_single.c:453-481, :612-617). */
@@ -300,6 +316,28 @@ base_pair (const gdp_single_gap_t &g) {
   return p;
 }
 
+gdp_pair_t
+fill_pair (const gdp_single_gap_t &g, const gdpi_single_cfg &cfg, int64_t seg, bool has_alt) {
+  const GapSetup st = gap_setup(g, cfg);
+  gdp_pair_t p = base_pair(g);
+  p.lband = st.lband; p.uband = st.uband;
+  p.precision = (int8_t) st.precision;
+  p.mismatchtype = (int8_t) st.mismatchtype;
+  p.open = (int16_t) st.open; p.extend = (int16_t) st.extend;
+  p.flags = GDP_FLAG_TRACEBACK | GDP_FLAG_GWINDOW | (g.jump_late_p ? GDP_FLAG_JUMP_LATE : 0);
+  p.gseq = seg;
+  p.gseq_alt = has_alt ? seg + g.glength : seg;
+  return p;
+}
+
+/* An upper bound of a fill's direction words: (rlength / W + 1) blocks of
+   at most W + lband + uband swept columns, W / 8 words each. */
+int64_t
+words_bound (const gdp_pair_t &p) {
+  const int W = p.precision == 8 ? 32 : 16;
+  return ((int64_t) p.rlength / W + 1) * ((int64_t) W + p.lband + p.uband) * (W / 8);
+}
+
 }  // namespace
 
 #define SCK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return gdpi_fail(ctx, #call, e_); } while (0)
@@ -330,53 +368,73 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
   cudaStream_t s = v.stream;
 
   /* host decisions: NULL paths, simple candidates, fills */
-  std::vector<int8_t> kind((size_t) n, GDP_SINGLE_NULL);
+  std::vector<int8_t> kind((size_t) n), cls((size_t) n);   /* cls: 0 no fill, 1 diagonal candidate, 2 fill */
+  par_for(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; i++) {
+      const gdp_single_gap_t &g = gaps[i];
+      gdp_result_t &r = results[i];
+      memset(&r, 0, sizeof(r));
+      kind[i] = GDP_SINGLE_NULL;
+      cls[i] = 0;
+      if (g.rlength <= 0 || g.glength <= 0 || g.rlength > g.max_rlength || g.glength > g.max_glength) {
+        r.tb_score = NEG_INFINITY_32;
+      } else if (g.rseq < 0 || g.rseq + g.rlength > arena_bytes || g.rseq_uc < 0 ||
+                 g.rseq_uc + g.rlength > arena_bytes) {
+        r.status = GDP_ERR_LEN;
+      } else if (g.genestrand < 0 || g.genestrand > 2) {
+        r.status = GDP_ERR_PARAM;
+      } else if (!segment_resident(g, v.genome_len)) {
+        r.status = GDP_ERR_NOGENOME;
+      } else {
+        kind[i] = GDP_SINGLE_DP;
+        cls[i] = (g.glength == g.rlength) ? 1 : 2;
+      }
+    }
+  });
   std::vector<int64_t> cand, fill;
+  std::vector<int32_t> where((size_t) n, -1);   /* a gap's candidate or fill index */
+  int64_t seg_bytes = 0;
   for (int64_t i = 0; i < n; i++) {
-    const gdp_single_gap_t &g = gaps[i];
-    gdp_result_t &r = results[i];
-    memset(&r, 0, sizeof(r));
-    if (g.rlength <= 0 || g.glength <= 0 || g.rlength > g.max_rlength || g.glength > g.max_glength) {
-      r.tb_score = NEG_INFINITY_32;
-      continue;
-    }
-    if (g.rseq < 0 || g.rseq + g.rlength > arena_bytes || g.rseq_uc < 0 || g.rseq_uc + g.rlength > arena_bytes) {
-      r.status = GDP_ERR_LEN;
-      continue;
-    }
-    if (g.genestrand < 0 || g.genestrand > 2) { r.status = GDP_ERR_PARAM; continue; }
-    if (!segment_resident(g, v.genome_len)) { r.status = GDP_ERR_NOGENOME; continue; }
-    kind[i] = GDP_SINGLE_DP;
-    if (g.glength == g.rlength) cand.push_back(i); else fill.push_back(i);
+    if (cls[i] == 1) { where[i] = (int32_t) cand.size(); cand.push_back(i); }
+    else if (cls[i] == 2) { where[i] = (int32_t) fill.size(); fill.push_back(i); }
+    if (cls[i] != 0) seg_bytes += (int64_t) gaps[i].glength * (v.has_alt ? 2 : 1);
   }
 
   gdpi_single_cfg *C = v.single;
   /* the arena, followed by the segments of the gaps that may need a fill */
   const int64_t seg_base = (arena_bytes + 15) / 16 * 16;
-  int64_t seg_bytes = 0;
-  for (int64_t i = 0; i < n; i++)
-    if (kind[i] == GDP_SINGLE_DP) seg_bytes += (int64_t) gaps[i].glength * (v.has_alt ? 2 : 1);
   char *d_arena = nullptr;
   SCK(dev_slot(C, D_ARENA, &d_arena, seg_base + seg_bytes));
   if (arena_bytes > 0) SCK(cudaMemcpyAsync(d_arena, arena, arena_bytes, cudaMemcpyHostToDevice, s));
 
-  /* phase 1: the ungapped diagonal of the equal-length gaps */
+  /* fill descriptors: the gaps that are not candidates first; the
+     candidates whose diagonal does not hold join after phase 1 */
   const int64_t nc = (int64_t) cand.size();
+  const int64_t nf_max = (int64_t) fill.size() + nc;
+  gdp_pair_t *fp = nullptr;
+  int64_t *fseg = nullptr;
+  SCK(host_slot(C, H_FILL, &fp, nf_max));
+  SCK(host_slot(C, H_FSEG, &fseg, nf_max + 1));
+  const int64_t mult = v.has_alt ? 2 : 1;
+  fseg[0] = seg_base;
+  for (size_t k = 0; k < fill.size(); k++) fseg[k + 1] = fseg[k] + gaps[fill[k]].glength * mult;
+
+  /* phase 1: the ungapped diagonal of the equal-length gaps */
   gdp_rec_t *d_srecs = nullptr;
   int64_t *d_soff = nullptr;
   SimpleOut *d_sout = nullptr;
+  SimpleOut *sout = nullptr;
   if (nc > 0) {
     gdp_pair_t *cp = nullptr, *d_cp = nullptr;
     int64_t *soff = nullptr;
-    SimpleOut *sout = nullptr;
     SCK(host_slot(C, H_CAND, &cp, nc));
     SCK(host_slot(C, H_SOFF, &soff, nc + 1));
     SCK(host_slot(C, H_SOUT, &sout, nc));
     soff[0] = 0;
-    for (int64_t k = 0; k < nc; k++) {
-      cp[k] = base_pair(gaps[cand[k]]);
-      soff[k + 1] = soff[k] + gaps[cand[k]].rlength;
-    }
+    for (int64_t k = 0; k < nc; k++) soff[k + 1] = soff[k] + gaps[cand[k]].rlength;
+    par_for(nc, [&](int64_t lo, int64_t hi) {
+      for (int64_t k = lo; k < hi; k++) cp[k] = base_pair(gaps[cand[k]]);
+    });
     SCK(dev_slot(C, D_CAND, &d_cp, nc));
     SCK(dev_slot(C, D_SOFF, &d_soff, nc));
     SCK(dev_slot(C, D_SOUT, &d_sout, nc));
@@ -389,40 +447,38 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
     gdpi_count_launch(ctx);
     SCK(cudaGetLastError());
     SCK(cudaMemcpyAsync(sout, d_sout, nc * sizeof(SimpleOut), cudaMemcpyDeviceToHost, s));
+  }
+  /* while the diagonal runs: the other fills' descriptors */
+  par_for((int64_t) fill.size(), [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; k++) fp[k] = fill_pair(gaps[fill[k]], *C, fseg[k], v.has_alt);
+  });
+  if (nc > 0) {
     SCK(cudaStreamSynchronize(s));
     for (int64_t k = 0; k < nc; k++) {
-      if (sout[k].simple) kind[cand[k]] = GDP_SINGLE_SIMPLE;
-      else fill.push_back(cand[k]);
+      const int64_t i = cand[k];
+      if (sout[k].simple) {
+        kind[i] = GDP_SINGLE_SIMPLE;
+      } else {
+        const int64_t f = (int64_t) fill.size();
+        fp[f] = fill_pair(gaps[i], *C, fseg[f], v.has_alt);
+        fseg[f + 1] = fseg[f] + gaps[i].glength * mult;
+        where[i] = (int32_t) f;
+        fill.push_back(i);
+      }
     }
-    std::sort(fill.begin(), fill.end());
   }
 
-  /* phase 2: fills and tracebacks of the rest, in plans within the budget */
+  /* phase 2: fills and tracebacks, in plans within the budget */
   const int64_t nf = (int64_t) fill.size();
-  gdp_pair_t *fp = nullptr, *d_fp = nullptr;
+  gdp_pair_t *d_fp = nullptr;
   gdp_result_t *d_fres = nullptr;
   gdp_rec_t *d_slots = nullptr;
   const gdp_rec_t **fslot = nullptr, **d_fslot = nullptr;
-  SCK(host_slot(C, H_FILL, &fp, nf));
   SCK(host_slot(C, H_FSLOT, &fslot, nf));
-  int64_t slot_total = 0;   /* record slots of all fills: rlength + glength + 2 each */
-  {
-    int64_t seg = seg_base;
-    for (int64_t k = 0; k < nf; k++) {
-      const gdp_single_gap_t &g = gaps[fill[k]];
-      const GapSetup st = gap_setup(g, *C);
-      gdp_pair_t p = base_pair(g);
-      p.lband = st.lband; p.uband = st.uband;
-      p.precision = (int8_t) st.precision;
-      p.mismatchtype = (int8_t) st.mismatchtype;
-      p.open = (int16_t) st.open; p.extend = (int16_t) st.extend;
-      p.flags = GDP_FLAG_TRACEBACK | GDP_FLAG_GWINDOW | (g.jump_late_p ? GDP_FLAG_JUMP_LATE : 0);
-      p.gseq = seg;
-      p.gseq_alt = v.has_alt ? seg + g.glength : seg;
-      seg += (int64_t) g.glength * (v.has_alt ? 2 : 1);
-      fp[k] = p;
-      slot_total += (int64_t) g.rlength + g.glength + 2;
-    }
+  int64_t slot_total = 0, bound = 0;   /* record slots (rlength + glength + 2 each), direction words */
+  for (int64_t k = 0; k < nf; k++) {
+    slot_total += (int64_t) fp[k].rlength + fp[k].glength + 2;
+    bound += words_bound(fp[k]);
   }
   SCK(dev_slot(C, D_FILL, &d_fp, nf));
   SCK(dev_slot(C, D_FRES, &d_fres, nf));
@@ -431,12 +487,14 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
   int64_t slot_used = 0;
   for (int64_t k0 = 0; k0 < nf;) {
     /* one plan: gaps k0..k1 while their direction bytes stay in the budget */
-    int64_t k1 = k0, bytes = 0;
-    while (k1 < nf) {
-      const int64_t b = gdp_pair_words(&fp[k1], fp[k1].precision == 8 ? 32 : 16) * 4;
-      if (k1 > k0 && bytes + b > v.budget) break;
-      bytes += b;
-      k1++;
+    int64_t k1 = nf;
+    if (bound * 4 > v.budget) {
+      int64_t bytes = 0;
+      for (k1 = k0; k1 < nf; k1++) {
+        const int64_t b = gdp_pair_words(&fp[k1], fp[k1].precision == 8 ? 32 : 16) * 4;
+        if (k1 > k0 && bytes + b > v.budget) break;
+        bytes += b;
+      }
     }
     int rc = gdpi_plan_reuse(ctx, &C->plan, fp + k0, k1 - k0);
     if (rc != GDP_OK) return rc;
@@ -453,23 +511,18 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
   /* results and records in gap order, on the device */
   GapSrc *src = nullptr, *d_src = nullptr;
   SCK(host_slot(C, H_SRC, &src, n));
-  {
-    int64_t ci = 0, fi = 0;
-    for (int64_t i = 0; i < n; i++) {
+  par_for(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; i++) {
       GapSrc g{SRC_NULL, 0};
       if (kind[i] == GDP_SINGLE_NULL) {
         if (results[i].status != GDP_OK) g = GapSrc{SRC_ERROR, results[i].status};
-      } else if (kind[i] == GDP_SINGLE_SIMPLE) {
-        while (cand[ci] < i) ci++;
-        g = GapSrc{SRC_SIMPLE, (int32_t) ci};
       } else {
-        while (fill[fi] < i) fi++;
-        g = GapSrc{SRC_FILL, (int32_t) fi};
+        g = GapSrc{kind[i] == GDP_SINGLE_SIMPLE ? SRC_SIMPLE : SRC_FILL, where[i]};
       }
       src[i] = g;
       if (path) path[i] = kind[i];
     }
-  }
+  });
   int64_t *d_count = nullptr, *d_off = nullptr, *words = nullptr;
   gdp_result_t *d_res = nullptr;
   gdp_rec_t *d_out = nullptr;
