@@ -152,8 +152,9 @@ single_count_kernel (const GapSrc *src, int64_t n, const SimpleOut *sout, const 
 
 /*
  * Final results and records in gap order, one warp per gap: the gap's
- * records go to out[off[i] ..) (gaps whose records would pass max_recs get
- * GDP_ERR_RECS and none), and *used gets the end of the records written.
+ * records go to out[off[i] ..) (a gap with records that would pass
+ * max_recs gets GDP_ERR_RECS and none), and *used gets the end of the
+ * records written.
  */
 __global__ void __launch_bounds__(256)
 single_gather_kernel (const GapSrc *src, int64_t n, const int64_t *off, int64_t max_recs, const SimpleOut *sout,
@@ -183,7 +184,7 @@ single_gather_kernel (const GapSrc *src, int64_t n, const int64_t *off, int64_t 
       from = fslots[g.idx] + r.rec_offset;
     }
     const int64_t o = off[i];
-    if (o + cnt > max_recs) {
+    if (cnt > 0 && o + cnt > max_recs) {
       r.status = GDP_ERR_RECS;
       cnt = 0;
     }

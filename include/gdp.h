@@ -406,8 +406,9 @@ void gdp_server_destroy(gdp_server *server);
  * of the List the reference returns, head first (the DP path's push order
  * after its List_reverse; the simple path from its last query position
  * down).  path[i] (may be NULL) gets the path taken.  The caller advances
- * its dynprogindex by one per gap, as the reference does.  Records that do
- * not fit into max_recs: that gap and every later one get GDP_ERR_RECS.
+ * its dynprogindex by one per gap, as the reference does.  When the
+ * records do not fit into max_recs, the first gap whose records pass it and
+ * every later gap with records get GDP_ERR_RECS (and no records).
  * The context keeps the call's working memory for the next call, so calls
  * on one context must not overlap (one context per thread, or the gap
  * queue below).

@@ -172,3 +172,31 @@ def test_gap_queue_from_threads_equals_batch(gdplib, genome):
         o = int(res_b["rec_offset"][i])
         assert np.array_equal(recs, recs_b[o:o + int(res_b["nrecs"][i])]), i
     assert stats["gaps"] == gaps.size and stats["batches"] < gaps.size and stats["max_batch"] > 1
+
+
+@pytest.mark.gpu
+def test_single_gap_record_cut_and_empty_batch(gdplib, genome):
+    g, alt, blocks, altblocks = genome
+    gaps, arena = single_cases.single_gap_cases(41, 300, g, 500, 2000)
+    ctx = gdp.Context(gdplib)
+    try:
+        ctx.set_genome(blocks, None, GENOME_LEN)
+        full, path, recs = ctx.single_gaps(gaps, arena)
+        cut = int(recs.size // 2)
+        part, path2, recs2 = ctx.single_gaps(gaps, arena, max_recs=cut)
+        empty = ctx.single_gaps(gaps[:0], arena)
+    finally:
+        ctx.close()
+    assert np.array_equal(path, path2)
+    ends = full["rec_offset"] + full["nrecs"]
+    fits = ends <= cut
+    first_out = int(np.argmin(fits)) if not fits.all() else gaps.size
+    assert fits[:first_out].all() and not fits[first_out:].any()
+    keys = ("status", "tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs", "rec_offset")
+    assert all(np.array_equal(part[k][:first_out], full[k][:first_out]) for k in keys)
+    late = np.arange(gaps.size) >= first_out
+    had = late & (full["nrecs"] > 0)
+    assert (part["status"][had] == 7).all() and (part["nrecs"][late] == 0).all()   # GDP_ERR_RECS
+    assert np.array_equal(part["status"][late & ~had], full["status"][late & ~had])
+    assert np.array_equal(recs2, recs[:recs2.size]) and recs2.size <= cut
+    assert empty[0].size == 0 and empty[2].size == 0
