@@ -1,5 +1,8 @@
 """Dynprog_single_gap over a batch (gdp_single_gap_batch).
 
+* CPU: the committed golden vectors of the reference's Dynprog_single_gap
+  (tests/golden/single_gap.npz) are reproduced by the restatement, and by
+  the reference library itself.
 * CPU: the restated single gap (oracle.single_gap_restated: the host
   decisions and single_gap_simple in Python, the fill and traceback of the
   C restatement) equals the reference's own Dynprog_single_gap
@@ -13,6 +16,7 @@
   time from eight threads gives each gap the result and records of the
   batch call, and batches the threads' gaps together.
 """
+import os
 import threading
 
 import numpy as np
@@ -48,6 +52,32 @@ def _check_same(stats_a, off_a, recs_a, stats_b, off_b, recs_b, what):
         a = recs_a[int(off_a[i]):int(off_a[i]) + k]
         b = recs_b[int(off_b[i]):int(off_b[i]) + k]
         assert np.array_equal(a, b), f"{what}: records of gap {i} differ"
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "single_gap.npz")
+
+
+def _golden():
+    z = np.load(GOLDEN)
+    return {k: z[k] for k in z.files}
+
+
+def test_restatement_matches_golden(restatement):
+    """The restated single gap reproduces the committed golden vectors of the
+    reference's Dynprog_single_gap (tests/golden/make_golden_single.py)."""
+    z = _golden()
+    restatement.set_genome(z["genome_blocks"], z["genome_alt_blocks"], z["genome"].size)
+    st, off, recs = oracle.single_gap_restated(restatement, z["gaps"], z["arena"], z["genome"], z["genome_alt"])
+    _check_same(z["stats"], z["rec_offset"], z["recs"], st, off, recs, "golden")
+
+
+def test_reference_matches_golden(reference, ref_single):
+    z = _golden()
+    reference.set_genome(z["genome_blocks"], z["genome_alt_blocks"], z["genome"].size)
+    ref_single.setup()
+    st, off, recs = ref_single.run(z["gaps"], z["arena"])
+    _check_same(z["stats"], z["rec_offset"], z["recs"], st, off, recs, "reference vs golden")
+    assert np.array_equal(st[:, 7], z["stats"][:, 7])
 
 
 def test_restatement_matches_reference(reference, restatement, ref_single, genome):
