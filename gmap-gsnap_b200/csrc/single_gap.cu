@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -364,6 +365,7 @@ gdp_single_gap_batch (gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t n, con
       arena_bytes < 0 || (arena_bytes > 0 && arena == nullptr) || max_recs < 0 || (max_recs > 0 && recs == nullptr))
     return GDP_ERR_PARAM;
   if (nrecs_used) *nrecs_used = 0;
+  if (n > INT32_MAX) return GDP_ERR_LEN;   /* gap indices are 32-bit on the device */
   if (n == 0) return GDP_OK;
   SCK(cudaSetDevice(v.device));
   cudaStream_t s = v.stream;
