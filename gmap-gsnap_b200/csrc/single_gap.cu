@@ -54,10 +54,11 @@ struct SimpleOut {
  * genomeoffset + q).  A '*' genome character (past the chromosome) pushes
  * nothing and scores nothing; an exact match against the genome or the
  * alternate genome scores MATCH ('*'), a consistent pair
- * (Dynprog_consistent_p) MATCH (':'), anything else MISMATCH (' ').  The path is taken when at most one position mismatched
- * and at least one pair was pushed (Pairpool_push drops negative
- * positions).  Records are written head first: the reference pushes from
- * the first position, so its List starts at the last one.
+ * (Dynprog_consistent_p) MATCH (':'), anything else MISMATCH (' ').  The
+ * path is taken when at most one position mismatched and at least one pair
+ * was pushed (Pairpool_push drops negative positions).  Records are written
+ * head first: the reference pushes from the first position, so its List
+ * starts at the last one.
  */
 __device__ __forceinline__ int
 simple_class (const gdp_pair_t &p, const char *ruc, int q, const uint32_t *genome, const uint32_t *genomealt,
