@@ -23,11 +23,17 @@
  *
  * The first call on a device does the set-up: it takes the device
  * addresses of both arrays with cudaGetSymbolAddress (a host-side symbol
- * name is not a device address) and uploads the tables.  That first call
- * should therefore come before any stream capture.  Every call shares the
- * same scratch array and leaves its contents behind.  Calls that overlap on
- * the GPU (on different streams, or from different threads on one device)
- * race on it, so a caller must order its calls.
+ * name is not a device address), uploads the tables and waits for the
+ * upload to land.  That first call should therefore come before any stream
+ * capture.  Every call shares the same scratch array and leaves its
+ * contents behind.  Calls that overlap on the GPU (on different streams, or
+ * from different threads on one device) race on it, so a caller must order
+ * its calls.
+ *
+ * The call leaves the calling thread's current device as it found it, and
+ * checks its own launches by their return codes, so a CUDA error left
+ * pending by the caller's earlier work neither fails this call nor is
+ * cleared by it.
  */
 #include <cuda_runtime.h>
 #include <mutex>
@@ -70,7 +76,7 @@ static gdp_tables_t g_host_tables;   /* host staging for the one-time upload */
  * walked in chunks with a block-wide scan of their direction words.
  */
 __global__ void __launch_bounds__(1024)
-noalloc_prep_kernel (const gdp_pair_t *pairs, int64_t n, int64_t cap, gdp_result_t *res,
+noalloc_prep_kernel (const gdp_pair_t *pairs, int64_t n, int64_t arena_bytes, int64_t cap, gdp_result_t *res,
                      gdp_meta_t *meta, int32_t *list_late, int32_t *list_early, int32_t *counts) {
   __shared__ int64_t s_words[1024];
   __shared__ int64_t s_base;
@@ -83,11 +89,19 @@ noalloc_prep_kernel (const gdp_pair_t *pairs, int64_t n, int64_t cap, gdp_result
     gdp_pair_t p;
     if (i < n) {
       p = pairs[i];
+      /* the fill reads rsequence, gsequence and gsequence_alt from the
+         caller's arena: each must lie inside it before any read */
+      const bool in_arena = p.rseq >= 0 && p.rseq + p.rlength <= arena_bytes && p.gseq >= 0 &&
+                            p.gseq + p.glength <= arena_bytes && p.gseq_alt >= 0 &&
+                            p.gseq_alt + p.glength <= arena_bytes;
       if (p.variant != GDP_FULL || p.precision != 16 || p.mismatchtype < 0 || p.mismatchtype > 3 ||
-          p.open < -127 || p.open > 0 || p.extend < -127 || p.extend > 0) {
+          p.open < -127 || p.open > 0 || p.extend < -127 || p.extend > 0 ||
+          (p.flags & ~(GDP_FLAG_JUMP_LATE | GDP_FLAG_REVP)) != 0 || p.genestrand < 0 || p.genestrand > 2 ||
+          (p.xflags & ~GDP_XFLAG_SEGMENT) != 0) {
+        /* no traceback, rerun, genome window or endpoint search here */
         st = GDP_ERR_PARAM;
       } else if (p.rlength <= 0 || p.glength <= 0 || p.glength >= GDP_NOALLOC_MAX_COLS ||
-                 p.rlength > (1 << 20)) {
+                 p.rlength > (1 << 20) || !in_arena) {
         st = GDP_ERR_LEN;
       } else if (p.lband < 0 || p.uband < 0) {
         st = GDP_ERR_BAND;
@@ -145,6 +159,9 @@ noalloc_setup (int device, int mode, unsigned char **scratch, gdp_tables_t **tab
     gdp_build_tables(&g_host_tables, mode);
     if (cudaMemcpyToSymbol(g_noalloc_tables, &g_host_tables, sizeof(gdp_tables_t)) != cudaSuccess)
       return GDP_ERR_CUDA;
+    /* from pageable memory the copy may return before the DMA lands; a
+       caller's non-blocking stream would not wait for it */
+    if (cudaDeviceSynchronize() != cudaSuccess) return GDP_ERR_CUDA;
     g_scratch_dev[device] = (unsigned char *) ps;
     g_tables_dev[device] = (gdp_tables_t *) pt;
     g_tables_mode[device] = mode;
@@ -157,18 +174,15 @@ noalloc_setup (int device, int mode, unsigned char **scratch, gdp_tables_t **tab
   return GDP_OK;
 }
 
-extern "C" int
-gdp_fill16_noalloc (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
-                    uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results, void *stream) {
-  if (npairs < 0 || npairs > GDP_NOALLOC_MAX_PAIRS) return GDP_ERR_LEN;
-  if (mode < 0 || mode > 6) return GDP_ERR_PARAM;
-  if (npairs == 0) return GDP_OK;
-  if (cudaSetDevice(device) != cudaSuccess) return GDP_ERR_CUDA;
+/* The launches of one call, on `device` (current). */
+static int
+noalloc_run (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
+             int64_t arena_bytes, uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results,
+             cudaStream_t s) {
   unsigned char *scratch = nullptr;
   gdp_tables_t *tables = nullptr;
   int rc = noalloc_setup(device, mode, &scratch, &tables);
   if (rc != GDP_OK) return rc;
-  cudaStream_t s = (cudaStream_t) stream;
   int2 *carry = (int2 *) scratch;
   gdp_meta_t *meta = (gdp_meta_t *) (scratch + NA_META_OFF);
   int32_t *list_late = (int32_t *) (scratch + NA_LIST_OFF);
@@ -176,9 +190,13 @@ gdp_fill16_noalloc (int device, int mode, const gdp_pair_t *d_pairs, int64_t npa
   int32_t *counts = (int32_t *) (scratch + NA_COUNT_OFF);
   /* the list counts must start at zero on every call */
   if (cudaMemsetAsync(counts, 0, 2 * sizeof(int32_t), s) != cudaSuccess) return GDP_ERR_CUDA;
-  noalloc_prep_kernel<<<1, 1024, 0, s>>>(d_pairs, npairs, dir_words_cap, d_results, meta, list_late,
-                                          list_early, counts);
-  if (cudaGetLastError() != cudaSuccess) return GDP_ERR_CUDA;
+  {
+    void *args[] = {(void *) &d_pairs, (void *) &npairs, (void *) &arena_bytes, (void *) &dir_words_cap,
+                    (void *) &d_results, (void *) &meta, (void *) &list_late, (void *) &list_early,
+                    (void *) &counts};
+    if (cudaLaunchKernel((const void *) noalloc_prep_kernel, dim3(1), dim3(1024), args, 0, s) != cudaSuccess)
+      return GDP_ERR_CUDA;
+  }
   FillParams P;
   P.pairs = d_pairs;
   P.arena = d_arena;
@@ -191,13 +209,30 @@ gdp_fill16_noalloc (int device, int mode, const gdp_pair_t *d_pairs, int64_t npa
   P.scratch_rows = GDP_NOALLOC_MAX_COLS;
   P.tab = tables;
   P.reach_from4 = 0;
-  P.list = list_late;
-  P.count = counts;
-  fill_thread_kernel<16, GDP_FULL, true, 0><<<GDP_NOALLOC_BLOCKS, GDP_NOALLOC_THREADS, 0, s>>>(P);
-  if (cudaGetLastError() != cudaSuccess) return GDP_ERR_CUDA;
-  P.list = list_early;
-  P.count = counts + 1;
-  fill_thread_kernel<16, GDP_FULL, false, 0><<<GDP_NOALLOC_BLOCKS, GDP_NOALLOC_THREADS, 0, s>>>(P);
-  if (cudaGetLastError() != cudaSuccess) return GDP_ERR_CUDA;
+  for (int late = 1; late >= 0; late--) {
+    P.list = late ? list_late : list_early;
+    P.count = counts + (late ? 0 : 1);
+    void *args[] = {(void *) &P};
+    const void *fn = late ? (const void *) fill_thread_kernel<16, GDP_FULL, true, 0>
+                          : (const void *) fill_thread_kernel<16, GDP_FULL, false, 0>;
+    if (cudaLaunchKernel(fn, dim3(GDP_NOALLOC_BLOCKS), dim3(GDP_NOALLOC_THREADS), args, 0, s) != cudaSuccess)
+      return GDP_ERR_CUDA;
+  }
   return GDP_OK;
+}
+
+extern "C" int
+gdp_fill16_noalloc (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
+                    int64_t arena_bytes, uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results,
+                    void *stream) {
+  if (npairs < 0 || npairs > GDP_NOALLOC_MAX_PAIRS) return GDP_ERR_LEN;
+  if (mode < 0 || mode > 6 || arena_bytes < 0) return GDP_ERR_PARAM;
+  if (npairs == 0) return GDP_OK;
+  int caller_device = -1;
+  if (cudaGetDevice(&caller_device) != cudaSuccess) return GDP_ERR_CUDA;
+  if (device != caller_device && cudaSetDevice(device) != cudaSuccess) return GDP_ERR_CUDA;
+  const int rc = noalloc_run(device, mode, d_pairs, npairs, d_arena, arena_bytes, d_dirs, dir_words_cap,
+                             d_results, (cudaStream_t) stream);
+  if (device != caller_device && cudaSetDevice(caller_device) != cudaSuccess) return GDP_ERR_CUDA;
+  return rc;
 }

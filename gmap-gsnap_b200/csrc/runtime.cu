@@ -1854,7 +1854,9 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
   cudaStream_t s = ctx->stream;
   DevBuf dpairs, dres;
   for (int k = 0; k < NSLOTS; k++) cudaEventSynchronize(ctx->slot[k].out_done);
-  if (rc == GDP_OK) rc = plan_upload(ctx, pl.h, pl.d, true, s);
+  /* without H the fills run exactly as in production: no score dump, so
+     the steady and half-width column bodies take their columns */
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl.h, pl.d, H != nullptr, s);
   if (rc == GDP_OK) {
     cudaError_t e = ctx->arena.ensure(std::max<int64_t>(arena_bytes, 16));
     if (e == cudaSuccess) e = dpairs.ensure(std::max<int64_t>(n, 1) * sizeof(gdp_pair_t));
@@ -1866,12 +1868,13 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
   if (rc == GDP_OK)
     rc = plan_run(ctx, pl.h, pl.d, dpairs.as<gdp_pair_t>(), ctx->arena.as<char>(), dres.as<gdp_result_t>(), nullptr);
   std::vector<uint32_t> words(std::max<int64_t>(pl.h.dir_words, 1));
-  std::vector<int16_t> hs(std::max<int64_t>(pl.h.dir_words, 1) * 8);
+  std::vector<int16_t> hs(H != nullptr ? std::max<int64_t>(pl.h.dir_words, 1) * 8 : 0);
   std::vector<gdp_meta_t> meta(std::max<int64_t>(n, 1));
   if (rc == GDP_OK) {
     cudaError_t e = cudaMemcpyAsync(results, dres.p, n * sizeof(gdp_result_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(words.data(), pl.d.dirs.p, pl.h.dir_words * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), pl.d.hdump.p, pl.h.dir_words * 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && H != nullptr)
+      e = cudaMemcpyAsync(hs.data(), pl.d.hdump.p, pl.h.dir_words * 16, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(meta.data(), pl.d.meta.p, n * sizeof(gdp_meta_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = set_err(ctx, "dump copy", e);

@@ -107,7 +107,7 @@ def load(path=LIB_PATH):
     lib.gdp_profile_reset.argtypes = [vp]
     lib.gdp_measure_int_peak.argtypes = [vp]
     lib.gdp_measure_int_peak.restype = ctypes.c_double
-    lib.gdp_fill16_noalloc.argtypes = [i32, i32, vp, i64, vp, vp, i64, vp, vp]
+    lib.gdp_fill16_noalloc.argtypes = [i32, i32, vp, i64, vp, i64, vp, i64, vp, vp]
     lib.gdp_fill_dump.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, vp, vp, vp]
     lib.gdp_launch_count.argtypes = [vp]
     lib.gdp_launch_count.restype = i64
@@ -363,13 +363,17 @@ class Context:
             raise RuntimeError(f"gdp_single_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
         return results, path, recs[:used.value]
 
-    def fill_dump(self, pairs, arena):
+    def fill_dump(self, pairs, arena, scores=True):
+        """Dense in-band scores and directions of every pair.  With
+        scores=False the fills run exactly as in production (no score
+        dump), H comes back None and the directions are decoded from the
+        production direction words."""
         n = pairs.size
         sizes = (pairs["glength"].astype(np.int64) + 1) * (pairs["rlength"].astype(np.int64) + 1)
         offs = np.zeros(n, dtype=np.int64)
         offs[1:] = np.cumsum(sizes)[:-1]
         total = int(sizes.sum())
-        H = np.zeros(total, dtype=np.int16)
+        H = np.zeros(total, dtype=np.int16) if scores else None
         dN = np.zeros(total, dtype=np.int8)
         dE = np.zeros(total, dtype=np.int8)
         dF = np.zeros(total, dtype=np.int8)

@@ -282,6 +282,9 @@ int gdp_sync(gdp_ctx *ctx);
  * reference's compare domain (src/dynprog_simd.c:1044-1051, :1089-1096,
  * :1134-1141).  Directions use the reference's codes: DIAG 0, HORIZ -1,
  * VERT -2.  dense_offsets[i] is pair i's first element in the dense arrays.
+ * With H == NULL no scores are dumped, and the fills run exactly as a
+ * production batch does (the same column bodies for every column); the
+ * directions are then decoded from the production direction words.
  */
 int gdp_fill_dump(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
                   const char *arena, int64_t arena_bytes, const int64_t *dense_offsets,
@@ -325,7 +328,11 @@ double gdp_measure_int_peak(gdp_ctx *ctx);
  *
  *   npairs <= 65,536 per call, every pair full band and precision 16,
  *   glength <= 1,023; otherwise the call returns GDP_ERR_LEN (too many
- *   pairs) or the pair gets GDP_ERR_PARAM / GDP_ERR_LEN.
+ *   pairs) or the pair gets GDP_ERR_PARAM / GDP_ERR_LEN.  Only the flags
+ *   GDP_FLAG_JUMP_LATE and GDP_FLAG_REVP are taken (no traceback, rerun,
+ *   genome window or endpoint search): a pair with any other flag gets
+ *   GDP_ERR_PARAM.  A pair whose rseq, gseq or gseq_alt bytes do not lie
+ *   inside the arena's first arena_bytes gets GDP_ERR_LEN and is not read.
  *
  * Outputs: d_results[i] (status, score, precision) and pair i's direction
  * words (the library's block-column layout), written to d_dirs (8-byte
@@ -334,13 +341,16 @@ double gdp_measure_int_peak(gdp_ctx *ctx);
  * cudaStream_t; NULL for the legacy stream).
  *
  * The first call on a device sets up that device (it takes the array
- * addresses and uploads the tables for `mode`), so it should come before
- * any stream capture; later calls must use the same mode.  All calls share
- * the array: calls that overlap on the GPU race and must be ordered by the
- * caller.
+ * addresses, uploads the tables for `mode` and waits for the upload), so it
+ * should come before any stream capture; later calls must use the same
+ * mode.  All calls share the array: calls that overlap on the GPU race and
+ * must be ordered by the caller.  The call restores the calling thread's
+ * current device before it returns, and neither fails on nor clears a CUDA
+ * error that the caller's earlier work left pending.
  */
 int gdp_fill16_noalloc(int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, const char *d_arena,
-                       uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results, void *stream);
+                       int64_t arena_bytes, uint32_t *d_dirs, int64_t dir_words_cap, gdp_result_t *d_results,
+                       void *stream);
 
 /*
  * Serving loop (continuous batching).  A server owns `nworkers` contexts

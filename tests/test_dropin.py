@@ -18,7 +18,19 @@ import oracle as orc
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "tests", "dropin_driver.py")
-REF_HEADER = "/root/reference/src/dynprog_simd.h"
+
+
+def _ref_header():
+    """src/dynprog_simd.h of the reference: under GDP_REFSRC, else under the
+    directory oracle/Makefile compiled the reference from (recorded in
+    oracle/_ref/refsrc.txt); None when neither is present."""
+    src = os.environ.get("GDP_REFSRC")
+    if not src:
+        rec = os.path.join(ROOT, "oracle", "_ref", "refsrc.txt")
+        if os.path.exists(rec):
+            src = open(rec).read().strip()
+    path = os.path.join(src, "dynprog_simd.h") if src else None
+    return path if path and os.path.exists(path) else None
 
 
 def _run(*args):
@@ -64,11 +76,12 @@ def _params(text, name):
 
 
 def test_dropin_declarations_match_the_reference():
-    if not os.path.exists(REF_HEADER):
-        pytest.skip("reference sources not present")
+    ref_header = _ref_header()
+    if ref_header is None:
+        pytest.skip("reference sources not present (set GDP_REFSRC)")
     ours = open(os.path.join(ROOT, "include", "gdp_dynprog_simd.h")).read()
     ours = re.sub(r"/\*.*?\*/", "", ours, flags=re.S)
-    theirs = open(REF_HEADER).read()
+    theirs = open(ref_header).read()
     names = sorted(set(re.findall(r"\b(Dynprog_(?:simd|traceback)_[0-9a-z_]+)\s*\(", theirs)))
     names = [n for n in names if "nonavx2" not in n]
     assert len(names) == 12, names

@@ -48,6 +48,37 @@ def test_fill_random(env, seed, variants, precs):
     assert not fails, "\n".join(fails)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("prec,rerun", [(16, False), (8, False), (8, True)])
+def test_production_bodies_cell_by_cell(env, variant, prec, rerun):
+    """The column bodies a production batch runs -- the steady-column and
+    half-width bodies, and for rerun pairs the 16-bit pass that tracks the
+    in-band maximum and the 8-bit pass -- compared cell by cell: every
+    in-band E/F/nogap direction decoded from the production direction
+    words, and the final score, for both tie rules.  Bands are wide enough
+    for most columns of a block to be steady."""
+    ctx, ref, _ = env
+    seed = 500 + 10 * variant + prec + (1 if rerun else 0)
+    pairs, arena = cases.random_cases(seed, 240, variants=(variant,), precisions=(prec,), min_len=8,
+                                      max_len=220, extras=(4, 9, 16, 20, 31, 40, 64))
+    if rerun:
+        pairs["flags"] |= gdp.FLAG_RERUN16
+    assert set(np.unique(pairs["flags"] & gdp.FLAG_JUMP_LATE).tolist()) == {0, gdp.FLAG_JUMP_LATE}
+    fails = parity.check_fill(ctx, ref, pairs, arena, production=True)
+    assert not fails, "\n".join(fails)
+
+
+@pytest.mark.parametrize("kind,n", [(gdp.WL_SHORT, 400), (gdp.WL_CDNA, 6), (gdp.WL_LONG, 3)])
+def test_production_bodies_on_workload_pairs(env, gdplib, kind, n):
+    """The bench's own workload distributions through the production column
+    bodies: every in-band direction and the final score against the
+    reference, at the precision the rerun contract keeps."""
+    ctx, ref, _ = env
+    pairs, arena = gdp.make_pairs(gdplib, kind, 90 + kind, GENOME['g'], n)
+    fails = parity.check_fill(ctx, ref, pairs, arena, production=True)
+    assert not fails, "\n".join(fails)
+
+
 @pytest.mark.parametrize("seed", [201, 202, 203])
 def test_traceback_random(env, seed):
     ctx, ref, rest = env

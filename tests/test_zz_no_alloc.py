@@ -7,9 +7,10 @@ inputs and outputs, and the entry point keeps its working memory in a
 fixed file-scope device array. This test is such a caller. It allocates its
 own buffers and then calls the entry point twice in a row through the C
 ABI. Both times, the scores and every in-band E/F/nogap direction must
-equal those of the regular entry point (gdp_fill_dump), bit for bit.
-Run alone in a fresh process, the first call also performs the entry
-point's one-time device set-up.
+equal those of the regular entry point (gdp_fill_dump) and of the CPU
+oracle (the reference compiled from its sources, or its C restatement),
+bit for bit. Run alone in a fresh process, the first call also performs
+the entry point's one-time device set-up.
 """
 import ctypes
 
@@ -55,10 +56,13 @@ def _decode(pairs, i, words, base):
     return dN, dE, dF, m.ravel()
 
 
-def test_noalloc_fill_matches_batch_entry_point(gdplib):
+def test_noalloc_fill_matches_batch_entry_point(gdplib, restatement):
     import torch
     pairs, arena = cases.random_cases(4242, 200, variants=(0,), precisions=(16,), max_len=120)
     pairs["flags"] &= ~gdp.FLAG_TRACEBACK
+    ref = orc.reference() if orc.reference_available() else restatement
+    ref.init(0)
+    expect = [ref.align(pairs, i, arena) for i in range(pairs.size)]
     # the regular entry point, for comparison
     ctx = gdp.Context(gdplib)
     offs, H, dN, dE, dF, res_ref = ctx.fill_dump(pairs, arena)
@@ -77,8 +81,9 @@ def test_noalloc_fill_matches_batch_entry_point(gdplib):
         d_dirs.zero_()
         d_res.zero_()
         rc = gdplib.gdp_fill16_noalloc(0, 0, ctypes.c_void_p(d_pairs.data_ptr()), pairs.size,
-                                       ctypes.c_void_p(d_arena.data_ptr()), ctypes.c_void_p(d_dirs.data_ptr()),
-                                       cap, ctypes.c_void_p(d_res.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+                                       ctypes.c_void_p(d_arena.data_ptr()), arena.size,
+                                       ctypes.c_void_p(d_dirs.data_ptr()), cap, ctypes.c_void_p(d_res.data_ptr()),
+                                       ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, f"call {call}: {gdp.STATUS.get(rc, rc)}"
         torch.cuda.synchronize()
         res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
@@ -89,21 +94,28 @@ def test_noalloc_fill_matches_batch_entry_point(gdplib):
             n = (int(pairs[i]["rlength"]) + 1) * (int(pairs[i]["glength"]) + 1)
             a0 = int(offs[i])
             gN, gE, gF, m = _decode(pairs, i, words, int(res["rec_offset"][i]))
-            assert np.array_equal(gN[m], dN[a0:a0 + n][m]), (call, i, "nogap")
-            assert np.array_equal(gE[m], dE[a0:a0 + n][m]), (call, i, "Egap")
-            assert np.array_equal(gF[m], dF[a0:a0 + n][m]), (call, i, "Fgap")
+            o = expect[i]
+            assert int(res["score"][i]) == o["score"], (call, i, "score vs oracle")
+            for name, got, batch in (("dN", gN, dN), ("dE", gE, dE), ("dF", gF, dF)):
+                assert np.array_equal(got[m], batch[a0:a0 + n][m]), (call, i, name, "vs batch entry point")
+                assert np.array_equal(got[m], o[name][m]), (call, i, name, "vs oracle")
 
 
 def test_noalloc_rejects_oversize_requests(gdplib):
     import torch
     # more pairs than the fixed array holds: rejected before any device work
-    rc = gdplib.gdp_fill16_noalloc(0, 0, None, 65537, None, None, 0, None, None)
+    rc = gdplib.gdp_fill16_noalloc(0, 0, None, 65537, None, 0, None, 0, None, None)
     assert rc == 1   # GDP_ERR_LEN
-    # a pair longer than the fixed column limit, and one that is not full-band 16-bit
+    # a pair longer than the fixed column limit, one that is not full-band
+    # 16-bit, one whose genome window lies past the arena's end, and one
+    # asking for a genome window this entry point does not fetch
     pairs, arena = cases.random_cases(7, 2, variants=(0,), precisions=(16,), max_len=40)
-    pairs = np.concatenate([pairs, pairs])
+    pairs["flags"] &= ~gdp.FLAG_TRACEBACK
+    pairs = np.concatenate([pairs, pairs, pairs])
     pairs["glength"][0] = 1024
     pairs["precision"][1] = 8
+    pairs["gseq"][2] = arena.size - int(pairs["glength"][2]) + 1
+    pairs["flags"][3] |= gdp.FLAG_GWINDOW
     dev = torch.device("cuda", 0)
     d_pairs = torch.from_numpy(pairs.view(np.uint8).copy()).to(dev)
     big = np.zeros(4096, np.uint8)
@@ -112,10 +124,12 @@ def test_noalloc_rejects_oversize_requests(gdplib):
     d_dirs = torch.zeros(1 << 16, dtype=torch.int32, device=dev)
     d_res = torch.zeros(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     rc = gdplib.gdp_fill16_noalloc(0, 0, ctypes.c_void_p(d_pairs.data_ptr()), pairs.size,
-                                   ctypes.c_void_p(d_arena.data_ptr()), ctypes.c_void_p(d_dirs.data_ptr()),
-                                   1 << 16, ctypes.c_void_p(d_res.data_ptr()), None)
+                                   ctypes.c_void_p(d_arena.data_ptr()), arena.size,
+                                   ctypes.c_void_p(d_dirs.data_ptr()), 1 << 16, ctypes.c_void_p(d_res.data_ptr()),
+                                   None)
     assert rc == 0
     torch.cuda.synchronize()
     res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
-    assert res["status"][0] == 1 and res["status"][1] == 3
-    assert (res["status"][2:] == 0).all()
+    assert list(res["status"][:4]) == [1, 3, 1, 3], res["status"]
+    assert (res["status"][4:] == 0).all()
+    assert torch.cuda.current_device() == 0
