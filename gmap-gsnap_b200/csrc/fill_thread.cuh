@@ -64,10 +64,20 @@ struct FillParams {
   const gdp_tables_t *tab;
   /* Byte k: for mismatch type k, the smallest row and column index at which
      an in-band score can reach 127 (at most 255).  Every score is the score
-     of a path from the matrix corner, so H(r, c) <= min(r, c) times the
+     of a path from the matrix corner, whose own score is at most one table
+     entry (upper and lower fills), so H(r, c) <= (min(r, c) + 1) times the
      table's largest entry.  The in-band 127 checks (MODE != 0) skip cells
      below it; 0 checks every cell. */
   uint32_t reach_from4;
+  /* Byte k: for mismatch type k, how far a 16-bit lower-fill score can lie
+     above the 8-bit one at the same cell.  The reference's 8-bit lower
+     fill scores its corner against character code 4 (src/dynprog_simd.c:
+     5459), the 16-bit one against 'N' (:8689), so the 16-bit scores of
+     paths from the corner are that much higher; elsewhere every operation
+     is monotone and the 8-bit scores are never the lower ones.  A 16-bit
+     pass (MODE 1) of a lower fill proves the 8-bit overflow only from
+     127 + this slack. */
+  uint32_t lower_slack4;
 };
 
 /* Lanes lo..hi (0 <= lo <= hi <= 31) as a bit mask. */
@@ -96,6 +106,7 @@ struct PairView {
   int open, ext, oe, mt, lband, uband;
   int dlo, dhi;                  /* in-band lanes of column y: y - dhi <= x <= y + dlo */
   int reach_from;                /* FillParams::reach_from of the pair's mismatch type */
+  int lim;                       /* an in-band score at or above this proves the 8-bit overflow */
   int endmode;                   /* 0, or 1 (GDP_FLAG_ENDPOINT), or 2 (GDP_FLAG_ENDPOINT_QEND) */
   const char *lseq, *lalt, *sseq, *salt;
   int llen, slen;
@@ -111,6 +122,7 @@ pair_view (const gdp_pair_t &p, const char *arena, PairView &v) {
   v.lband = p.lband; v.uband = p.uband;
   v.dlo = (VARIANT == GDP_FULL) ? p.lband : 0;
   v.dhi = (VARIANT == GDP_FULL) ? p.uband : (VARIANT == GDP_UPPER ? p.uband : p.lband);
+  v.lim = 127;
   v.lseq = arena + (VARIANT == GDP_LOWER ? p.gseq : p.rseq);
   v.lalt = arena + (VARIANT == GDP_LOWER ? p.gseq_alt : p.rseq);
   v.llen = (VARIANT == GDP_LOWER) ? p.glength : p.rlength;
@@ -374,7 +386,7 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
       const uint32_t dom = lane_range(max(dl, 0), dh);
 #pragma unroll
       for (int i = LS; i < W; i++)
-        if ((dom & (1u << i)) && B.H[i] >= 127) reached = true;
+        if ((dom & (1u << i)) && B.H[i] >= v.lim) reached = true;
     }
   }
   if (y == v.g.Y) {
@@ -569,6 +581,7 @@ fill_thread_kernel (FillParams P) {
     PairView v;
     pair_view<W, VARIANT>(p, P.arena, v);
     v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
+    if (MODE == 1 && VARIANT == GDP_LOWER) v.lim += (int) ((P.lower_slack4 >> (8 * (v.mt & 3))) & 255u);
     v.endmode = (VARIANT == GDP_FULL) ? 0 : (p.flags & GDP_FLAG_ENDPOINT) ? 1 : (p.flags & GDP_FLAG_ENDPOINT_QEND) ? 2 : 0;
     EndBest eb;
     eb.score = 0; eb.r = 0; eb.c = 0; eb.found = false;
@@ -630,7 +643,7 @@ fill_thread_kernel (FillParams P) {
       dir = dcol;
       if (MODE == 2 && reached) break;
     }
-    if (vmax >= 127) reached = true;
+    if (vmax >= v.lim) reached = true;
     if (v.endmode == 2 && !eb.found) {
       /* the last-row search starts at (rlength, 0) */
       eb.score = LO;

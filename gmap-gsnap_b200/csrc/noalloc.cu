@@ -209,6 +209,7 @@ noalloc_run (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, co
   P.scratch_rows = GDP_NOALLOC_MAX_COLS;
   P.tab = tables;
   P.reach_from4 = 0;
+  P.lower_slack4 = 0;
   for (int late = 1; late >= 0; late--) {
     P.list = late ? list_late : list_early;
     P.count = counts + (late ? 0 : 1);

@@ -292,6 +292,7 @@ struct gdp_ctx {
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
   int reach_from[4] = {0, 0, 0, 0};   /* FillParams::reach_from of h_tab */
+  int lower_slack[4] = {0, 0, 0, 0};  /* FillParams::lower_slack4 of h_tab */
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
@@ -385,15 +386,27 @@ prof_end (gdp_ctx *ctx, int id, cudaEvent_t a, cudaStream_t s = nullptr) {
 }
 
 /* Per mismatch type, the smallest row and column index at which a score
-   can reach 127 under h_tab: every score is a path score from the matrix
-   corner, at most min(r, c) times the table's largest entry. */
+   can reach 127 under h_tab.  Every score is a path score from the matrix
+   corner.  The corner itself scores one table entry in the upper and lower
+   fills (their row and column 0 profiles meet the 'N' row or class 4 at
+   (0, 0), src/dynprog_simd.c:7879, :8782), so a score at (r, c) is at most
+   min(r, c) + 1 times the table's largest entry: a 42 x 42 exact match of
+   an upper fill scores 3 + 42 * 3 = 129. */
 static void
 update_reach (gdp_ctx *ctx) {
   for (int mt = 0; mt < 4; mt++) {
     int mx = -32768;
     for (int a = 0; a < 128; a++)
       for (int b = 0; b < 128; b++) mx = std::max(mx, (int) ctx->h_tab->pd[mt][a][b]);
-    ctx->reach_from[mt] = (mx <= 0) ? (1 << 30) : (127 + mx - 1) / mx;
+    ctx->reach_from[mt] = (mx <= 0) ? (1 << 30) : std::max(0, (127 + mx - 1) / mx - 1);
+    /* lower fills: the 16-bit corner profile ('N') against the 8-bit one
+       (character code 4), for each query class (FillParams::lower_slack4) */
+    int slack = 0;
+    for (int k = 0; k < 5; k++) {
+      const int q = "ACGTN"[k];
+      slack = std::max(slack, (int) ctx->h_tab->pd[mt][q]['N'] - (int) ctx->h_tab->pd[mt][q][4]);
+    }
+    ctx->lower_slack[mt] = std::min(slack, 255);
   }
 }
 
@@ -1315,7 +1328,11 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
       P.reach_from4 = 0;
-      for (int q = 0; q < 4; q++) P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
+      P.lower_slack4 = 0;
+      for (int q = 0; q < 4; q++) {
+        P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
+        P.lower_slack4 |= (uint32_t) ctx->lower_slack[q] << (8 * q);
+      }
       cudaStream_t ks = s;
       if (warp || cta || early8) {
         if (!forked) {

@@ -68,6 +68,48 @@ def test_production_bodies_cell_by_cell(env, variant, prec, rerun):
     assert not fails, "\n".join(fails)
 
 
+def test_rerun_bound_counts_the_corner(env):
+    """The upper and lower fills score the corner cell (0, 0) with one table
+    entry, so an exact match of 42 x 42 reaches 3 + 42 * 3 = 129 in 16 bits
+    and saturates the 8-bit fill at (42, 42).  Rerun pairs of 40-44 rows
+    around that bound, exact and with one mismatch, in every variant, must
+    keep the precision the rerun contract gives, with every output
+    bit-exact."""
+    ctx, ref, rest = env
+    rng = np.random.default_rng(4242)
+    rows, chunks, off = [], [], 0
+    for variant in (0, 1, 2):
+        for n in (40, 41, 42, 43, 44):
+            for mism in (0, 1):
+                for late in (0, 1):
+                    q = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=n)
+                    g = q.copy()
+                    if mism:
+                        k = int(rng.integers(0, n))
+                        g[k] = ord("A") if g[k] != ord("A") else ord("C")
+                    rows.append((variant, n, late, off))
+                    chunks += [q, q, g, g]
+                    off += 4 * n
+    pairs = np.zeros(len(rows), dtype=gdp.PAIR_DTYPE)
+    for j, (variant, n, late, o) in enumerate(rows):
+        p = pairs[j]
+        p["rseq"], p["rseq_uc"], p["gseq"], p["gseq_alt"] = o, o + n, o + 2 * n, o + 3 * n
+        p["rlength"] = p["glength"] = n
+        p["lband"], p["uband"] = (3, 3) if variant == 0 else ((0, 4) if variant == 1 else (4, 0))
+        p["variant"], p["precision"], p["mismatchtype"] = variant, 8, 1
+        p["open"], p["extend"] = -30, -56
+        p["flags"] = gdp.FLAG_TRACEBACK | gdp.FLAG_RERUN16 | (gdp.FLAG_JUMP_LATE if late else 0)
+        p["tb_r"], p["tb_c"] = n, n
+        p["genomeoffset"], p["chrhigh"], p["watsonp"], p["dynprogindex"] = 100, 60000, 1, 1
+    arena = np.concatenate(chunks).astype(np.uint8)
+    fails = parity.check_fill(ctx, ref, pairs, arena, production=True)
+    assert not fails, "\n".join(fails)
+    fails = parity.check_fill(ctx, ref, pairs, arena)
+    assert not fails, "\n".join(fails)
+    fails, _ = parity.check_traceback(ctx, ref, rest, pairs, arena)
+    assert not fails, "\n".join(fails)
+
+
 @pytest.mark.parametrize("kind,n", [(gdp.WL_SHORT, 400), (gdp.WL_CDNA, 6), (gdp.WL_LONG, 3)])
 def test_production_bodies_on_workload_pairs(env, gdplib, kind, n):
     """The bench's own workload distributions through the production column
