@@ -6,17 +6,24 @@ rlength U{75..300}, lband/uband U{3..30}, 3% substitutions, 1% indels, 5%
 random non-matching windows, 8-bit fills with the 16-bit rerun on overflow,
 traceback of every pair.  Synthetic, seeded.  Metric: GCUPS over the
 in-band cells of the reference's compare domain, whole job, fill +
-traceback.  `value` is measured with pairs and sequences resident in HBM;
+traceback.  `value` is measured with pairs and sequences resident in HBM,
+the plan replayed as a CUDA graph with the autotuner's routing in force;
 `e2e` goes through the host-buffer C-ABI call gdp_align_batch (host->device
 copies, planning, kernels, device->host copies of results and Pair records
-all inside the timed region).
+all inside the timed region).  The CPU leg times the reference on a prefix
+of the same pairs and checks the device's outputs on it pair by pair
+(`parity`).  Configurations 1 (10,000 fixed 150 x 160 pairs), 3 (50,000
+cDNA gaps, upper and lower fills) and 4 (2,000,000 mixed pairs) are
+measured at their sizes beside it, each with its CPU figure and parity
+sample on the same pairs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gdp|reference]
 
 For N > 1 launch with torchrun; each rank aligns its own shard of the same
 size (weak scaling, no data-path collective: pairs are independent).
 `--impl reference` times the reference's own CPU code (oracle/_ref, built
-from the reference sources) on the host cores over a bounded sample.
+from the reference sources) on the host cores over a prefix of the same
+pairs; that process loads no CUDA library.
 """
 import argparse
 import ctypes
@@ -26,7 +33,6 @@ import statistics
 import subprocess
 import sys
 import threading
-import time
 
 import numpy as np
 
@@ -39,8 +45,9 @@ import gdp  # noqa: E402
 WORKLOADS = {
     "short": (gdp.WL_SHORT, 1_000_000, "short reads r U{75..300}, bands U{3..30}, 8-bit + 16-bit rerun"),
     "fixed": (gdp.WL_FIXED, 10_000, "fixed 150x160, lband=uband=10, 16-bit"),
-    "mix": (gdp.WL_MIX, 20_000, "70/25/5 short/long/cdna mix"),
-    "cdna": (gdp.WL_CDNA, 2_000, "cDNA upper fill, r log-U[200,5000]"),
+    "mix": (gdp.WL_MIX, 2_000_000, "70/25/5 short/long/cDNA draws (a cDNA draw is its upper and lower fill)"),
+    "cdna": (gdp.WL_CDNA, 100_000, "cDNA gaps, r log-U[200,5000], g = r U(1,1.5): upper fill (uband g-r+14) "
+                                    "with traceback plus lower fill (lband 14), 16-bit"),
     "long": (gdp.WL_LONG, 2_000, "long reads r U{1000..10000}, bands U{50..200}, 16-bit"),
 }
 OPS_PER_CELL = 9          # E: 2 add + 1 max, F: 2 add + 1 max, H: 1 add + 2 max
@@ -202,53 +209,94 @@ def sum_over_ranks(world, value):
 
 
 def make_workload(lib, name, npairs, seed, genome_len=1 << 24):
+    """The seeded workload `name` (libgdp.so or the standalone generator
+    libgdpwl.so give the same pairs)."""
     kind = WORKLOADS[name][0]
     genome, blocks = gdp.make_genome(lib, 777, genome_len)
     pairs, arena = gdp.make_pairs(lib, kind, seed, genome, npairs)
     return genome, blocks, pairs, arena
 
 
-def cpu_baseline(lib, name, seed, target_seconds, threads=None, genome=None):
-    """The reference's own code (oracle/_ref) on a bounded sample of the same
-    workload, all host threads (or the port when the reference is absent).
-    `genome` = (sequence, genomecomp blocks) already set in the library."""
+def _final_cell_in_band(pairs):
+    """Whether each pair's final cell (rlength, glength) lies in its band:
+    outside it the reference leaves the cell unwritten (a cDNA gap's lower
+    fill when glength > rlength), so no final score is compared there."""
+    d = pairs["rlength"].astype(np.int64) - pairs["glength"].astype(np.int64)
+    v = pairs["variant"]
+    lo = np.where(v == gdp.FULL, -pairs["uband"].astype(np.int64),
+                  np.where(v == gdp.UPPER, -pairs["uband"].astype(np.int64), 0))
+    hi = np.where(v == gdp.UPPER, 0, pairs["lband"].astype(np.int64))
+    return (d >= lo) & (d <= hi)
+
+
+def parity_sample(sample, kept, ref_out, res, recs):
+    """Per sampled pair, the device's outputs (results and records of the
+    same pairs) against the reference's (ref_out from oracle outputs()):
+    status, kept precision, final score, traceback score and counts,
+    record count and record digest."""
+    n = sample.size
+    res = res[:n]
+    tb = (sample["flags"] & gdp.FLAG_TRACEBACK) != 0
+    want_prec = np.where((sample["precision"] == 8) & ((sample["flags"] & gdp.FLAG_RERUN16) != 0),
+                         kept, sample["precision"])
+    ok = (res["status"] == 0) & (res["precision"] == want_prec)
+    ok &= ~_final_cell_in_band(sample) | (res["score"] == ref_out[:, 0])
+    for j, k in enumerate(("tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs")):
+        ok &= ~tb | (res[k] == ref_out[:, 1 + j])
+    dig = gdp.record_digests(recs, np.where(tb, res["rec_offset"], 0), np.where(tb, res["nrecs"], 0))
+    ok &= ~tb | (dig == ref_out[:, 7].view(np.uint32))
+    bad = np.nonzero(~ok)[0]
+    return {"pairs": int(n), "mismatches": int(bad.size), "first_mismatches": bad[:5].tolist(),
+            "compared": "status, kept precision, final score, traceback score and counts, record count "
+                        "and a digest of every Pair record, per pair"}
+
+
+def cpu_leg(pairs, arena, blocks, genome_len, seconds, threads=None, res=None, recs=None, max_pairs=None):
+    """The reference's own code (oracle/_ref; the restatement when the
+    reference is absent) timed on the host cores over a prefix of the very
+    pairs the device aligned, sized to about `seconds`: every pair once at
+    the precision the rerun contract keeps (from the restatement, untimed).
+    Beside it the same build with the per-column _mm_clflush compiled out
+    (the "strong CPU" figure) on the same sample, and -- given the device's
+    results and records of those pairs -- the per-pair parity of the
+    sample (an untimed run with outputs)."""
     import oracle
     kind = "reference" if oracle.reference_available() else "port"
     ref = oracle.reference() if kind == "reference" else oracle.restatement()
-    threads = threads or os.cpu_count() or 1
-    if genome is None:
-        ref.init(0)
-        genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
-        ref.set_genome(blocks, None, genome.size)
-    else:
-        genome, blocks = genome
-    # calibration: rerun pairs in 16-bit, which costs about what the kept precisions do
-    n = 200
-    while True:
-        pairs, arena = gdp.make_pairs(lib, WORKLOADS[name][0], seed + 99, genome, n)
-        secs, _ = ref.bench(pairs, arena, threads)
-        if secs >= target_seconds / 4 or n >= 2_000_000:
-            break
-        n = int(min(2_000_000, n * max(2.0, target_seconds / max(secs, 1e-3))))
-    # the timed sample runs each pair at the precision the rerun contract keeps
-    kept = kept_precisions(lib, genome, blocks, pairs, arena, threads)
-    secs, _ = ref.bench(pairs, arena, threads, kept)
-    cells = int(gdp.band_cells(pairs).sum())
-    return {"value": round(cells / secs / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
-            "sample": f"{n} pairs of the '{name}' workload ({cells} in-band cells), fill + traceback at the "
-                      f"kept precision ({int((kept == 8).sum())} 8-bit), {secs:.2f} s wall on {threads} threads",
-            "seconds": secs, "pairs": n, "cells": cells, "kept": kept, "data": (pairs, arena)}
-
-
-def kept_precisions(lib, genome, blocks, pairs, arena, threads):
-    """Per pair, the precision the rerun contract keeps (an 8-bit pair
-    flagged RERUN16 keeps 8 unless its 8-bit fill saturates or its 8-bit
-    traceback would read unwritten cells), from the restatement, untimed."""
-    import oracle
+    ref.init(0)
+    ref.set_genome(blocks, None, genome_len)
     rest = oracle.restatement()
     rest.init(0)
-    rest.set_genome(blocks, None, genome.size)
-    return rest.kept_precision(pairs, arena, threads)
+    rest.set_genome(blocks, None, genome_len)
+    threads = threads or os.cpu_count() or 1
+    limit = min(pairs.size, max_pairs or pairs.size)
+    n = min(limit, 256)
+    while True:
+        sample = pairs[:n]
+        kept = rest.kept_precision(sample, arena, threads)
+        secs, _ = ref.bench(sample, arena, threads, kept)
+        if n >= limit or secs >= seconds * 0.7:
+            break
+        n = min(limit, int(n * min(16.0, max(1.3, seconds / max(secs, 1e-4)))))
+    cells = int(gdp.band_cells(sample).sum())
+    out = {"value": round(cells / secs / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+           "sample": f"the first {n} of the same pairs ({cells} in-band cells), fill + traceback at the "
+                     f"kept precision ({int((kept == 8).sum())} 8-bit), {secs:.2f} s wall on {threads} threads",
+           "seconds": round(secs, 3), "pairs": int(n), "cells": cells,
+           "alignments_per_s": round(n / secs, 1)}
+    if kind == "reference" and os.path.exists(oracle.REF_LIB_NOFLUSH):
+        nf = oracle.reference(noflush=True)
+        nf.init(0)
+        nf.set_genome(blocks, None, genome_len)
+        s2, _ = nf.bench(sample, arena, threads, kept)
+        out["noflush"] = {"value": round(cells / s2 / 1e9, 4), "unit": "GCUPS", "cores": threads,
+                          "seconds": round(s2, 3),
+                          "build": "the same reference sources with the per-column _mm_clflush compiled out "
+                                   "(oracle/_ref/libgdpref_noflush.so)"}
+    if res is not None:
+        _, ref_out = ref.outputs(sample, arena, threads, kept)
+        out["parity"] = parity_sample(sample, kept, ref_out, res, recs)
+    return out
 
 
 def endpoint_search(lib, ctx, seed, ngaps=200000):
@@ -343,11 +391,13 @@ def stage3_gaps(genome, seed, ngaps, max_rlength, max_glength):
     return gaps, arena
 
 
-def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=20000):
+def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=100000):
     """Dynprog_single_gap over a batch of stage-3 single gaps, end to end
     through gdp_single_gap_batch (host gaps and sequences in, host records
-    out), against the reference's own Dynprog_single_gap on the host (one
-    thread, a bounded sample of the same gaps)."""
+    out), against the reference's own Dynprog_single_gap on the host (all
+    host threads, each with its own Dynprog_T and Pairpool_T, over a
+    bounded prefix of the same gaps; its results are checked against the
+    device's on that prefix, untimed)."""
     import torch
     genome, blocks = gdp.make_genome(lib, 778, 1 << 24)
     ctx.set_genome(blocks, None, genome.size)
@@ -403,88 +453,20 @@ def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=20000):
         ref.set_genome(blocks, None, genome.size)
         rs = oracle.ReferenceSingleGap(ref, 200, 40)
         sample = gaps[:cpu_gaps]
-        t0 = time.perf_counter()
+        threads = os.cpu_count() or 1
+        secs, _ = rs.bench(sample, arena, threads, 200, 40)
+        secs1, _ = rs.bench(sample[:cpu_gaps // 8], arena, 1, 200, 40)
         st, off, rrecs = rs.run(sample, arena)
-        secs = time.perf_counter() - t0
         same = (np.array_equal(st[:, 0], res["tb_score"][:cpu_gaps]) and
                 np.array_equal(st[:, 5], res["nrecs"][:cpu_gaps]) and
                 np.array_equal(rrecs, recs[:int(res["nrecs"][:cpu_gaps].sum())]))
-        out["cpu_baseline"] = {"value": round(cpu_gaps / secs, 1), "unit": "gaps/s", "cores": 1,
+        out["cpu_baseline"] = {"value": round(cpu_gaps / secs, 1), "unit": "gaps/s", "cores": threads,
                                "kind": "reference",
                                "sample": f"the first {cpu_gaps} gaps, Dynprog_single_gap of oracle/_ref, "
-                                         f"{secs:.2f} s on 1 thread",
+                                         f"{secs:.2f} s on {threads} threads",
+                               "one_thread_gaps_per_s": round((cpu_gaps // 8) / secs1, 1),
                                "same_results": bool(same)}
     return out
-
-
-def per_pair_vs_batched(lib, ctx, seed, npairs=20000, nsample=500):
-    """The same mixed-length pairs (70/25/5 short/long/cDNA) aligned as one
-    batch and as one plan per pair (every pair its own kernel launches),
-    both device-resident, timed with CUDA events on the context's stream."""
-    import torch
-    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
-    pairs, arena = gdp.make_pairs(lib, gdp.WL_MIX, seed, genome, npairs)
-    ctx.set_genome(blocks, None, genome.size)
-    stream = torch.cuda.ExternalStream(ctx.stream_handle())
-    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
-    d_arena = torch.from_numpy(arena).cuda()
-    d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
-
-    def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            fn()
-        b.record(stream)
-        b.synchronize()
-        return a.elapsed_time(b) / reps
-
-    plan = ctypes.c_void_p()
-    assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan)) == 0, ctx.error()
-    d_recs = torch.empty(max(int(lib.gdp_plan_total_recs(plan)), 1) * gdp.REC_DTYPE.itemsize, dtype=torch.uint8,
-                         device="cuda")
-    batch_ms = timed(lambda: lib.gdp_plan_execute(ctx.h, plan, ctypes.c_void_p(d_pairs.data_ptr()),
-                                                  ctypes.c_void_p(d_arena.data_ptr()),
-                                                  ctypes.c_void_p(d_res.data_ptr()),
-                                                  ctypes.c_void_p(d_recs.data_ptr())), 2)
-    batch_res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE).copy()
-    lib.gdp_plan_destroy(plan)
-    cells = gdp.band_cells(pairs)
-
-    sample = np.arange(min(nsample, pairs.size))
-    plans, offs, tot = [], [], 0
-    for i in sample:
-        pl = ctypes.c_void_p()
-        assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs[i:i + 1]), 1, ctypes.byref(pl)) == 0, ctx.error()
-        plans.append(pl)
-        offs.append(tot)
-        tot += max(int(lib.gdp_plan_total_recs(pl)), 1)
-    d_recs1 = torch.empty(tot * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
-    pb, ab, rb, cb = d_pairs.data_ptr(), d_arena.data_ptr(), d_res.data_ptr(), d_recs1.data_ptr()
-
-    def one_by_one():
-        for k, i in enumerate(sample):
-            lib.gdp_plan_execute(ctx.h, plans[k], ctypes.c_void_p(pb + int(i) * gdp.PAIR_DTYPE.itemsize),
-                                 ctypes.c_void_p(ab), ctypes.c_void_p(rb + int(i) * gdp.RESULT_DTYPE.itemsize),
-                                 ctypes.c_void_p(cb + offs[k] * gdp.REC_DTYPE.itemsize))
-
-    pair_ms = timed(one_by_one, 1)
-    one_res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
-    for pl in plans:
-        lib.gdp_plan_destroy(pl)
-    same = all(np.array_equal(one_res[k][sample], batch_res[k][sample])
-               for k in ("status", "score", "tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs"))
-    batched = float(cells.sum()) / (batch_ms * 1e-3) / 1e9
-    per_pair = float(cells[sample].sum()) / (pair_ms * 1e-3) / 1e9
-    return {"workload": f"mix 70/25/5 short/long/cDNA, {pairs.size} pairs ({int(cells.sum())} cells)",
-            "batched_gcups": round(batched, 3), "per_pair_gcups": round(per_pair, 3),
-            "per_pair_sample": f"first {sample.size} of the same pairs, one plan (own launches) per pair",
-            "ratio": round(batched / per_pair, 2),
-            "batched_alignments_per_s": round(pairs.size / (batch_ms * 1e-3), 1),
-            "per_pair_alignments_per_s": round(sample.size / (pair_ms * 1e-3), 1),
-            "results_identical": bool(same)}
 
 
 def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000,
@@ -518,30 +500,195 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
             "peak_admitted_dir_gb": round(st["peak_reserved_bytes"] / 2**30, 3)}
 
 
+def measure_config(lib, ctx, label, name, npairs, seed, chunk, cpu_seconds, genome=None, tune_pairs=0,
+                   per_pair=0, cpu_max_pairs=None):
+    """One workload at its stated size on the device, chunk by chunk (each
+    chunk its own seeded draw of the distribution, generated outside every
+    timed region):
+      * device: each chunk as a device-resident plan executed as a CUDA
+        graph (the first execution runs and captures the plan, the second,
+        timed, launches the graph);
+      * e2e: each chunk through gdp_align_batch from pinned host buffers to
+        host results and Pair records (the internal waves stream the
+        direction memory);
+      * per_pair (optional): the first `per_pair` pairs, one plan each;
+      * cpu_baseline: the reference on a prefix of chunk 0, with the
+        per-pair parity of that prefix against chunk 0's e2e outputs.
+    With tune_pairs, gdp_autotune first picks the routing parameters on a
+    separate draw of the same distribution, and they stay in force."""
+    import torch
+    kind = WORKLOADS[name][0]
+    if genome is None:
+        genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
+    else:
+        genome, blocks = genome
+    ctx.set_genome(blocks, None, genome.size)
+    out = {"workload": WORKLOADS[name][2], "pairs": int(npairs), "chunk_pairs": int(chunk)}
+    if tune_pairs:
+        tp, ta = gdp.make_pairs(lib, kind, seed + 4242, genome, tune_pairs)
+        params, best = ctx.autotune(tp, ta)
+        out["autotune"] = {"sample_pairs": int(tune_pairs), "params": params, "sample_ms": round(best, 3)}
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    nchunks = (npairs + chunk - 1) // chunk
+    cells = dev_ms = e2e_ms = 0.0
+    bad = e2e_bad = launches = h2d = d2h = 0
+    first = None
+    host = {}
+
+    def pinned(key, nbytes):
+        have = host.get(key)
+        if have is None or have.numel() < nbytes:
+            host[key] = torch.empty(max(nbytes, 16), dtype=torch.uint8, pin_memory=True)
+        return host[key]
+
+    for k in range(nchunks):
+        m = min(chunk, npairs - k * chunk)
+        pairs, arena = gdp.make_pairs(lib, kind, seed + k, genome, m)
+        cells += float(gdp.band_cells(pairs).sum())
+        plan = ctypes.c_void_p()
+        assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan)) == 0, ctx.error()
+        lib.gdp_plan_use_graph(plan, 1)
+        total_recs = int(lib.gdp_plan_total_recs(plan))
+        d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+        d_arena = torch.from_numpy(arena).cuda()
+        d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        d_recs = torch.empty(max(total_recs, 1) * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        args4 = [ctypes.c_void_p(t.data_ptr()) for t in (d_pairs, d_arena, d_res, d_recs)]
+        assert lib.gdp_plan_execute(ctx.h, plan, *args4) == 0, ctx.error()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches()
+        a.record(stream)
+        assert lib.gdp_plan_execute(ctx.h, plan, *args4) == 0, ctx.error()
+        b.record(stream)
+        b.synchronize()
+        launches += ctx.launches() - l0
+        dev_ms += a.elapsed_time(b)
+        res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+        bad += int((res["status"] != 0).sum())
+        lib.gdp_plan_destroy(plan)
+        del d_pairs, d_arena, d_res, d_recs
+        torch.cuda.empty_cache()
+        # end to end from pinned host buffers
+        hp = pinned("pairs", pairs.nbytes).numpy()[:pairs.nbytes].view(gdp.PAIR_DTYPE)
+        hp[...] = pairs
+        ha = pinned("arena", arena.nbytes).numpy()[:arena.nbytes]
+        ha[...] = arena
+        hr = pinned("res", pairs.size * gdp.RESULT_DTYPE.itemsize).numpy()[
+            :pairs.size * gdp.RESULT_DTYPE.itemsize].view(gdp.RESULT_DTYPE)
+        cap = max(total_recs, 1)
+        hc = pinned("recs", cap * gdp.REC_DTYPE.itemsize).numpy()[:cap * gdp.REC_DTYPE.itemsize].view(gdp.REC_DTYPE)
+        used = ctypes.c_int64(0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.gdp_align_batch(ctx.h, gdp._ptr(hp), hp.size, gdp._ptr(ha), ha.size, gdp._ptr(hr), gdp._ptr(hc),
+                                 cap, ctypes.byref(used))
+        e1.record(stream)
+        e1.synchronize()
+        assert rc == 0, ctx.error()
+        e2e_ms += e0.elapsed_time(e1)
+        e2e_bad += int((hr["status"] != 0).sum())
+        h2d += pairs.nbytes + arena.nbytes
+        d2h += hr.nbytes + int(used.value) * gdp.REC_DTYPE.itemsize
+        if k == 0:
+            first = (pairs, arena, hr.copy(), hc[:int(used.value)].copy())
+    out["device"] = {"gcups": round(cells / (dev_ms * 1e-3) / 1e9, 3), "ms": round(dev_ms, 3),
+                     "alignments_per_s": round(npairs / (dev_ms * 1e-3), 1), "graph": True,
+                     "gpu_launches": int(launches), "bad_status_pairs": bad,
+                     "timing": "device-resident plans, one per chunk, each executed as a CUDA graph; "
+                               "CUDA events on the context stream around each chunk's graph launch"}
+    out["e2e"] = {"gcups": round(cells / (e2e_ms * 1e-3) / 1e9, 3), "ms": round(e2e_ms, 3),
+                  "h2d_bytes": int(h2d), "d2h_bytes": int(d2h), "bad_status_pairs": e2e_bad,
+                  "host_buffers": "pinned"}
+    out["cells"] = int(cells)
+    pairs, arena, res0, recs0 = first
+    if per_pair:
+        sample = np.arange(min(per_pair, pairs.size))
+        d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+        d_arena = torch.from_numpy(arena).cuda()
+        d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        plans, offs, tot = [], [], 0
+        for i in sample:
+            pl = ctypes.c_void_p()
+            assert lib.gdp_plan_create(ctx.h, gdp._ptr(pairs[i:i + 1]), 1, ctypes.byref(pl)) == 0, ctx.error()
+            plans.append(pl)
+            offs.append(tot)
+            tot += max(int(lib.gdp_plan_total_recs(pl)), 1)
+        d_recs = torch.empty(tot * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        pb, ab, rb, cb = d_pairs.data_ptr(), d_arena.data_ptr(), d_res.data_ptr(), d_recs.data_ptr()
+
+        def one_by_one():
+            for j, i in enumerate(sample):
+                lib.gdp_plan_execute(ctx.h, plans[j], ctypes.c_void_p(pb + int(i) * gdp.PAIR_DTYPE.itemsize),
+                                     ctypes.c_void_p(ab), ctypes.c_void_p(rb + int(i) * gdp.RESULT_DTYPE.itemsize),
+                                     ctypes.c_void_p(cb + offs[j] * gdp.REC_DTYPE.itemsize))
+
+        one_by_one()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        one_by_one()
+        b.record(stream)
+        b.synchronize()
+        pair_ms = a.elapsed_time(b)
+        one = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+        for pl in plans:
+            lib.gdp_plan_destroy(pl)
+        same = all(np.array_equal(one[k][sample], res0[k][sample])
+                   for k in ("status", "score", "precision", "tb_score", "nmatches", "nmismatches", "nopens",
+                             "nindels", "nrecs"))
+        pcells = float(gdp.band_cells(pairs[sample]).sum())
+        per = pcells / (pair_ms * 1e-3) / 1e9
+        out["per_pair"] = {"gcups": round(per, 3), "pairs": int(sample.size),
+                           "alignments_per_s": round(sample.size / (pair_ms * 1e-3), 1),
+                           "sample": f"the first {sample.size} pairs of chunk 0, one plan (its own launches) "
+                                     f"per pair, back to back on one stream",
+                           "results_identical_to_batch": bool(same)}
+        out["batched_vs_per_pair"] = round(out["device"]["gcups"] / per, 2)
+    if cpu_seconds > 0:
+        out["cpu_baseline"] = cpu_leg(pairs, arena, blocks, genome.size, cpu_seconds, res=res0, recs=recs0,
+                                      max_pairs=cpu_max_pairs)
+    return out
+
+
 def run_reference_arm(args):
+    """The reference's own CPU code (oracle/_ref, compiled from its sources)
+    on the host cores, over a prefix of the same seeded pairs the device
+    arm aligns.  This process loads no CUDA library: the pairs come from the
+    standalone generator libgdpwl.so and the code timed from oracle/."""
     # host cores only: rank 0 runs the sample, the other ranks exit at once
     # (no process group, so nothing waits on rank 0's minutes of CPU work)
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    lib = gdp.load()
+    wl = gdp.load_workload()
     name = args.workload
+    npairs = args.npairs or WORKLOADS[name][1]
+    genome, blocks, pairs, arena = make_workload(wl, name, npairs, args.seed)
     import oracle
     kind = "reference" if oracle.reference_available() else "port"
     ref = oracle.reference() if kind == "reference" else oracle.restatement()
     ref.init(0)
-    threads = os.cpu_count() or 1
-    genome, blocks = gdp.make_genome(lib, 777, 1 << 24)
     ref.set_genome(blocks, None, genome.size)
-    cal = cpu_baseline(lib, name, args.seed, args.cpu_seconds / max(args.steps, 1), threads, (genome, blocks))
-    pairs, arena = cal["data"]
-    kept = cal["kept"]
-    cells = int(gdp.band_cells(pairs).sum())
+    rest = oracle.restatement()
+    rest.init(0)
+    rest.set_genome(blocks, None, genome.size)
+    threads = os.cpu_count() or 1
+    per_step = args.ref_seconds / max(args.steps + 0.25 * args.warmup, 1)
+    n = min(pairs.size, 512)
+    while True:
+        sample = pairs[:n]
+        kept = rest.kept_precision(sample, arena, threads)
+        secs, _ = ref.bench(sample, arena, threads, kept)
+        if n >= pairs.size or secs >= per_step * 0.7:
+            break
+        n = min(pairs.size, int(n * min(16.0, max(1.3, per_step / max(secs, 1e-4)))))
+    cells = int(gdp.band_cells(sample).sum())
     for _ in range(args.warmup):
-        m = max(1, pairs.size // 20)
-        ref.bench(pairs[:m], arena, threads, kept[:m])
+        m = max(1, n // 4)
+        ref.bench(sample[:m], arena, threads, kept[:m])
     times = []
     for _ in range(args.steps):
-        secs, _ = ref.bench(pairs, arena, threads, kept)
+        secs, _ = ref.bench(sample, arena, threads, kept)
         times.append(secs)
     t = sum(times)
     value = cells * args.steps / t / 1e9
@@ -549,15 +696,44 @@ def run_reference_arm(args):
             "unit": "GCUPS", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * t / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16/int8",
-            "data": "synthetic", "config": {"workload": name, "pairs_per_step": int(pairs.size),
+            "data": "synthetic", "config": {"workload": name, "pairs_per_step": int(sample.size),
+                                            "pairs_of_workload": int(pairs.size),
                                             "description": WORKLOADS[name][2]},
             "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
-                             "sample": f"{pairs.size} pairs of '{name}' per step, fill + traceback at the "
-                                       f"kept precision, on {threads} threads"},
+                             "sample": f"the first {sample.size} of the {pairs.size} pairs of '{name}' "
+                                       f"(seed {args.seed}, the device arm's pairs) per step, fill + traceback "
+                                       f"at the kept precision, on {threads} threads"},
             "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "alignments_per_s": round(pairs.size * args.steps / t, 1)}
+            "alignments_per_s": round(sample.size * args.steps / t, 1)}
+    if kind == "reference" and os.path.exists(oracle.REF_LIB_NOFLUSH):
+        nf = oracle.reference(noflush=True)
+        nf.init(0)
+        nf.set_genome(blocks, None, genome.size)
+        s2, _ = nf.bench(sample, arena, threads, kept)
+        line["strong_cpu"] = {"value": round(cells / s2 / 1e9, 4), "unit": "GCUPS", "cores": threads,
+                              "build": "the reference with the per-column _mm_clflush compiled out, same sample"}
     print(json.dumps(line), flush=True)
+
+
+def kernel_cells(pairs, kernel, ctx):
+    """In-band cells of the pairs a fill kernel group fills in one step:
+    the kernel's variant; its pass (16-bit kinds fill the 16-bit pairs and
+    the 16-bit pass of every rerun pair); pairs with fewer lanes (query
+    rows; lower: genome columns) than warp_min_x go one thread per pair
+    (fill_thread), the others to lane groups or CTAs."""
+    variant = {"full": gdp.FULL, "upper": gdp.UPPER, "lower": gdp.LOWER}[kernel.split(",")[1]]
+    rerun = ((pairs["precision"] == 8) & ((pairs["flags"] & gdp.FLAG_RERUN16) != 0))
+    if "W16" in kernel:
+        sel = (pairs["precision"] == 16) | rerun
+    elif "8bit-check" in kernel:
+        sel = rerun   # at most: the pass runs only where the 16-bit pass left it open
+    else:
+        sel = (pairs["precision"] == 8) & ~rerun
+    lanes = np.where(pairs["variant"] == gdp.LOWER, pairs["glength"], pairs["rlength"])
+    thread = lanes < ctx.get_param("warp_min_x")
+    sel &= (pairs["variant"] == variant) & (thread if kernel.startswith("fill_thread") else ~thread)
+    return int(gdp.band_cells(pairs[sel]).sum())
 
 
 def run_gdp(args):
@@ -566,16 +742,28 @@ def run_gdp(args):
     torch.cuda.set_device(local)
     lib = gdp.load()
     name = args.workload
+    kind = WORKLOADS[name][0]
     npairs = args.npairs or WORKLOADS[name][1]
     genome, blocks, pairs, arena = make_workload(lib, name, npairs, args.seed + 1000 * rank)
     cells = int(gdp.band_cells(pairs).sum())
     ctx = gdp.Context(lib, device=local)
     ctx.set_genome(blocks, None, genome.size)
 
-    # resident inputs and outputs
+    # routing parameters from the autotuner, on a separate draw of the
+    # workload of the batch's own size (which routing wins depends on how
+    # many pairs each kind holds)
+    tuned = None
+    if not args.no_autotune:
+        tp, ta = gdp.make_pairs(lib, kind, args.seed + 77 + 1000 * rank, genome, min(args.tune_pairs or npairs, npairs))
+        params, best = ctx.autotune(tp, ta)
+        tuned = {"sample_pairs": int(tp.size), "params": params, "sample_ms": round(best, 3)}
+        del tp, ta
+
+    # resident inputs and outputs; the plan runs as a CUDA graph
     plan = ctypes.c_void_p()
     rc = lib.gdp_plan_create(ctx.h, gdp._ptr(pairs), pairs.size, ctypes.byref(plan))
     assert rc == 0, ctx.error()
+    lib.gdp_plan_use_graph(plan, 1)
     total_recs = int(lib.gdp_plan_total_recs(plan))
     d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
     d_arena = torch.from_numpy(arena).cuda()
@@ -590,15 +778,13 @@ def run_gdp(args):
                                   ctypes.c_void_p(d_recs.data_ptr()))
         assert rc == 0, ctx.error()
 
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 2)):
         step()
     lib.gdp_sync(ctx.h)
     res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
     bad = int((res["status"] != 0).sum())
 
     sampler = ClockSampler(local)
-    ctx.profile(True)
-    ctx.profile_reset()
     barrier(world)
     torch.cuda.synchronize()
     launches0 = ctx.launches()
@@ -614,23 +800,41 @@ def run_gdp(args):
     launches = ctx.launches() - launches0
     barrier(world)
     ms = t0.elapsed_time(t1)
-    prof = ctx.profile_read()
-    ctx.profile(False)
     ms_max = max_over_ranks(world, ms)
     total_cells = sum_over_ranks(world, float(cells))
     total_pairs = sum_over_ranks(world, float(pairs.size))
     value = total_cells * args.steps / (ms_max * 1e-3) / 1e9
 
-    # dominant kernel and its roofline (integer issue bound)
-    top = max(prof.items(), key=lambda kv: kv[1][0])
-    top_name, (top_ms, top_n) = top
-    avg_launch_ms = top_ms / top_n
+    # per-kernel device times: the same K steps once more with CUDA events
+    # around every launch (the profiled launches run without the graph)
+    ctx.profile(True)
+    ctx.profile_reset()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(args.steps):
+        step()
+    p1.record(stream)
+    p1.synchronize()
+    prof_ms = p0.elapsed_time(p1)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    # the dominant kernel: one fill body, instantiated once per tie rule
+    # (jump late / early); its two instantiations fill disjoint halves of
+    # the batch and are counted together
+    groups = {}
+    for k, (kms, kn) in prof.items():
+        g = k.replace(",early,", ",*,").replace(",late,", ",*,")
+        tot, n_launch, members = groups.get(g, (0.0, 0, []))
+        groups[g] = (tot + kms, n_launch + kn, members + [k])
+    top_name, (top_ms, top_n, top_members) = max(groups.items(), key=lambda kv: kv[1][0])
+    avg_launch_ms = top_ms / args.steps          # the group's device time per step
     int_peak = ctx.int_peak()
-    achieved_ops = cells * OPS_PER_CELL / (avg_launch_ms * 1e-3)
+    top_cells = kernel_cells(pairs, top_name, ctx)
+    achieved_ops = top_cells * OPS_PER_CELL / (avg_launch_ms * 1e-3)
     dir_bytes = int(lib.gdp_plan_dir_bytes(plan))
 
     # end to end through the host-buffer C ABI call, inputs and outputs in pinned host memory
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = max(1, args.e2e_steps)
 
     def pinned_like(arr):
         t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -665,13 +869,23 @@ def run_gdp(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(lib, name, args.seed, args.cpu_seconds)
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = cpu_leg(pairs, arena, blocks, genome.size, args.cpu_seconds, res=results,
+                      recs=recs[:int(used.value)])
 
     lib.gdp_plan_destroy(plan)
+    del d_pairs, d_arena, d_res, d_recs
+    torch.cuda.empty_cache()
     extra = {}
+    if rank == 0 and world == 1 and not args.no_configs:
+        cfg_genome = (genome, blocks)
+        extra["config1_fixed"] = measure_config(lib, ctx, "config1", "fixed", 10_000, args.seed + 11, 10_000,
+                                                args.cpu_seconds / 3, cfg_genome, per_pair=500)
+        extra["config3_cdna"] = measure_config(lib, ctx, "config3", "cdna", 100_000, args.seed + 13, 100_000,
+                                               args.cpu_seconds, cfg_genome)
+        extra["config4_mix"] = measure_config(lib, ctx, "config4", "mix", args.mix_pairs, args.seed + 14,
+                                              100_000, args.cpu_seconds, cfg_genome, tune_pairs=100_000,
+                                              per_pair=1000)
     if rank == 0 and world == 1 and not args.no_per_pair:
-        extra["per_pair_vs_batched"] = per_pair_vs_batched(lib, ctx, args.seed + 7)
         extra["endpoint_search"] = endpoint_search(lib, ctx, args.seed + 9)
         extra["single_gap"] = single_gap_batch(lib, ctx, args.seed + 10)
     if rank == 0 and world == 1 and not args.no_serving:
@@ -688,9 +902,9 @@ def run_gdp(args):
     # grow with the cells (directions and carries per swept cell)
     traffic, traffic_src = None, None
     if name == "short" and top_name.startswith("fill_thread<W16,full"):
-        traffic = int(round((123.696896e6 + 266.455296e6) / 300657762 * cells))
+        traffic = int(round((123.696896e6 + 266.455296e6) / 300657762 * top_cells))
         traffic_src = ("ncu capture of this kernel on 50,000 pairs (390.2 MB), scaled by in-band cells "
-                       "to this launch")
+                       "to one step's launches")
     if rank == 0:
         line = {
             "metric": "GCUPS (in-band cells, fill + traceback), batched",
@@ -701,26 +915,33 @@ def run_gdp(args):
             "config": {"workload": name, "pairs_per_gpu": int(pairs.size), "description": WORKLOADS[name][2],
                        "cells_per_gpu": cells, "l2": "inputs larger than L2 (sequence arena %.0f MB, "
                        "direction words %.0f MB per step)" % (arena.nbytes / 1e6, dir_bytes / 1e6),
-                       "parallelism": f"pairs sharded, {world} independent rank(s)"},
+                       "parallelism": f"pairs sharded, {world} independent rank(s)",
+                       "graph": True, "autotune": tuned},
             "alignments_per_s": round(total_pairs * args.steps / (ms_max * 1e-3), 1),
             "e2e": {"value": round(e2e_value, 3), "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3), "steps": e2e_steps,
                     "host_buffers": "pinned", "bad_status_pairs": e2e_bad},
-            "roofline": {"bound": "int", "kernel": top_name,
+            "roofline": {"bound": "int", "kernel": top_name, "instantiations": top_members,
+                         "cells_per_step": int(top_cells),
                          "achieved": round(achieved_ops / 1e12, 3), "peak": round(int_peak / 1e12, 3),
                          "unit": "Tops/s (int32 lane-ops)", "frac": round(achieved_ops / int_peak, 4),
                          "peak_source": "measured int32 issue probe (gdp_measure_int_peak)",
-                         "ops_per_cell": OPS_PER_CELL, "avg_launch_ms": round(avg_launch_ms, 3),
+                         "ops_per_cell": OPS_PER_CELL, "ms_per_step": round(avg_launch_ms, 3),
+                         "kernel_times": "a profiled pass of the same K steps right after the timed region "
+                                         "(CUDA events around every launch, on the launching stream)",
                          "traffic": traffic,
                          "traffic_source": traffic_src,
                          "dir_write_gbs": round(dir_bytes / (avg_launch_ms * 1e-3) / 1e9, 1),
                          "hbm_peak_gbs": hbm},
             "kernels": {k: {"ms_total": round(v[0], 3), "launches": v[1]} for k, v in prof.items()},
+            "profiled_ms_per_step": round(prof_ms / args.steps, 3),
             "gpu_launches": int(launches),
             "clocks": clocks,
             "bad_status_pairs": bad,
             "cpu_baseline": cpu,
         }
+        if cpu is not None and "parity" in cpu:
+            line["parity"] = cpu["parity"]
         line.update(extra)
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -738,9 +959,15 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="short")
     ap.add_argument("--npairs", type=int, default=0)
     ap.add_argument("--seed", type=int, default=1002)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=90.0,
+                    help="reference arm: total CPU seconds of the timed steps")
+    ap.add_argument("--tune-pairs", type=int, default=0, help="autotuner sample (0: the batch's size)")
+    ap.add_argument("--mix-pairs", type=int, default=2_000_000)
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--no-per-pair", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()

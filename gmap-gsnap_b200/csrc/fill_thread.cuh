@@ -428,9 +428,11 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
     r->score = final_score;
     r->precision = W == 16 ? 16 : 8;
     r->rerun = (MODE == 1) ? 1 : 0;
-    /* an end-gap half needs no final cell: the lower matrix of a gap with
-       glength > rlength, for one, holds none (score stays NEG_INFINITY) */
-    if (!swept && eb == nullptr) r->status = GDP_ERR_BAND;
+    /* only a traceback needs the final cell: an end-gap half, or the
+       lower fill of a gap with glength > rlength (a cDNA gap's lower
+       half), holds none and keeps GDP_OK with score NEG_INFINITY, the
+       cell the reference leaves unwritten */
+    if (!swept && eb == nullptr && (P.pairs[pi].flags & GDP_FLAG_TRACEBACK)) r->status = GDP_ERR_BAND;
     if (eb != nullptr) {
       r->end_score = eb->score;
       r->end_r = eb->r;

@@ -13,10 +13,16 @@
  *   long    rlength U{1000..10000}, lband/uband U{50..200}, 3% subs,
  *           1% indels (16-bit)
  *   cdna    rlength log-U[200, 5000], glength = rlength * U(1.0, 1.5),
- *           1% subs, 2% indels of geometric length (mean 4); upper fill with
- *           uband = glength - rlength + 14 (src/dynprog.c:1246-1261 wideband
- *           with extraband_paired = 14, src/gmap.c:292)
+ *           1% subs, 2% indels of geometric length (mean 4); an upper fill
+ *           with uband = glength - rlength + 14 (src/dynprog.c:1246-1261
+ *           wideband with extraband_paired = 14, src/gmap.c:292) traced back
+ *           from (rlength, glength), followed by the lower fill of the same
+ *           sequences with lband = 14 and no traceback, as a cDNA gap fills
+ *           both halves (src/dynprog_cdna.c:944-1098); the lower fill takes
+ *           the next slot of the batch
  * Gap penalties default to HIGHQ open -8 / extend -3 (src/dynprog.h:61-65).
+ * Draws alternate the tie rule: even draws jump late, odd draws jump early
+ * (jump_late_p), so both fills of every kind are exercised.
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -377,6 +383,27 @@ make_pair_resident (rng_t *r, int kind, const char *genome, int64_t glen_total,
 }
 
 /*
+ * Completes draw `draw` whose first fill is pairs[i]: odd draws jump early;
+ * a cDNA draw appends the lower fill of the same sequences (lband 14, no
+ * traceback) in the next slot when there is one.  Returns the index of the
+ * draw's last fill.
+ */
+static int64_t
+finish_draw (gdp_pair_t *pairs, int64_t i, int64_t npairs, int kind, int64_t draw) {
+  if (draw & 1) pairs[i].flags = (int8_t) (pairs[i].flags & ~GDP_FLAG_JUMP_LATE);
+  if (kind == WL_CDNA && i + 1 < npairs) {
+    gdp_pair_t *lo = &pairs[i + 1];
+    *lo = pairs[i];
+    lo->variant = GDP_LOWER;
+    lo->lband = 14;
+    lo->uband = 0;
+    lo->flags = (int8_t) (lo->flags & ~GDP_FLAG_TRACEBACK);
+    return i + 1;
+  }
+  return i;
+}
+
+/*
  * Like gdp_workload_pairs, with every genome window a slice of `genome`
  * and flagged GDP_FLAG_GWINDOW (genomeoffset = the slice's first position,
  * chroffset 0, chrhigh genome_length, plus strand).  The window bytes are
@@ -388,7 +415,7 @@ gdp_workload_resident_pairs (int kind, uint64_t seed, const char *genome, int64_
                              int64_t npairs, gdp_pair_t *pairs, char *arena, int64_t arena_cap,
                              int64_t *arena_used) {
   rng_t r;
-  int64_t i, off = 0;
+  int64_t i, off = 0, draw = 0;
   rng_seed(&r, seed);
   for (i = 0; i < npairs; i++) {
     int k = kind;
@@ -400,6 +427,7 @@ gdp_workload_resident_pairs (int kind, uint64_t seed, const char *genome, int64_
     used = make_pair_resident(&r, k, genome, genome_length, &pairs[i], arena, off, arena_cap);
     if (used < 0) break;
     off += (used + 15) & ~(int64_t) 15;
+    i = finish_draw(pairs, i, npairs, k, draw++);
   }
   if (arena_used) *arena_used = off;
   return i;
@@ -416,7 +444,7 @@ gdp_workload_pairs (int kind, uint64_t seed, const char *genome, int64_t genome_
                     int64_t npairs, gdp_pair_t *pairs, char *arena, int64_t arena_cap,
                     int64_t *arena_used) {
   rng_t r;
-  int64_t i, off = 0;
+  int64_t i, off = 0, draw = 0;
   rng_seed(&r, seed);
   for (i = 0; i < npairs; i++) {
     int k = kind;
@@ -428,6 +456,7 @@ gdp_workload_pairs (int kind, uint64_t seed, const char *genome, int64_t genome_
     used = make_pair(&r, k, genome, genome_length, &pairs[i], arena, off, arena_cap);
     if (used < 0) break;
     off += (used + 15) & ~(int64_t) 15;
+    i = finish_draw(pairs, i, npairs, k, draw++);
   }
   if (arena_used) *arena_used = off;
   return i;

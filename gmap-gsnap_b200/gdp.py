@@ -144,6 +144,53 @@ def load(path=LIB_PATH):
     return lib
 
 
+WORKLOAD_LIB_PATH = os.path.join(HERE, "lib", "libgdpwl.so")
+
+
+def load_workload(path=WORKLOAD_LIB_PATH):
+    """Loads libgdpwl.so, the seeded workload generator alone (no CUDA):
+    make_genome / make_pairs / make_resident_pairs accept it in place of
+    libgdp.so, so a process that only runs CPU code generates the same
+    pairs without loading the CUDA library."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"libgdpwl.so not built at {path}: run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    lib.gdp_workload_genome.argtypes = [ctypes.c_uint64, vp, i64]
+    lib.gdp_workload_genomecomp.argtypes = [vp, i64, vp]
+    lib.gdp_workload_pairs.argtypes = [i32, ctypes.c_uint64, vp, i64, i64, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_workload_pairs.restype = i64
+    lib.gdp_workload_resident_pairs.argtypes = lib.gdp_workload_pairs.argtypes
+    lib.gdp_workload_resident_pairs.restype = i64
+    lib.gdp_pair_cells.argtypes = [vp]
+    lib.gdp_pair_cells.restype = i64
+    return lib
+
+
+def record_digests(recs, offsets, counts):
+    """Per pair, a 32-bit digest of its Pair records in push order (the
+    same digest oracle/ computes for the reference's records): the sum over
+    records k of (w0 * 0x9E3779B1 + w1 * 0x85EBCA77 + w2 * 0xC2B2AE3D + 1) *
+    (2k + 1) mod 2^32, w0..w2 the record's three little-endian words."""
+    counts = np.asarray(counts, dtype=np.int64)
+    offsets = np.asarray(offsets, dtype=np.int64)
+    out = np.zeros(counts.size, dtype=np.uint32)
+    tot = int(counts.sum())
+    if tot == 0:
+        return out
+    seg = np.repeat(np.arange(counts.size), counts)
+    first = np.repeat(np.cumsum(counts) - counts, counts)
+    k = np.arange(tot, dtype=np.int64) - first
+    idx = np.repeat(offsets, counts) + k
+    w = np.ascontiguousarray(recs).view(np.uint32).reshape(-1, 3)[idx].astype(np.uint64)
+    m = np.uint64(0xFFFFFFFF)
+    h = (w[:, 0] * np.uint64(0x9E3779B1) + w[:, 1] * np.uint64(0x85EBCA77) +
+         w[:, 2] * np.uint64(0xC2B2AE3D) + np.uint64(1)) & m
+    h = (h * (2 * k.astype(np.uint64) + np.uint64(1))) & m
+    np.add.at(out, seg, h.astype(np.uint32))
+    return out
+
+
 def endpoint_combine(lib, upper, lower, jump_late, qend, precision, rlength):
     """The reference's (finalscore, bestr, bestc) of one end gap from the
     results of its upper and lower halves (gdp_endpoint_combine)."""

@@ -158,7 +158,8 @@ typedef struct gdp_rec {
 /* Per-pair result. */
 typedef struct gdp_result {
   int32_t status;        /* GDP_OK or GDP_ERR_* */
-  int32_t score;         /* matrix[glength][rlength] (lower: matrix[rlength][glength]) */
+  int32_t score;         /* matrix[glength][rlength] (lower: matrix[rlength][glength]); NEG_INFINITY_8/16
+                            when that cell lies outside the band of a fill without traceback */
   int32_t precision;     /* 8 or 16: the precision whose outputs were kept */
   int32_t rerun;         /* 1 if an 8-bit fill overflowed and was rerun in 16 bits */
   int32_t tb_score, nmatches, nmismatches, nopens, nindels;  /* traceback totals */

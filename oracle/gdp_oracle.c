@@ -645,36 +645,67 @@ typedef struct {
   const gdp_pair_t *pairs; const char *arena; int64_t n; int tid, nt; int64_t sum;
   const int8_t *kept_in;
   int8_t *kept_out;
+  int32_t *out;      /* orc_outputs: 8 words per pair, else NULL */
 } job_t;
+
+/* 32-bit digest of n Pair records in push order, as the reference harness
+   and the benchmark compute it: the sum over records k of (w0 *
+   0x9E3779B1 + w1 * 0x85EBCA77 + w2 * 0xC2B2AE3D + 1) * (2k + 1). */
+static uint32_t
+rec_digest (const gdp_rec_t *recs, int n) {
+  uint32_t d = 0;
+  int k;
+  for (k = 0; k < n; k++) {
+    uint32_t w[3];
+    memcpy(w, &recs[k], sizeof(w));
+    d += (w[0] * 0x9E3779B1u + w[1] * 0x85EBCA77u + w[2] * 0xC2B2AE3Du + 1u) * (uint32_t) (2 * k + 1);
+  }
+  return d;
+}
 
 static void *
 worker (void *arg) {
   job_t *j = (job_t *) arg;
   int64_t i;
+  gdp_rec_t *recs = NULL;
+  int cap = 0;
   for (i = j->tid; i < j->n; i += j->nt) {
     const gdp_pair_t *p = &j->pairs[i];
+    gdp_pair_t q;
     int32_t fs = 0, st[6] = {0};
+    int n = 0;
     if (j->kept_out) {
       j->kept_out[i] = (int8_t) kept_precision(p, j->arena);
       continue;
     }
     if (p->precision == 8 && (p->flags & GDP_FLAG_RERUN16)) {
       /* only the kept precision runs */
-      gdp_pair_t q = *p;
+      q = *p;
       q.flags &= ~GDP_FLAG_RERUN16;
       q.precision = j->kept_in ? j->kept_in[i] : 16;
-      orc_align(&q, j->arena, NULL, NULL, NULL, NULL, &fs, st, NULL, 0);
-    } else {
-      orc_align(p, j->arena, NULL, NULL, NULL, NULL, &fs, st, NULL, 0);
+      p = &q;
     }
+    if (j->out && (p->flags & GDP_FLAG_TRACEBACK) && p->rlength + p->glength + 8 > cap) {
+      free(recs);
+      cap = 2 * (p->rlength + p->glength + 8);
+      recs = (gdp_rec_t *) malloc((size_t) cap * sizeof(gdp_rec_t));
+    }
+    n = orc_align(p, j->arena, NULL, NULL, NULL, NULL, &fs, st, j->out ? recs : NULL, j->out ? cap : 0);
     j->sum += fs + st[0];
+    if (j->out) {
+      int32_t *w = j->out + 8 * i;
+      w[0] = fs;
+      memcpy(w + 1, st, sizeof(st));
+      w[7] = (p->flags & GDP_FLAG_TRACEBACK) ? (int32_t) rec_digest(recs, n < cap ? n : cap) : 0;
+    }
   }
+  free(recs);
   return NULL;
 }
 
 static double
 run_jobs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int64_t *checksum,
-          const int8_t *kept_in, int8_t *kept_out) {
+          const int8_t *kept_in, int8_t *kept_out, int32_t *out) {
   pthread_t *th;
   job_t *jobs;
   struct timespec t0, t1;
@@ -688,6 +719,7 @@ run_jobs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthrea
   for (t = 0; t < nthreads; t++) {
     jobs[t].pairs = pairs; jobs[t].arena = arena; jobs[t].n = npairs; jobs[t].tid = t;
     jobs[t].nt = nthreads; jobs[t].sum = 0; jobs[t].kept_in = kept_in; jobs[t].kept_out = kept_out;
+    jobs[t].out = out;
     pthread_create(&th[t], NULL, worker, &jobs[t]);
   }
   for (t = 0; t < nthreads; t++) { pthread_join(th[t], NULL); sum += jobs[t].sum; }
@@ -705,12 +737,21 @@ run_jobs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthrea
 double
 orc_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int64_t *checksum,
            const int8_t *kept) {
-  return run_jobs(pairs, arena, npairs, nthreads, checksum, kept, NULL);
+  return run_jobs(pairs, arena, npairs, nthreads, checksum, kept, NULL, NULL);
+}
+
+/* The same run, keeping per pair 8 words: the final score, the traceback
+   score, nmatches, nmismatches, nopens, nindels, the record count and the
+   records' digest (rec_digest; 0 without a traceback). */
+double
+orc_outputs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, const int8_t *kept,
+             int32_t *out) {
+  return run_jobs(pairs, arena, npairs, nthreads, NULL, kept, NULL, out);
 }
 
 /* kept[i] = the precision the rerun contract keeps for pair i, computed on
    nthreads threads. */
 void
 orc_kept_precision (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, int8_t *kept) {
-  run_jobs(pairs, arena, npairs, nthreads, NULL, NULL, kept);
+  run_jobs(pairs, arena, npairs, nthreads, NULL, NULL, kept, NULL);
 }

@@ -56,6 +56,10 @@ class CpuOracle:
         self._bench = getattr(self.lib, prefix + "bench")
         self._bench.argtypes = [vp, vp, i64, i32, ctypes.POINTER(i64), vp]
         self._bench.restype = ctypes.c_double
+        self._outputs = getattr(self.lib, prefix + "outputs", None)
+        if self._outputs is not None:
+            self._outputs.argtypes = [vp, vp, i64, i32, vp, vp]
+            self._outputs.restype = ctypes.c_double
         self._pd = getattr(self.lib, prefix + "pairdistance")
         self._pd.argtypes = [i32, i32, i32]
         self._cons = getattr(self.lib, prefix + "consistent")
@@ -94,6 +98,18 @@ class CpuOracle:
                            _ptr(final), _ptr(stats), _ptr(recs), max_recs)
         return {"score": int(final[0]), "H": H, "dN": dN, "dE": dE, "dF": dF,
                 "stats": stats, "recs": recs[:min(nrec, max_recs)], "nrecs": nrec}
+
+    def outputs(self, pairs, arena, nthreads, kept=None):
+        """Every pair once on nthreads threads, as bench() runs them, with
+        its outputs: an (n, 8) int32 array of the final score, traceback
+        score, nmatches, nmismatches, nopens, nindels, record count and the
+        records' 32-bit digest (gdp.record_digests computes the same digest
+        of the device's records).  Returns (seconds, outputs)."""
+        out = np.zeros((pairs.size, 8), dtype=np.int32)
+        if kept is not None:
+            kept = np.ascontiguousarray(kept, dtype=np.int8)
+        secs = self._outputs(_ptr(pairs), _ptr(arena), pairs.size, nthreads, _ptr(kept), _ptr(out))
+        return secs, out
 
     def bench(self, pairs, arena, nthreads, kept=None):
         """Wall seconds and a score checksum for every pair once on nthreads
@@ -137,6 +153,19 @@ class ReferenceSingleGap:
 
     def setup(self, user_open=0, user_extend=0, user_dynprog_p=False):
         self.lib.ref_single_setup(user_open, user_extend, int(user_dynprog_p))
+
+    def bench(self, gaps, arena, nthreads, maxlookback, extraquerygap):
+        """Wall seconds and a checksum of Dynprog_single_gap over every gap
+        once on nthreads threads, each with its own Dynprog_T (sized by
+        maxlookback / extraquerygap) and Pairpool_T."""
+        lib = self.lib
+        lib.ref_single_gap_bench.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+        lib.ref_single_gap_bench.restype = ctypes.c_double
+        cs = ctypes.c_int64(0)
+        secs = lib.ref_single_gap_bench(_ptr(gaps), gaps.size, _ptr(arena), nthreads, maxlookback, extraquerygap,
+                                        ctypes.byref(cs))
+        return secs, cs.value
 
     def run(self, gaps, arena):
         """Per gap: stats (traceback_score, nmatches, nmismatches, nopens,

@@ -383,19 +383,40 @@ typedef struct {
   int64_t npairs;
   int tid, nthreads;
   int64_t checksum;
+  int32_t *out;      /* ref_outputs: 8 words per pair, else NULL */
 } benchjob_t;
+
+/* 32-bit digest of n Pair records in push order: the sum over records k
+   of (w0 * 0x9E3779B1 + w1 * 0x85EBCA77 + w2 * 0xC2B2AE3D + 1) * (2k + 1),
+   w0..w2 the record's three words (the benchmark computes the same digest
+   of the device's records). */
+static uint32_t
+rec_digest (const gdp_rec_t *recs, int n) {
+  uint32_t d = 0;
+  int k;
+  for (k = 0; k < n; k++) {
+    uint32_t w[3];
+    memcpy(w, &recs[k], sizeof(w));
+    d += (w[0] * 0x9E3779B1u + w[1] * 0x85EBCA77u + w[2] * 0xC2B2AE3Du + 1u) * (uint32_t) (2 * k + 1);
+  }
+  return d;
+}
 
 static void *
 bench_worker (void *arg) {
   benchjob_t *job = (benchjob_t *) arg;
   refstate_t st;
   int64_t i, sum = 0;
+  gdp_rec_t *recs = NULL;
+  int cap = 0;
   memset(&st, 0, sizeof(st));
   for (i = job->tid; i < job->npairs; i += job->nthreads) {
     const gdp_pair_t *p = &job->pairs[i];
     gdp_pair_t q;
     fillout_t o;
-    int stats[6];
+    int stats[6] = {0, 0, 0, 0, 0, 0};
+    int fs;
+    uint32_t dig = 0;
     if (p->precision == 8 && (p->flags & GDP_FLAG_RERUN16)) {
       /* only the kept precision runs */
       q = *p;
@@ -404,15 +425,35 @@ bench_worker (void *arg) {
     }
     run_fill(&st, p, job->arena, &o);
     if (p->variant == GDP_LOWER) {
-      sum += get_cell(o.matrix, o.prec, p->rlength, p->glength);
+      fs = get_cell(o.matrix, o.prec, p->rlength, p->glength);
     } else {
-      sum += get_cell(o.matrix, o.prec, p->glength, p->rlength);
+      fs = get_cell(o.matrix, o.prec, p->glength, p->rlength);
     }
+    sum += fs;
     if (p->flags & GDP_FLAG_TRACEBACK) {
-      run_traceback(&st, p, job->arena, &o, stats, NULL, 0);
+      if (job->out) {
+        const int need = p->rlength + p->glength + 8;
+        int n;
+        if (need > cap) {
+          free(recs);
+          cap = 2 * need;
+          recs = (gdp_rec_t *) malloc((size_t) cap * sizeof(gdp_rec_t));
+        }
+        n = run_traceback(&st, p, job->arena, &o, stats, recs, cap);
+        dig = rec_digest(recs, n < cap ? n : cap);
+      } else {
+        run_traceback(&st, p, job->arena, &o, stats, NULL, 0);
+      }
       sum += stats[0];
     }
+    if (job->out) {
+      int32_t *w = job->out + 8 * i;
+      w[0] = fs;
+      memcpy(w + 1, stats, sizeof(stats));
+      w[7] = (int32_t) dig;
+    }
   }
+  free(recs);
   refstate_free(&st);
   job->checksum = sum;
   return NULL;
@@ -423,9 +464,9 @@ bench_worker (void *arg) {
    RERUN16 runs at the precision kept[i] only (16 when kept is NULL): the
    least work that gives the rerun contract's outputs, and never an 8-bit
    traceback that would read unwritten scratch. */
-double
-ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
-           int64_t *checksum, const int8_t *kept) {
+static double
+run_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
+           int64_t *checksum, const int8_t *kept, int32_t *out) {
   pthread_t *th;
   benchjob_t *jobs;
   struct timespec t0, t1;
@@ -438,7 +479,7 @@ ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthre
   clock_gettime(CLOCK_MONOTONIC, &t0);
   for (t = 0; t < nthreads; t++) {
     jobs[t].pairs = pairs; jobs[t].arena = arena; jobs[t].npairs = npairs; jobs[t].kept = kept;
-    jobs[t].tid = t; jobs[t].nthreads = nthreads;
+    jobs[t].tid = t; jobs[t].nthreads = nthreads; jobs[t].out = out;
     pthread_create(&th[t], NULL, bench_worker, &jobs[t]);
   }
   for (t = 0; t < nthreads; t++) {
@@ -450,4 +491,20 @@ ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthre
   free(jobs);
   if (checksum) *checksum = sum;
   return (double) (t1.tv_sec - t0.tv_sec) + 1e-9 * (double) (t1.tv_nsec - t0.tv_nsec);
+}
+
+double
+ref_bench (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads,
+           int64_t *checksum, const int8_t *kept) {
+  return run_bench(pairs, arena, npairs, nthreads, checksum, kept, NULL);
+}
+
+/* The same run, keeping per pair 8 words: the final score, the traceback
+   score, nmatches, nmismatches, nopens, nindels, the record count and the
+   records' digest (rec_digest; 0 without a traceback).  Returns wall
+   seconds. */
+double
+ref_outputs (const gdp_pair_t *pairs, const char *arena, int64_t npairs, int nthreads, const int8_t *kept,
+             int32_t *out) {
+  return run_bench(pairs, arena, npairs, nthreads, NULL, kept, out);
 }

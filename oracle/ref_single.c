@@ -20,6 +20,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <time.h>
 
 #include "dynprog.h"
 #include "dynprog_single.h"
@@ -173,4 +175,75 @@ ref_single_gap_batch (const gdp_single_gap_t *gaps, int n, const char *arena, in
     used += k;
   }
   return used;
+}
+
+/* ------------------------------------------------------------------ */
+/* CPU baseline: Dynprog_single_gap over a batch, one pthread per core   */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  const gdp_single_gap_t *gaps;
+  const char *arena;
+  int n, tid, nthreads, maxlookback, extraquerygap;
+  int64_t checksum;
+} singlejob_t;
+
+static void *
+single_worker (void *arg) {
+  singlejob_t *j = (singlejob_t *) arg;
+  /* each thread owns its Dynprog_T and Pairpool_T, as each GMAP worker
+     thread does (src/gmap.c:4907-4911) */
+  Dynprog_T dp = Dynprog_new(j->maxlookback, j->extraquerygap, 0, 0, 0, /*doublep*/false);
+  Pairpool_T pool = Pairpool_new();
+  int64_t sum = 0;
+  int i;
+  for (i = j->tid; i < j->n; i += j->nthreads) {
+    const gdp_single_gap_t *g = &j->gaps[i];
+    int dpi = g->dynprogindex, score = 0, nmatches = 0, nmismatches = 0, nopens = 0, nindels = 0;
+    List_T pairs;
+    Pairpool_reset(pool);
+    pairs = Dynprog_single_gap(&dpi, &score, &nmatches, &nmismatches, &nopens, &nindels, dp,
+                               (char *) j->arena + g->rseq, (char *) j->arena + g->rseq_uc, g->rlength,
+                               g->glength, g->roffset, g->goffset, (Univcoord_T) g->chroffset,
+                               (Univcoord_T) g->chrhigh, g->watsonp != 0, g->genestrand, g->jump_late_p != 0,
+                               ref_genome_main(), ref_genome_alt(), pool, g->extraband_single,
+                               g->widebandp != 0, g->defect_rate);
+    sum += score + List_length(pairs);
+  }
+  Pairpool_free(&pool);
+  Dynprog_free(&dp);
+  j->checksum = sum;
+  return NULL;
+}
+
+/* Dynprog_single_gap for every gap once, on nthreads threads (static
+   round-robin); returns wall seconds and a checksum of the traceback
+   scores and list lengths.  The user penalties of ref_single_setup
+   apply. */
+double
+ref_single_gap_bench (const gdp_single_gap_t *gaps, int n, const char *arena, int nthreads, int maxlookback,
+                      int extraquerygap, int64_t *checksum) {
+  pthread_t *th;
+  singlejob_t *jobs;
+  struct timespec t0, t1;
+  int64_t sum = 0;
+  int t;
+  if (nthreads < 1) nthreads = 1;
+  th = (pthread_t *) calloc(nthreads, sizeof(pthread_t));
+  jobs = (singlejob_t *) calloc(nthreads, sizeof(singlejob_t));
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (t = 0; t < nthreads; t++) {
+    jobs[t].gaps = gaps; jobs[t].arena = arena; jobs[t].n = n; jobs[t].tid = t; jobs[t].nthreads = nthreads;
+    jobs[t].maxlookback = maxlookback; jobs[t].extraquerygap = extraquerygap;
+    pthread_create(&th[t], NULL, single_worker, &jobs[t]);
+  }
+  for (t = 0; t < nthreads; t++) {
+    pthread_join(th[t], NULL);
+    sum += jobs[t].checksum;
+  }
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  free(th);
+  free(jobs);
+  if (checksum) *checksum = sum;
+  return (double) (t1.tv_sec - t0.tv_sec) + 1e-9 * (double) (t1.tv_nsec - t0.tv_nsec);
 }

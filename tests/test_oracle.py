@@ -143,3 +143,55 @@ def test_kept_precision_and_cpu_bench(restatement, gdplib):
         ref.set_genome(blocks, None, genome.size)
         _, cs_ref = ref.bench(pairs, arena, 3, kept)
         assert cs_ref == cs
+
+
+def test_outputs_and_record_digests(restatement, gdplib):
+    """The per-pair outputs the benchmark's parity sample compares: the
+    multi-threaded runs of the reference and of the restatement give the
+    same final score, traceback totals and record digest per pair, and the
+    digest equals gdp.record_digests over the records of a one-pair run (the
+    digest the benchmark computes for the device's records)."""
+    genome, blocks = gdp.make_genome(gdplib, 95, 1 << 20)
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_MIX, 96, genome, 60)
+    restatement.set_genome(blocks, None, genome.size)
+    kept = restatement.kept_precision(pairs, arena, 4)
+    _, out = restatement.outputs(pairs, arena, 3, kept)
+    for i in range(pairs.size):
+        q = pairs[i:i + 1].copy()
+        q["precision"] = kept[i]
+        q["flags"] = q["flags"] & ~gdp.FLAG_RERUN16
+        o = restatement.align(q, 0, arena, want_matrix=False)
+        assert out[i, 0] == o["score"], i
+        if q["flags"][0] & gdp.FLAG_TRACEBACK:
+            assert list(out[i, 1:7]) == list(o["stats"]), i
+            dig = gdp.record_digests(o["recs"], [0], [o["recs"].size])[0]
+            assert np.uint32(out[i, 7]) == dig, i
+    assert (pairs["variant"] == gdp.LOWER).any() and (pairs["variant"] == gdp.UPPER).any()
+    if orc.reference_available():
+        ref = orc.reference()
+        ref.set_genome(blocks, None, genome.size)
+        _, out_ref = ref.outputs(pairs, arena, 3, kept)
+        assert np.array_equal(out_ref, out)
+
+
+def test_workload_tie_rules_and_cdna_halves(gdplib):
+    """The seeded workloads alternate the tie rule by draw, and every cDNA
+    gap is an upper fill with a traceback followed by the lower fill of the
+    same sequences (lband 14, no traceback); the standalone generator
+    library gives the same pairs as libgdp.so."""
+    genome, _ = gdp.make_genome(gdplib, 97, 1 << 20)
+    pairs, arena = gdp.make_pairs(gdplib, gdp.WL_CDNA, 98, genome, 40)
+    up, lo = pairs[0::2], pairs[1::2]
+    assert (up["variant"] == gdp.UPPER).all() and (lo["variant"] == gdp.LOWER).all()
+    assert (lo["lband"] == 14).all() and (lo["uband"] == 0).all()
+    assert (up["flags"] & gdp.FLAG_TRACEBACK).all() and not (lo["flags"] & gdp.FLAG_TRACEBACK).any()
+    for k in ("rseq", "gseq", "rlength", "glength"):
+        assert np.array_equal(up[k], lo[k])
+    late = (up["flags"] & gdp.FLAG_JUMP_LATE) != 0
+    assert late[0::2].all() and not late[1::2].any()
+    short, _ = gdp.make_pairs(gdplib, gdp.WL_SHORT, 99, genome, 100)
+    assert ((short["flags"] & gdp.FLAG_JUMP_LATE) != 0).sum() == 50
+    wl = gdp.load_workload()
+    g2, _ = gdp.make_genome(wl, 97, 1 << 20)
+    p2, a2 = gdp.make_pairs(wl, gdp.WL_CDNA, 98, g2, 40)
+    assert p2.tobytes() == pairs.tobytes() and a2.tobytes() == arena.tobytes()
