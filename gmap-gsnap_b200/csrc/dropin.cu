@@ -315,16 +315,14 @@ fill_entry (const char *name, int precision, int variant, S ***dirN, S ***dirE, 
     for (int y = y0; y <= y1; y++) {
       const int64_t col = boff + (int64_t) (y - y0) * (W / 8);
       S *h = H[y] + xlo, *n = N[y] + xlo, *e = E[y] + xlo, *f = F ? F[y] + xlo : nullptr;
-      for (int j = 0; j < W / 8; j++) {
-        const uint32_t w = words[col + j];
-        const int16_t *sc = scores + (col + j) * 8;
-        for (int i = 0; i < 8; i++) {
-          const int lane = 8 * j + i;
-          h[lane] = (S) sc[i];
-          n[lane] = (S) (((w >> (8 + i)) & 1) ? DIR_VERT : ((w >> i) & 1) ? DIR_HORIZ : DIR_DIAG);
-          e[lane] = (S) (((w >> (16 + i)) & 1) ? DIR_HORIZ : DIR_DIAG);
-          if (f) f[lane] = (S) (((w >> (24 + i)) & 1) ? DIR_VERT : DIR_DIAG);
-        }
+      const int16_t *sc = scores + col * 8;   /* the column's scores, lane by lane */
+      for (int lane = 0; lane < W; lane++) {
+        const uint32_t w = words[col + gdp_dir_word(W, lane)];
+        const int i = gdp_dir_bit(W, lane);
+        h[lane] = (S) sc[lane];
+        n[lane] = (S) (((w >> (8 + i)) & 1) ? DIR_VERT : ((w >> i) & 1) ? DIR_HORIZ : DIR_DIAG);
+        e[lane] = (S) (((w >> (16 + i)) & 1) ? DIR_HORIZ : DIR_DIAG);
+        if (f) f[lane] = (S) (((w >> (24 + i)) & 1) ? DIR_VERT : DIR_DIAG);
       }
     }
     boff += gdp_block_words(&g, xlo);

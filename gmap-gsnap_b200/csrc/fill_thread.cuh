@@ -78,6 +78,11 @@ struct FillParams {
      pass (MODE 1) of a lower fill proves the 8-bit overflow only from
      127 + this slack. */
   uint32_t lower_slack4;
+  /* Full-band 16-bit pairs (plain fills and the 16-bit pass of rerun
+     pairs) with min(rlength, glength) at most this run the packed two-lane
+     fill (fill_packed.cuh); the others, and every pair when it is below 0,
+     the one-lane-per-register fill below. */
+  int packed_len;
 };
 
 /* Lanes lo..hi (0 <= lo <= hi <= 31) as a bit mask. */
@@ -351,8 +356,8 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
     }
     B.H[i] = Hn;
     B.E[i] = Ee;
-    if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
-    if (pN) w[i >> 3] |= 1u << (i & 7);
+    if (pE) w[gdp_dir_word(W, i)] |= 1u << (16 + gdp_dir_bit(W, i));
+    if (pN) w[gdp_dir_word(W, i)] |= 1u << gdp_dir_bit(W, i);
   }
   int2 out;
   if (VARIANT == GDP_FULL) {
@@ -372,8 +377,8 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
         B.H[i] = Hn;
         Hp = Hn;
         Fp = F;
-        if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
-        if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
+        if (pF) w[gdp_dir_word(W, i)] |= 1u << (24 + gdp_dir_bit(W, i));
+        if (pV) w[gdp_dir_word(W, i)] |= 1u << (8 + gdp_dir_bit(W, i));
       }
     }
     out = make_int2(B.H[W - 1], Fp);
@@ -412,7 +417,10 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
              const EndBest *eb = nullptr) {
   int y0l, y1l;
   gdp_block_sweep(&g, (g.X / W) * W, &y0l, &y1l);
-  const bool swept = (g.Y >= y0l && g.Y <= y1l);   /* the final cell was filled */
+  /* the final cell was filled: swept, and for the full band not above the
+     band's top (the lanes above the band are not kept once they leave it) */
+  const bool swept = (g.Y >= y0l && g.Y <= y1l) && !(g.variant == GDP_FULL && g.Y - g.X > g.uband);
+  if (!swept) final_score = (W == 32) ? -128 : -32768;
   if (MODE == 1) {
     mp->maxh16 = reached ? 127 : -32768;   /* >= 127 iff an in-band 16-bit score reached 127 */
     mp->final16 = final_score;
@@ -489,8 +497,8 @@ block_column_steady (Block<W> &B, const PairView &v, int diag, int2 above, int k
     bool pN;
     B.H[i] = tie_max<LATE>(Ee, Hv, pN);
     B.E[i] = Ee;
-    if (pE) w[i >> 3] |= 1u << (16 + (i & 7));
-    if (pN) w[i >> 3] |= 1u << (i & 7);
+    if (pE) w[gdp_dir_word(W, i)] |= 1u << (16 + gdp_dir_bit(W, i));
+    if (pN) w[gdp_dir_word(W, i)] |= 1u << gdp_dir_bit(W, i);
   }
   int2 out;
   if (VARIANT == GDP_FULL) {
@@ -504,8 +512,8 @@ block_column_steady (Block<W> &B, const PairView &v, int diag, int2 above, int k
       B.H[i] = Hn;
       Hp = Hn;
       Fp = F;
-      if (pF) w[i >> 3] |= 1u << (24 + (i & 7));
-      if (pV) w[i >> 3] |= 1u << (8 + (i & 7));
+      if (pF) w[gdp_dir_word(W, i)] |= 1u << (24 + gdp_dir_bit(W, i));
+      if (pV) w[gdp_dir_word(W, i)] |= 1u << (8 + gdp_dir_bit(W, i));
     }
     out = make_int2(B.H[W - 1], Fp);
   } else {
@@ -553,6 +561,8 @@ column_steady (const PairView &v, int xlo, int y) {
 #define GDP_FILL_MINB8 3
 #endif
 
+#include "fill_packed.cuh"
+
 /* MODE: 0 plain fill, 1 = 16-bit fill of a rerun pair (records whether an
    in-band score reaches 127), 2 = 8-bit pass of a rerun pair (skipped when
    the 16-bit pass proved an overflow; stops at the first in-band 127).
@@ -585,6 +595,12 @@ fill_thread_kernel (FillParams P) {
     v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
     if (MODE == 1 && VARIANT == GDP_LOWER) v.lim += (int) ((P.lower_slack4 >> (8 * (v.mt & 3))) & 255u);
     v.endmode = (VARIANT == GDP_FULL) ? 0 : (p.flags & GDP_FLAG_ENDPOINT) ? 1 : (p.flags & GDP_FLAG_ENDPOINT_QEND) ? 2 : 0;
+    if constexpr (W == 16 && VARIANT == GDP_FULL && MODE != 2) {
+      if (min(p.rlength, p.glength) <= P.packed_len) {
+        pair_fill_packed<LATE, MODE>(P, pi, mp, v, s_nt2int, slot);
+        continue;
+      }
+    }
     EndBest eb;
     eb.score = 0; eb.r = 0; eb.c = 0; eb.found = false;
     const int end_start = (v.endmode == 2) ? LO : 0;

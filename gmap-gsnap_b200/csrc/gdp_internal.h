@@ -8,13 +8,15 @@
  * Its traceback can read any cell such a sweep wrote -- including the
  * below-band cells of a block (src/dynprog_simd.c:9174 walks one column
  * past the band edge) -- so the device keeps every swept cell: for block b
- * and swept column y, W/8 consecutive uint32 words, word j covering lanes
- * xlo + 8j .. xlo + 8j + 7 with
+ * and swept column y, W/8 consecutive uint32 words with
  *     bits  0..7   nogap == HORIZ   (set by the vector step)
  *     bits  8..15  nogap == VERT    (set by the F loop; overrides HORIZ)
  *     bits 16..23  Egap  != DIAG
  *     bits 24..31  Fgap  == VERT
- * (bit i of each byte = lane xlo + 8j + i): 4 bits per cell.  Blocks are
+ * 4 bits per cell.  Which word and which bit of each byte hold lane i
+ * (gdp_dir_word, gdp_dir_bit): for W = 16, word i % 2, bit i / 2 (the
+ * even lanes in word 0, the odd lanes in word 1, as the packed two-lane
+ * fill produces them); for W = 32, word i / 8, bit i % 8.  Blocks are
  * stored one after another; block b starts at the sum of the sizes of
  * blocks 0..b-1.  "Lanes" are query rows for the full and upper fills and
  * genome columns for the lower fill (which the reference computes
@@ -34,6 +36,11 @@
 
 #define GDP_NEGINT (-32768)   /* NEG_INFINITY_INT (src/dynprog.h:176) */
 #define GDP_MICROINTRON 9     /* MICROINTRON_LENGTH (src/pairpool.c:18) */
+
+/* Word (of the W/8 words of a block column) and bit (of each byte) of
+   lane `lane`'s direction bits. */
+GDP_HD int gdp_dir_word (int W, int lane) { return W == 16 ? (lane & 1) : (lane >> 3); }
+GDP_HD int gdp_dir_bit (int W, int lane) { return W == 16 ? (lane >> 1) : (lane & 7); }
 
 /* Substitution and consistency tables, built on the host as Dynprog_init
    does (src/dynprog.c:1007-1196) and copied to the device. */

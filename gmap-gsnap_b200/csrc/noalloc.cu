@@ -67,6 +67,7 @@ static unsigned char *g_scratch_dev[GDP_NOALLOC_MAX_DEVICES];
 static gdp_tables_t *g_tables_dev[GDP_NOALLOC_MAX_DEVICES];
 static int g_tables_mode[GDP_NOALLOC_MAX_DEVICES];
 static bool g_ready[GDP_NOALLOC_MAX_DEVICES];
+static int g_packed_len[GDP_NOALLOC_MAX_DEVICES];
 static gdp_tables_t g_host_tables;   /* host staging for the one-time upload */
 
 /*
@@ -162,6 +163,7 @@ noalloc_setup (int device, int mode, unsigned char **scratch, gdp_tables_t **tab
     /* from pageable memory the copy may return before the DMA lands; a
        caller's non-blocking stream would not wait for it */
     if (cudaDeviceSynchronize() != cudaSuccess) return GDP_ERR_CUDA;
+    g_packed_len[device] = gdp_packed_len_of(&g_host_tables);
     g_scratch_dev[device] = (unsigned char *) ps;
     g_tables_dev[device] = (gdp_tables_t *) pt;
     g_tables_mode[device] = mode;
@@ -210,6 +212,7 @@ noalloc_run (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, co
   P.tab = tables;
   P.reach_from4 = 0;
   P.lower_slack4 = 0;
+  P.packed_len = g_packed_len[device];
   for (int late = 1; late >= 0; late--) {
     P.list = late ? list_late : list_early;
     P.count = counts + (late ? 0 : 1);

@@ -293,6 +293,7 @@ struct gdp_ctx {
   gdp_tables_t *d_tab = nullptr;
   int reach_from[4] = {0, 0, 0, 0};   /* FillParams::reach_from of h_tab */
   int lower_slack[4] = {0, 0, 0, 0};  /* FillParams::lower_slack4 of h_tab */
+  int packed_len = -1;                 /* FillParams::packed_len of h_tab */
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
@@ -408,6 +409,9 @@ update_reach (gdp_ctx *ctx) {
     }
     ctx->lower_slack[mt] = std::min(slack, 255);
   }
+  ctx->packed_len = gdp_packed_len_of(ctx->h_tab);
+  const char *pe = getenv("GDP_PACKED");   /* 0: every pair on the one-lane-per-register fill */
+  if (pe && atoi(pe) == 0) ctx->packed_len = -1;
 }
 
 static int
@@ -1329,6 +1333,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.tab = ctx->d_tab;
       P.reach_from4 = 0;
       P.lower_slack4 = 0;
+      P.packed_len = ctx->packed_len;
       for (int q = 0; q < 4; q++) {
         P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
         P.lower_slack4 |= (uint32_t) ctx->lower_slack[q] << (8 * q);
@@ -1921,8 +1926,8 @@ gdp_fill_dump (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *are
           const int64_t at = dense_offsets[i] + (int64_t) c * R + r;
           if (y < y0 || y > y1) continue;
           const int64_t col = base + boff[b] + (int64_t) (y - y0) * (W / 8);
-          const uint32_t w = words[col + (lane >> 3)];
-          const int sh = lane & 7;
+          const uint32_t w = words[col + gdp_dir_word(W, lane)];
+          const int sh = gdp_dir_bit(W, lane);
           const int nh = (w >> sh) & 1, nv = (w >> (8 + sh)) & 1, ee = (w >> (16 + sh)) & 1, ff = (w >> (24 + sh)) & 1;
           if (H) H[at] = hs[col * 8 + lane];
           if (dN) dN[at] = (int8_t) (nv ? -2 : nh ? -1 : 0);

@@ -71,8 +71,8 @@ struct DirCursor {
     if (nb != b) seek(nb);
     if (y < y0 || y > y1) return -1;
     const int lane = x - b * g.W;
-    const uint32_t w = __ldg(base + boff + (int64_t) (y - y0) * (g.W / 8) + (lane >> 3));
-    const int sh = lane & 7;
+    const uint32_t w = __ldg(base + boff + (int64_t) (y - y0) * (g.W / 8) + gdp_dir_word(g.W, lane));
+    const int sh = gdp_dir_bit(g.W, lane);
     return (int) (((w >> sh) & 1u) | (((w >> (8 + sh)) & 1u) << 1) |
                   (((w >> (16 + sh)) & 1u) << 2) | (((w >> (24 + sh)) & 1u) << 3));
   }

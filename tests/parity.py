@@ -44,6 +44,18 @@ def expected_precision(oracle, pairs, i, arena, restatement=None):
     return 8
 
 
+def final_cell_in_band(p):
+    """Whether pair p's final cell (rlength, glength) lies in its band.
+    Outside it the reference leaves the cell unwritten (the lower fill of a
+    gap with glength > rlength), so its "score" is whatever the scratch
+    held; the device reports NEG_INFINITY there."""
+    d = int(p["rlength"]) - int(p["glength"])
+    v = int(p["variant"])
+    lo = 0 if v == gdp.LOWER else -int(p["uband"])
+    hi = 0 if v == gdp.UPPER else int(p["lband"])
+    return lo <= d <= hi
+
+
 def check_fill(ctx, oracle, pairs, arena, max_report=5, production=False):
     """Fills every pair on the GPU and compares scores and directions over
     the reference's compare domain and the final score.  With
@@ -78,8 +90,11 @@ def check_fill(ctx, oracle, pairs, arena, max_report=5, production=False):
             if not np.array_equal(g[m], o[name][m]):
                 k = np.nonzero((g != o[name]) & m)[0][0]
                 bad.append(f"{name}@(c={k // (rl + 1)},r={k % (rl + 1)}) gpu {g[k]} cpu {o[name][k]}")
-        if int(res["score"][i]) != o["score"]:
-            bad.append(f"score gpu {res['score'][i]} cpu {o['score']}")
+        if final_cell_in_band(p):
+            if int(res["score"][i]) != o["score"]:
+                bad.append(f"score gpu {res['score'][i]} cpu {o['score']}")
+        elif int(res["score"][i]) != (-128 if prec == 8 else -32768):
+            bad.append(f"final cell outside the band: score gpu {res['score'][i]}, want NEG_INFINITY")
         if bad:
             fails.append(f"pair {i} var {p['variant']} prec {prec} r {rl} g {gl} l {p['lband']} "
                          f"u {p['uband']} flags {p['flags']}: " + "; ".join(bad[:3]))
@@ -121,7 +136,7 @@ def check_traceback(ctx, oracle, restatement, pairs, arena, max_report=5):
             fails.append(f"pair {i}: status {gdp.STATUS.get(st)}")
             continue
         bad = []
-        if int(res["score"][i]) != o["score"]:
+        if final_cell_in_band(p) and int(res["score"][i]) != o["score"]:
             bad.append(f"score {res['score'][i]} vs {o['score']}")
         got = [int(res[k][i]) for k in ("tb_score", "nmatches", "nmismatches", "nopens", "nindels", "nrecs")]
         if got != [int(v) for v in o["stats"]]:

@@ -47,8 +47,9 @@ def _decode(pairs, i, words, base):
         y0, y1 = sweeps[b]
         if not (y0 <= c <= y1):
             continue
-        w = int(words[base + boff[b] + (c - y0) * 2 + (lane >> 3)])
-        sh = lane & 7
+        # 16-lane columns: even lanes in word 0, odd lanes in word 1, bit lane // 2
+        w = int(words[base + boff[b] + (c - y0) * 2 + (lane & 1)])
+        sh = lane >> 1
         at = c * (rl + 1) + r
         dN[at] = -2 if (w >> (8 + sh)) & 1 else (-1 if (w >> sh) & 1 else 0)
         dE[at] = -1 if (w >> (16 + sh)) & 1 else 0
