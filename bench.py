@@ -732,7 +732,7 @@ def kernel_cells(pairs, kernel, ctx):
         sel = (pairs["precision"] == 8) & ~rerun
     lanes = np.where(pairs["variant"] == gdp.LOWER, pairs["glength"], pairs["rlength"])
     thread = lanes < ctx.get_param("warp_min_x")
-    sel &= (pairs["variant"] == variant) & (thread if kernel.startswith("fill_thread") else ~thread)
+    sel &= (pairs["variant"] == variant) & (thread if kernel.startswith(("fill_thread", "fill_packed")) else ~thread)
     return int(gdp.band_cells(pairs[sel]).sum())
 
 
@@ -901,7 +901,7 @@ def run_gdp(args):
     # cells), scaled to this launch by its in-band cells; the kernel's bytes
     # grow with the cells (directions and carries per swept cell)
     traffic, traffic_src = None, None
-    if name == "short" and top_name.startswith("fill_thread<W16,full"):
+    if name == "short" and top_name.startswith("fill_packed<W16,full"):
         traffic = int(round((123.696896e6 + 266.455296e6) / 300657762 * top_cells))
         traffic_src = ("ncu capture of this kernel on 50,000 pairs (390.2 MB), scaled by in-band cells "
                        "to one step's launches")

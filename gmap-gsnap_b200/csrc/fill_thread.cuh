@@ -80,8 +80,9 @@ struct FillParams {
   uint32_t lower_slack4;
   /* Full-band 16-bit pairs (plain fills and the 16-bit pass of rerun
      pairs) with min(rlength, glength) at most this run the packed two-lane
-     fill (fill_packed.cuh); the others, and every pair when it is below 0,
-     the one-lane-per-register fill below. */
+     fill (fill_packed_kernel, launched first for such a kind); the one-lane-
+     per-register fill_thread_kernel skips them and takes the others (every
+     pair when this is below 0). */
   int packed_len;
 };
 
@@ -596,10 +597,7 @@ fill_thread_kernel (FillParams P) {
     if (MODE == 1 && VARIANT == GDP_LOWER) v.lim += (int) ((P.lower_slack4 >> (8 * (v.mt & 3))) & 255u);
     v.endmode = (VARIANT == GDP_FULL) ? 0 : (p.flags & GDP_FLAG_ENDPOINT) ? 1 : (p.flags & GDP_FLAG_ENDPOINT_QEND) ? 2 : 0;
     if constexpr (W == 16 && VARIANT == GDP_FULL && MODE != 2) {
-      if (min(p.rlength, p.glength) <= P.packed_len) {
-        pair_fill_packed<LATE, MODE>(P, pi, mp, v, s_nt2int, slot);
-        continue;
-      }
+      if (min(p.rlength, p.glength) <= P.packed_len) continue;   /* fill_packed_kernel's */
     }
     EndBest eb;
     eb.score = 0; eb.r = 0; eb.c = 0; eb.found = false;

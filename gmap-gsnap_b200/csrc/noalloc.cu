@@ -217,10 +217,14 @@ noalloc_run (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, co
     P.list = late ? list_late : list_early;
     P.count = counts + (late ? 0 : 1);
     void *args[] = {(void *) &P};
-    const void *fn = late ? (const void *) fill_thread_kernel<16, GDP_FULL, true, 0>
-                          : (const void *) fill_thread_kernel<16, GDP_FULL, false, 0>;
-    if (cudaLaunchKernel(fn, dim3(GDP_NOALLOC_BLOCKS), dim3(GDP_NOALLOC_THREADS), args, 0, s) != cudaSuccess)
-      return GDP_ERR_CUDA;
+    /* the packed fill takes the pairs within its score range, the
+       one-lane-per-register fill the others */
+    const void *fns[2] = {late ? (const void *) fill_packed_kernel<true, 0> : (const void *) fill_packed_kernel<false, 0>,
+                          late ? (const void *) fill_thread_kernel<16, GDP_FULL, true, 0>
+                               : (const void *) fill_thread_kernel<16, GDP_FULL, false, 0>};
+    for (int f = (P.packed_len >= 0) ? 0 : 1; f < 2; f++)
+      if (cudaLaunchKernel(fns[f], dim3(GDP_NOALLOC_BLOCKS), dim3(GDP_NOALLOC_THREADS), args, 0, s) != cudaSuccess)
+        return GDP_ERR_CUDA;
   }
   return GDP_OK;
 }

@@ -199,6 +199,7 @@ struct PlanHost {
   int64_t start[NKINDS + 2] = {0};
   int32_t counts[NKINDS + 1] = {0};
   int maxY[NKINDS] = {0};
+  int maxMin[NKINDS] = {0};   /* per kind: the largest min(rlength, glength) */
   int64_t dir_words = 0, total_recs = 0;
   int64_t nwindow = 0;   /* pairs whose genome window the device extracts */
   /* planner scratch, kept from plan to plan (grown, never shrunk) */
@@ -364,7 +365,9 @@ kernel_name (int id) {
     return buf[id];
   }
   const int pass = id & 1, late = (id >> 1) & 1, vw = id >> 2, variant = vw % 3, w32 = vw / 3;
-  snprintf(buf[id], sizeof(buf[id]), "fill_thread<W%d,%s,%s,%s>", w32 ? 32 : 16,
+  /* full-band 16-bit thread kinds run the packed fill (fill_packed_kernel) */
+  snprintf(buf[id], sizeof(buf[id]), "%s<W%d,%s,%s,%s>", (!w32 && variant == 0) ? "fill_packed" : "fill_thread",
+           w32 ? 32 : 16,
            variant == 0 ? "full" : variant == 1 ? "upper" : "lower", late ? "late" : "early",
            pass ? (w32 ? "8bit-check" : "16bit-track") : "plain");
   return buf[id];
@@ -844,7 +847,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, n / 8192));
   /* per chunk: sums of direction words, record slots, fill entries,
      tracebacks, device windows, and the largest swept dimension per kind */
-  struct Chunk { int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0; int maxY[NKINDS] = {0}; };
+  struct Chunk { int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0; int maxY[NKINDS] = {0}, maxMin[NKINDS] = {0}; };
   std::vector<Chunk> ch(nt);
   uint32_t *k16 = grow(ph.k16, n), *k8 = grow(ph.k8, n);   /* fill keys of each pair (~0u: none) */
   const uint64_t glen = ctx->genome_len;
@@ -890,6 +893,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
         k16[i] = (uint32_t) k << KEY_KIND_SHIFT | work_key(p, 16);
         c.entries++;
         c.maxY[k] = std::max(c.maxY[k], Y);
+        c.maxMin[k] = std::max(c.maxMin[k], std::min(p.rlength, p.glength));
       }
       if (p.precision == 8) {
         int k = kind_id(1, p.variant, late, rerun ? 1 : 0);
@@ -912,6 +916,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
         k8[i] = (uint32_t) k << KEY_KIND_SHIFT | work_key(p, 32);
         c.entries++;
         c.maxY[k] = std::max(c.maxY[k], Y);
+        c.maxMin[k] = std::max(c.maxMin[k], std::min(p.rlength, p.glength));
       }
       if (p.flags & GDP_FLAG_TRACEBACK) {
         rec_off[i] = (int64_t) p.rlength + p.glength + 2;
@@ -924,11 +929,15 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   std::vector<int64_t> wbase(nt), rbase(nt), ebase(nt), tbase(nt);
   int64_t words = 0, recs = 0, entries = 0, ntb = 0, nwindow = 0;
   int maxY[NKINDS] = {0};
+  int maxMin[NKINDS] = {0};   /* per kind: the largest min(rlength, glength) */
   for (int t = 0; t < nt; t++) {
     wbase[t] = words; rbase[t] = recs; ebase[t] = entries; tbase[t] = ntb;
     words += ch[t].words; recs += ch[t].recs; entries += ch[t].entries; ntb += ch[t].ntb;
     nwindow += ch[t].nwindow;
-    for (int k = 0; k < NKINDS; k++) maxY[k] = std::max(maxY[k], ch[t].maxY[k]);
+    for (int k = 0; k < NKINDS; k++) {
+      maxY[k] = std::max(maxY[k], ch[t].maxY[k]);
+      maxMin[k] = std::max(maxMin[k], ch[t].maxMin[k]);
+    }
   }
   /* pass 2: sizes to offsets, fill entries in pair order */
   uint32_t *keys = grow(ph.keys, entries);
@@ -974,6 +983,7 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
     }
     ph.counts[k] = (int32_t) (pos - ph.start[k]);
     ph.maxY[k] = maxY[k];
+    ph.maxMin[k] = maxMin[k];
   }
   ph.start[NKINDS] = pos;
   ph.counts[NKINDS] = (int32_t) ntb;
@@ -1110,24 +1120,38 @@ compact_records_kernel (gdp_result_t *res, const int64_t *slot_off, const gdp_re
   }
 }
 
+/* A thread-per-pair kind.  Full-band 16-bit plain fills and 16-bit passes
+   run the packed fill first; the one-lane-per-register kernel follows only
+   when the kind holds pairs too long for it (their scores could pass the
+   packed range). */
 template <int W, int V, bool L, int M>
-static void launch_fill (FillParams P, int grid, cudaStream_t s) {
+static int launch_fill (FillParams P, int grid, cudaStream_t s, int max_min_len) {
+  if constexpr (W == 16 && V == GDP_FULL && M != 2) {
+    if (P.packed_len >= 0) {
+      fill_packed_kernel<L, M><<<grid, 128, 0, s>>>(P);
+      if (max_min_len <= P.packed_len) return 1;
+      fill_thread_kernel<W, V, L, M><<<grid, 128, 0, s>>>(P);
+      return 2;
+    }
+  }
   fill_thread_kernel<W, V, L, M><<<grid, 128, 0, s>>>(P);
+  return 1;
 }
 
-static void
-launch_kind (int k, FillParams P, int grid, cudaStream_t s) {
+/* Returns the number of kernels launched. */
+static int
+launch_kind (int k, FillParams P, int grid, cudaStream_t s, int max_min_len) {
   const int pass = k & 1, late = (k >> 1) & 1, vw = k >> 2, variant = vw % 3, w32 = vw / 3;
 #define GDP_CASE(W32, VAR, LATE)                                                                   \
   if (w32 == W32 && variant == VAR && late == LATE) {                                             \
-    if (W32) { if (pass) launch_fill<32, VAR, LATE, 2>(P, grid, s); else launch_fill<32, VAR, LATE, 0>(P, grid, s); } \
-    else { if (pass) launch_fill<16, VAR, LATE, 1>(P, grid, s); else launch_fill<16, VAR, LATE, 0>(P, grid, s); }     \
-    return;                                                                                        \
+    if (W32) return pass ? launch_fill<32, VAR, LATE, 2>(P, grid, s, max_min_len) : launch_fill<32, VAR, LATE, 0>(P, grid, s, max_min_len); \
+    return pass ? launch_fill<16, VAR, LATE, 1>(P, grid, s, max_min_len) : launch_fill<16, VAR, LATE, 0>(P, grid, s, max_min_len);          \
   }
   GDP_CASE(0, 0, false) GDP_CASE(0, 0, true) GDP_CASE(0, 1, false) GDP_CASE(0, 1, true)
   GDP_CASE(0, 2, false) GDP_CASE(0, 2, true) GDP_CASE(1, 0, false) GDP_CASE(1, 0, true)
   GDP_CASE(1, 1, false) GDP_CASE(1, 1, true) GDP_CASE(1, 2, false) GDP_CASE(1, 2, true)
 #undef GDP_CASE
+  return 0;
 }
 
 static inline int
@@ -1191,9 +1215,9 @@ launch_warp8_kind (int k, FillParams P, int grid, cudaStream_t s) {
 static void
 launch_early8_kind (int k, FillParams P, int grid, cudaStream_t s) {
   const int c = k - FIRST_EARLY8, variant = c / 2, late = c & 1;
-  if (variant == GDP_FULL) { if (late) launch_fill<32, GDP_FULL, true, 2>(P, grid, s); else launch_fill<32, GDP_FULL, false, 2>(P, grid, s); }
-  else if (variant == GDP_UPPER) { if (late) launch_fill<32, GDP_UPPER, true, 2>(P, grid, s); else launch_fill<32, GDP_UPPER, false, 2>(P, grid, s); }
-  else { if (late) launch_fill<32, GDP_LOWER, true, 2>(P, grid, s); else launch_fill<32, GDP_LOWER, false, 2>(P, grid, s); }
+  if (variant == GDP_FULL) { if (late) launch_fill<32, GDP_FULL, true, 2>(P, grid, s, 0); else launch_fill<32, GDP_FULL, false, 2>(P, grid, s, 0); }
+  else if (variant == GDP_UPPER) { if (late) launch_fill<32, GDP_UPPER, true, 2>(P, grid, s, 0); else launch_fill<32, GDP_UPPER, false, 2>(P, grid, s, 0); }
+  else { if (late) launch_fill<32, GDP_LOWER, true, 2>(P, grid, s, 0); else launch_fill<32, GDP_LOWER, false, 2>(P, grid, s, 0); }
 }
 
 static void
@@ -1355,13 +1379,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       }
       cudaEvent_t ev = nullptr;
       prof_begin(ctx, &ev, ks);
+      int nlaunch = 1;
       if (cta) launch_cta_kind(k, P, grid, ks);
       else if (warp) launch_warp_kind(k, P, grid, ks);
       else if (warp8) launch_warp8_kind(k, P, grid, ks);
       else if (early8) launch_early8_kind(k, P, grid, ks);
-      else launch_kind(k, P, grid, ks);
+      else nlaunch = launch_kind(k, P, grid, ks, ph.maxMin[k]);
       prof_end(ctx, k, ev, ks);
-      ctx->launches++;
+      ctx->launches += nlaunch;
       CK(ctx, cudaGetLastError());
     }
   }
