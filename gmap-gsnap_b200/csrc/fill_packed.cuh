@@ -42,7 +42,11 @@
  * Bodies.  A steady column (every lane inside the band) needs no lane
  * masks; the general body handles the band edges with per-word masks built
  * from the lane index; the half body skips lanes 0-7 once the top band lane
- * is 8 or more (they never feed an in-band cell again).
+ * is 8 or more (they never feed an in-band cell again).  Every body is one
+ * run of straight-line code over the eight words (edges are masks, not
+ * branches), so the compiler interleaves the words' independent steps:
+ * per-word skip branches, tried and measured, split the column into basic
+ * blocks and made the kernel a third slower.
  */
 #pragma once
 #include "gdp_internal.h"
@@ -185,164 +189,133 @@ pcol_scores (const PBlock &B, int ka, int kb, uint32_t ps[8]) {
   }
 }
 
-/* Per-pair constants of the packed step, lane i of word k = 2k + (0, 1). */
-struct PConst {
-  uint32_t open2, ext2, neg2;
-  uint32_t dofs[8];   /* open + extend - (i + 1) * extend: Hpre + this = D(i) */
-  uint32_t iext[8];   /* i * extend: F(i) = G(i) + this */
-};
-
-__device__ __forceinline__ void
-pconst_of (const PairView &v, PConst &C) {
-  using namespace gdp_pk;
-  C.open2 = bc(v.open); C.ext2 = bc(v.ext); C.neg2 = bc(NEG);
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    C.dofs[k] = pk(v.oe - (2 * k + 1) * v.ext, v.oe - (2 * k + 2) * v.ext);
-    C.iext[k] = pk(2 * k * v.ext, (2 * k + 1) * v.ext);
-  }
-}
-
-/* Bits of the lanes lo..hi (clamped to 0..15) in the accumulator layout:
-   lane 2j at bit j, lane 2j + 1 at bit 16 + j; branch-free. */
-__device__ __forceinline__ uint32_t
-lanes_acc_bf (int lo, int hi) {
-  lo = max(lo, 0);
-  const int e0 = (lo + 1) >> 1, e1 = hi >> 1, o0 = lo >> 1, o1 = (hi - 1) >> 1;
-  const uint32_t even = (0xffu << min(e0, 8)) & (0xffu >> min(max(7 - e1, 0), 8));
-  const uint32_t odd = (0xffu << min(o0, 8)) & (0xffu >> min(max(7 - o1, 0), 8));
-  return (even & 0xffu) | ((odd & 0xffu) << 16);
-}
-
 /*
- * One swept column y of a full-band block.  GEN = false: a steady column
- * (no band edge inside the block: the top band lane is above lane 0 and
- * the bottom one below lane 15, y >= 1, a full block).  GEN = true: any
- * column, with the band edges of block_column: the bottom cell (H from the
- * diagonal only, DIAG directions, :6926-6945), the top cell (F chain
- * restart, :6962-6974), F only on the lanes between them, column 0
- * (pairscores_col0, :6668-6678).  Once the top band lane t is 2 or more,
- * the words whose lanes all lie above it are skipped: those lanes never
- * feed an in-band cell again, and they keep their last values.
- *
- * The F chain runs as a prefix maximum: with G(i) = F(i) - i * extend and
- * D(i) = Hpre(i) + open + extend - (i + 1) * extend, G(i + 1) =
- * max(G(i), D(i)), two lanes per word step.  Lanes above the top cell get
- * D = -32768 and the chain enters with G = NEG_INFINITY + open + extend -
- * t * extend, so that F(t) = NEG_INFINITY + open + extend there.
+ * One swept column y of a full-band block, lanes 2 K0 .. 15.  GEN = false:
+ * a steady column (no band edge inside the block: the top band lane is
+ * above lane 0 and the bottom one below lane 15, y >= 1, a full block).
+ * GEN = true: any column, with the band edges of block_column: the bottom
+ * cell (H from the diagonal only, DIAG directions, :6926-6945), the top
+ * cell (F chain restart, :6962-6974), F only on the lanes between them,
+ * column 0 (pairscores_col0, :6668-6678).  K0 = 4 (the half body): lanes
+ * 0-7 lie above the band for good and are skipped (GEN, top lane >= 8).
  *
  *   diag    H[y-1][xlo-1] + OFF (or the row-0 value);
  *   Hc, Fc  H[y][xlo-1] and the F carry of the block above, + OFF.
  * Writes the column's two direction words and, with hd, its 16 scores.
- * Returns the carry for the block below: the last lane's H and F, packed.
+ * Returns the carry for the block below: the last lane's H and its F, packed.
  * With `track`, the in-band scores of the column go into vmax.
  */
-template <bool LATE, bool GEN>
+template <bool LATE, bool GEN, int K0>
 __device__ __forceinline__ uint32_t
-pcol (PBlock &B, const PairView &v, const PConst &C, int y, int diag, int Hc, int Fc, int ka, int kb,
-      uint32_t *dcol, int16_t *hd, uint32_t &vmax, bool track) {
+pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int kb, uint32_t *dcol,
+      int16_t *hd, uint32_t &vmax, bool track) {
   using namespace gdp_pk;
+  static_assert(K0 == 0 || GEN, "the half body handles band edges");
+  const uint32_t open2 = bc(v.open), ext2 = bc(v.ext), oe2 = bc(v.oe), neg2 = bc(NEG);
   const int xlo = B.xlo, last = B.last;
   const int rel = y - xlo;
   const int t = rel - v.uband;       /* top band lane */
   const int bt = rel + v.lband;      /* bottom band lane */
-  const int fhi = GEN ? min(bt, last) : 15;   /* last F lane */
-  const int k0 = GEN ? ((t >= 2) ? (t >> 1) : 0) : 0;   /* first word with a lane at or below the top */
-  const int kf = GEN ? (fhi >> 1) : 7;                   /* last word with an F lane */
   const bool col0 = GEN && (y == 0);
-  const bool hasbot = GEN && y > 0 && bt <= last;
-  const int kbot = bt >> 1;
-  const uint32_t capw = (bt & 1) ? 0x80007fffu : 0x7fff8000u;
+  const bool hasbot = GEN && y > 0 && bt >= 0 && bt <= last;
+  const int s = max(t + 1, 0);       /* first F lane */
+  const int fhi = min(bt, last);     /* last F lane */
+  const bool cut_hi = GEN && fhi < 15;
+  const bool cut_lo = GEN && t >= 1;
 
   uint32_t ps[8];
-  pcol_scores<0>(B, ka, kb, ps);
+  pcol_scores<K0>(B, ka, kb, ps);
 
   /* E and H steps (:6862-6913); accE / accN collect the Egap / HORIZ bits
      (jump late: their negations) */
   uint32_t accN = 0, accE = 0;
-  uint32_t prev = (uint32_t) diag << 16;
+  uint32_t prev = (K0 == 0) ? ((uint32_t) diag << 16) : B.H[K0 - 1];
+  const uint32_t negbt2 = bc(-bt);
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const uint32_t Hold = B.H[k];
-    if (GEN && k < k0) { prev = Hold; continue; }
-    const uint32_t Eold = B.E[k];
-    const uint32_t T1 = addmax(Hold, C.open2, C.neg2);
+  for (int k = K0; k < 8; k++) {
+    const uint32_t Hold = B.H[k], Eold = B.E[k];
+    const uint32_t T1 = addmax(Hold, open2, neg2);
     const uint32_t m = max2(Eold, T1);
     accE = ne01(m, LATE ? Eold : T1) * (1u << k) + accE;
-    const uint32_t Ee = addmax(m, C.ext2, C.neg2);
+    const uint32_t Ee = addmax(m, ext2, neg2);
     const uint32_t dg = prmt(prev, Hold, 0x5432u);    /* (H[2k-1], H[2k]) of the last column */
     prev = Hold;
-    uint32_t Hv = addmax(dg, ps[k], C.neg2);
-    if (col0) Hv = (k == 0 && xlo == 0) ? pk(lo16(dg), NEG) : C.neg2;
+    uint32_t Hv = addmax(dg, ps[k], neg2);
+    if (col0) Hv = (k == 0 && xlo == 0) ? pk(lo16(dg), NEG) : neg2;
+    uint32_t Eh = Ee;
     /* the bottom band cell takes the diagonal alone: its E is kept but
        does not enter its H */
-    const uint32_t Eh = (hasbot && k == kbot) ? min2(Ee, capw) : Ee;
+    if (hasbot) Eh = min2(Ee, 0x80008000u - nz01(add2(lanes2(k), negbt2)));
     const uint32_t Hp = max2(Eh, Hv);
     accN = ne01(Hp, LATE ? Eh : Hv) * (1u << k) + accN;
     B.H[k] = Hp;
     B.E[k] = Ee;
   }
 
-  /* F chain (:6950-7000) as a prefix maximum */
-  int Gin;
+  /* F chain (:6950-7000), entered with F(0) */
+  int Fin;
   uint32_t pF0 = 0;   /* F direction of lane 0 */
   if (t < 0) {
     const int Fp = (xlo == 0) ? NEG : Fc, Hp0 = (xlo == 0) ? NEG : Hc;
     const int a = Hp0 + v.open;
     pF0 = LATE ? (Fp >= a) : (Fp > a);
-    Gin = max(Fp, a) + v.ext;
+    Fin = max(Fp, a) + v.ext;
   } else {
-    Gin = NEG + v.oe - t * v.ext;
+    /* the top cell at lane t: the chain holds NEG_INFINITY + open + extend
+       there, the lanes above it masked out */
+    Fin = NEG + v.oe - t * v.ext;
   }
-  uint32_t accV = 0, accF = 0;
-  uint32_t PP = bc(Gin);   /* (G(2k), G(2k)) */
+  uint32_t accV = 0, accFj = 0;
+  uint32_t PP = bc(Fin + 2 * K0 * v.ext);     /* (F(2k), F(2k)) */
+  const uint32_t c01 = pk(0, v.ext);
+  const uint32_t negt2 = bc(-t), fhi2 = bc(fhi);
   uint32_t Flast = 0;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    if (GEN && k < k0) continue;
-    if (GEN && k > kf) break;
+  for (int k = K0; k < 8; k++) {
     const uint32_t Hpre = B.H[k];
-    uint32_t D = add2(Hpre, C.dofs[k]);
-    if (GEN && k == k0 && t >= 1 && (t & 1)) D = (D & 0xffff0000u) | 0x8000u;   /* lane 2k above the top cell */
-    const uint32_t Zg = prmt(D, LOW2, 0x1054u);    /* (LOW, D(2k)) */
-    const uint32_t Gw = max2(PP, Zg);              /* (G(2k), G(2k+1)) */
-    const uint32_t V = max2(Gw, D);                /* (G(2k+1), G(2k+2)) */
-    /* Fgap of lanes 2k+1 (bit k) and 2k+2 (bit 16 + k): jump late, the chain
-       kept its value (G(i) == G(i-1)); jump early, it beat the open
-       (G(i) != D(i-1)) */
-    accF = ne01(V, LATE ? Gw : D) * (1u << k) + accF;
+    uint32_t Hoe = add2(Hpre, oe2);
+    if (cut_lo) Hoe = lowwhere(Hoe, negmask(add2(lanes2(k), negt2)));    /* lanes above the top cell */
+    const uint32_t Z = prmt(Hoe, LOW2, 0x1054u);                           /* (LOW, Hoe(2k)) */
+    const uint32_t Wf = addmax(PP, c01, Z);                                /* (F(2k), F(2k+1)) */
+    const uint32_t V = addmax(Wf, ext2, Hoe);                              /* high half: F(2k+2) */
+    const uint32_t Y = prmt(Wf, V, 0x7632u);                               /* (F(2k+1), F(2k+2)) */
+    /* Fgap of lanes 2k+1 and 2k+2 (lane 2k+1 at bit k, lane 2k+2 at bit
+       16 + k): jump late, F(i) == F(i-1) + extend; jump early,
+       F(i) != Hpre(i-1) + open + extend */
+    accFj = ne01(Y, LATE ? add2(Wf, ext2) : Hoe) * (1u << k) + accFj;
     PP = prmt(V, V, 0x3232u);
-    uint32_t F = add2(Gw, C.iext[k]);              /* (F(2k), F(2k+1)) */
-    if (GEN && k == kf && !(fhi & 1)) F = (F & 0xffffu) | 0x80000000u;   /* lane 2k+1 below the last F lane */
-    const uint32_t Hn = max2(Hpre, F);
-    accV = ne01(Hn, LATE ? F : Hpre) * (1u << (8 + k)) + accV;
+    uint32_t Fm = Wf;
+    if (cut_hi) Fm = lowwhere(Fm, negmask(add2(fhi2, neglanes2(k))));     /* lanes below the last F lane */
+    const uint32_t Hn = max2(Hpre, Fm);
+    accV = ne01(Hn, LATE ? Fm : Hpre) * (1u << (8 + k)) + accV;
     B.H[k] = Hn;
-    if (k == 7) Flast = F;
+    if (k == 7) Flast = Wf;
   }
 
   /* the direction words (W = 16 layout of gdp_internal.h) */
-  const uint32_t comp = GEN ? ((0xffu << k0) & 0xffu) * 0x10001u : 0x00ff00ffu;   /* lanes computed */
-  const uint32_t frange = GEN ? lanes_acc_bf(t + 1, fhi) : 0x00ff00ffu;            /* lanes with an F step */
-  uint32_t nb = LATE ? ~accN : accN;
-  uint32_t vb = LATE ? ~accV : accV;
-  uint32_t eb = LATE ? ~accE : accE;
-  uint32_t fj = LATE ? ~accF : accF;
-  /* fj: lane 2k+1 at bit k, lane 2k+2 at bit 16 + k */
-  uint32_t fb = (((fj >> 16) << 1) & 0xfeu) | ((fj & 0xffu) << 16);
+  const uint32_t comp = lanes_acc(2 * K0, 15);                 /* lanes computed */
+  const uint32_t frange = lanes_acc(max(s, 2 * K0), fhi);      /* lanes with an F step */
+  uint32_t nb = LATE ? (accN ^ comp) : accN;
+  uint32_t vb = LATE ? (accV ^ (comp << 8)) : accV;
+  uint32_t eb = LATE ? (accE ^ comp) : accE;
+  uint32_t fj = accFj;
+  if (LATE) fj ^= (0xffu & ~((1u << K0) - 1u)) * 0x10001u;
+  const uint32_t odd = fj & 0xffu;                              /* lanes 2k+1 */
+  const uint32_t even = ((fj >> 16) << 1) & 0xfeu;              /* lanes 2k+2 */
+  uint32_t fb = (even | (odd << 16)) & ~1u;
   if (!LATE && v.open == 0) fb = 0;   /* jump early with open 0: F never beats H + open */
-  fb |= (t < 0) ? pF0 : 0u;
+  fb |= (s == 0) ? pF0 : 0u;
   nb = (nb & comp) | (vb & (frange << 8));
   eb = (eb & comp) | ((fb & frange) << 8);
-  if (hasbot) eb &= ~((bt & 1) ? (1u << (16 + kbot)) : (1u << kbot));
+  if (hasbot) eb &= ~lanes_acc(bt, bt);
   *reinterpret_cast<uint2 *>(dcol) = make_uint2(prmt(nb, eb, 0x5410u), prmt(nb, eb, 0x7632u));
 
   if (track) {
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      if (GEN && (k < k0 || k > kf)) continue;
+    for (int k = K0; k < 8; k++) {
       uint32_t h = B.H[k];
-      if (GEN && k == k0 && t >= 1 && (t & 1)) h = (h & 0xffff0000u) | 0x8000u;
-      if (GEN && k == kf && !(fhi & 1)) h = (h & 0xffffu) | 0x80000000u;
+      if (cut_lo) h = lowwhere(h, negmask(add2(lanes2(k), negt2)));
+      if (cut_hi) h = lowwhere(h, negmask(add2(fhi2, neglanes2(k))));
       vmax = max2(vmax, h);
     }
   }
@@ -369,8 +342,6 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
                   int64_t slot) {
   using namespace gdp_pk;
   static_assert(MODE == 0 || MODE == 1, "plain fills and the 16-bit pass of rerun pairs");
-  PConst C;
-  pconst_of(v, C);
   uint32_t *dir = P.dirs + mp->dir16;
   uint32_t *sc = reinterpret_cast<uint32_t *>(P.scratch) + slot;
   const int64_t scs = P.nslots;
@@ -403,18 +374,28 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
       bot_prev = lo16(above);
       int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
       const bool track = MODE == 1 && y >= 1 && y >= v.reach_from && xlo + B.last >= v.reach_from;
+      const int t = y - xlo - v.uband;
       uint32_t out;
       if (y >= ys0 && y <= ys1)
-        out = pcol<LATE, false>(B, v, C, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+        out = pcol<LATE, false, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+      else if (y >= 1 && t >= 8 && y != v.g.Y)
+        out = pcol<LATE, true, 4>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
       else
-        out = pcol<LATE, true>(B, v, C, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+        out = pcol<LATE, true, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
       sc[(int64_t) y * scs] = out;
       if (y == v.g.Y) {
         const int L = v.g.X - xlo;
         if (L >= 0 && L <= B.last) {
+          /* word L / 2 through all-ones / zero masks the compiler cannot
+             turn into a runtime array index (which would put the block's
+             words in local memory for the whole sweep) */
           uint32_t w = 0;
 #pragma unroll
-          for (int k = 0; k < 8; k++) w = (k == (L >> 1)) ? B.H[k] : w;
+          for (int k = 0; k < 8; k++) {
+            uint32_t m;
+            asm("{.reg .pred p; setp.eq.s32 p, %1, %2; selp.b32 %0, -1, 0, p;}" : "=r"(m) : "r"(k), "r"(L >> 1));
+            w |= B.H[k] & m;
+          }
           final_score = ((L & 1) ? hi16(w) : lo16(w)) - OFF;
         }
       }
@@ -428,7 +409,7 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
 }
 
 #ifndef GDP_PACKED_MINB
-#define GDP_PACKED_MINB 6
+#define GDP_PACKED_MINB 4
 #endif
 
 /*

@@ -395,9 +395,18 @@ block_column (Block<W> &B, const PairView &v, int y, int diag, int2 above, int k
         if ((dom & (1u << i)) && B.H[i] >= v.lim) reached = true;
     }
   }
-  if (y == v.g.Y) {
+  if (y == v.g.Y && v.g.X - xlo >= 0 && v.g.X - xlo < W) {
+    /* lane X - xlo through all-ones / zero masks the compiler cannot turn
+       into a runtime array index (which would keep B.H in local memory) */
+    const int L = v.g.X - xlo;
+    int fs = 0;
 #pragma unroll
-    for (int i = 0; i < W; i++) if (xlo + i == v.g.X) final_score = B.H[i];
+    for (int i = 0; i < W; i++) {
+      int m;
+      asm("{.reg .pred p; setp.eq.s32 p, %1, %2; selp.b32 %0, -1, 0, p;}" : "=r"(m) : "r"(i), "r"(L));
+      fs |= B.H[i] & m;
+    }
+    final_score = fs;
   }
   if (hd != nullptr) {
 #pragma unroll
