@@ -104,16 +104,15 @@ __device__ __forceinline__ uint32_t nz01 (uint32_t x) {
   return r;
 }
 /* Bits of the lanes lo..hi in the accumulator layout: lane 2j at bit j,
-   lane 2j + 1 at bit 16 + j (0 when the range is empty). */
+   lane 2j + 1 at bit 16 + j (0 when the range is empty); no branches, so
+   the column stays one run of straight-line code. */
 __device__ __forceinline__ uint32_t lanes_acc (int lo, int hi) {
-  if (lo < 0) lo = 0;
-  if (hi > 15) hi = 15;
-  if (lo > hi) return 0u;
+  lo = max(lo, 0);
+  hi = min(hi, 15);
   const int e0 = (lo + 1) >> 1, e1 = hi >> 1, o0 = lo >> 1, o1 = (hi - 1) >> 1;
-  uint32_t m = 0;
-  if (e1 >= e0) m |= ((1u << (e1 + 1)) - 1u) & ~((1u << e0) - 1u);
-  if (hi >= 1 && o1 >= o0) m |= (((1u << (o1 + 1)) - 1u) & ~((1u << o0) - 1u)) << 16;
-  return m;
+  const uint32_t even = (0xffu << min(e0, 8)) & (0xffu >> min(max(7 - e1, 0), 8));
+  const uint32_t odd = (0xffu << min(o0, 8)) & (0xffu >> min(max(7 - o1, 0), 8));
+  return (even & 0xffu) | ((odd & 0xffu) << 16);
 }
 /* PRMT selector: sign-extended byte `a` of lane 2k (first source) and of
    lane 2k + 1 (second source), as a 16x2 word */
