@@ -469,6 +469,137 @@ def single_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=100000):
     return out
 
 
+
+def stage3_end_gaps(genome, seed, ngaps, max_rlength, max_glength):
+    """End gaps as stage 3 sends them to Dynprog_end5_gap / Dynprog_end3_gap:
+    the query beyond the first (end 5) or last (end 3) aligned block, 8..250
+    nt (log-uniform), against the genome stretch next to the block, 0..32 nt
+    longer; half end 5, half end 3; the query matches the genome next to the
+    block with 1 % substitutions, and for 30 % of gaps only over a random
+    part of its length (an unaligned tail: adapter, poly-A, a missed exon);
+    75 % QUERYEND_GAP, 25 % QUERYEND_INDELS; extraband_end 6; plus strand."""
+    rng = np.random.default_rng(seed)
+    rl = np.exp(rng.uniform(np.log(8), np.log(251), ngaps)).astype(np.int64)
+    gl = rl + rng.integers(0, 33, ngaps)
+    end5 = rng.random(ngaps) < 0.5
+    L = genome.size
+    goff = np.where(end5, rng.integers(512, L - 512, ngaps), rng.integers(0, L - 512, ngaps))
+    keep = np.where(rng.random(ngaps) < 0.3, (rng.random(ngaps) * rl).astype(np.int64), rl)
+    tot = int(rl.sum())
+    qoff = np.zeros(ngaps, np.int64)
+    qoff[1:] = np.cumsum(rl)[:-1]
+    k = np.arange(tot) - np.repeat(qoff, rl)               # position in the query
+    rlr, keepr, goffr, e5 = (np.repeat(a, rl) for a in (rl, keep, goff, end5))
+    # end 3: query k against genome goff + k; end 5: query k against genome goff - (rl - 1) + k
+    idx = np.where(e5, goffr - (rlr - 1) + k, goffr + k)
+    q = genome[idx].copy()
+    tail = np.where(e5, k < rlr - keepr, k >= keepr)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    q[tail] = rng.choice(acgt, size=int(tail.sum()))
+    sub = rng.random(tot) < 0.01
+    q[sub] = rng.choice(acgt, size=int(sub.sum()))
+    q[q == ord("N")] = ord("A")
+    gaps = np.zeros(ngaps, dtype=gdp.END_GAP_DTYPE)
+    gaps["rseq"] = gaps["rseq_uc"] = np.where(end5, qoff + rl - 1, qoff)
+    gaps["rlength"], gaps["glength"] = rl, gl
+    gaps["roffset"] = np.where(end5, rl - 1 + rng.integers(0, 1000, ngaps), rng.integers(0, 1000, ngaps))
+    gaps["goffset"] = goff
+    gaps["chroffset"], gaps["chrhigh"] = 0, L
+    gaps["end"] = np.where(end5, 5, 3)
+    gaps["endalign"] = np.where(rng.random(ngaps) < 0.75, gdp.QUERYEND_GAP, gdp.QUERYEND_INDELS)
+    gaps["watsonp"] = 1
+    gaps["jump_late_p"] = rng.random(ngaps) < 0.5
+    gaps["extraband_end"] = 6
+    gaps["max_rlength"], gaps["max_glength"] = max_rlength, max_glength
+    gaps["dynprogindex"] = 1
+    return gaps, q
+
+
+def end_gap_cells(gaps):
+    """In-band cells of the upper and the lower fill of each end gap (the
+    reference computes both): upper rows max(1, c - uband)..min(r, c) per
+    column c, lower columns max(1, r - lband)..min(g, r) per row r."""
+    rl, gl = gaps["rlength"].astype(np.int64), gaps["glength"].astype(np.int64)
+    xb = gaps["extraband_end"].astype(np.int64)
+    wide = gaps["endalign"] != gdp.QUERYEND_INDELS
+    ub = np.where(wide & (gl >= rl), gl - rl + xb, xb)
+    lb = np.where(wide & (gl < rl), rl - gl + xb, xb)
+    cells = 0
+    for i in range(gaps.size):
+        c = np.arange(1, gl[i] + 1)
+        cells += int(np.maximum(0, np.minimum(rl[i], c) - np.maximum(1, c - ub[i]) + 1).sum())
+        r = np.arange(1, rl[i] + 1)
+        cells += int(np.maximum(0, np.minimum(gl[i], r) - np.maximum(1, r - lb[i]) + 1).sum())
+    return cells
+
+
+def end_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=50000):
+    """Dynprog_end5_gap / Dynprog_end3_gap over a batch of stage-3 end gaps,
+    end to end through gdp_end_gap_batch (host gaps and sequences in, host
+    records out), against the reference's own end-gap solvers on the host
+    (all host threads, each with its own Dynprog_T and Pairpool_T, over a
+    bounded prefix of the same gaps; its results are checked against the
+    device's on that prefix, untimed)."""
+    import torch
+    genome, blocks = gdp.make_genome(lib, 779, 1 << 24)
+    ctx.set_genome(blocks, None, genome.size)
+    gaps, arena = stage3_end_gaps(genome, seed, ngaps, 500, 2000)
+    res, recs = ctx.end_gaps(gaps, arena)
+    cells = end_gap_cells(gaps)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+
+    def pinned(arr):
+        t = torch.empty(max(arr.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        a = t.numpy()[:arr.nbytes].view(arr.dtype).reshape(arr.shape)
+        a[...] = arr
+        return t, a
+
+    keep = [pinned(gaps), pinned(arena), pinned(np.zeros(ngaps, dtype=gdp.RESULT_DTYPE)),
+            pinned(np.zeros(max(recs.size, 1), dtype=gdp.REC_DTYPE))]
+    h_gaps, h_arena, h_res, h_recs = (k[1] for k in keep)
+    used = ctypes.c_int64(0)
+    times = []
+    for _ in range(4):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rc = lib.gdp_end_gap_batch(ctx.h, gdp._ptr(h_gaps), ngaps, gdp._ptr(h_arena), h_arena.size,
+                                   gdp._ptr(h_res), gdp._ptr(h_recs), h_recs.size, ctypes.byref(used))
+        b.record(stream)
+        b.synchronize()
+        assert rc == 0 and used.value == recs.size, ctx.error()
+        times.append(a.elapsed_time(b))
+    ms = statistics.median(times[1:])
+    assert np.array_equal(h_res, res) and np.array_equal(h_recs[:recs.size], recs)
+    out = {"gaps": ngaps, "end5": int((gaps["end"] == 5).sum()),
+           "filled_8bit": int((res["precision"] == 8).sum()), "fill_cells": cells,
+           "records": int(recs.size), "ms": round(ms, 3), "gaps_per_s": round(ngaps / (ms * 1e-3), 1),
+           "fill_gcups": round(cells / (ms * 1e-3) / 1e9, 3), "bad_status": int((res["status"] != 0).sum()),
+           "h2d_bytes": int(gaps.nbytes + arena.nbytes), "d2h_bytes": int(res.nbytes + recs.nbytes),
+           "timing": "host gaps and sequences to host records (gdp_end_gap_batch, pinned host "
+                     "buffers), median of 3 after one warm-up, CUDA events on the context stream"}
+    import oracle
+    if cpu_gaps > 0 and oracle.reference_available():
+        ref = oracle.reference()
+        ref.init(0)
+        ref.set_genome(blocks, None, genome.size)
+        re = oracle.ReferenceEndGap(ref, 200, 40)
+        re.setup()
+        sample = gaps[:cpu_gaps]
+        threads = os.cpu_count() or 1
+        secs, _ = re.bench(sample, arena, threads, 200, 40)
+        secs1, _ = re.bench(sample[:cpu_gaps // 8], arena, 1, 200, 40)
+        st, off, rrecs = re.run(sample, arena)
+        same = (np.array_equal(st[:, 0], res["tb_score"][:cpu_gaps]) and
+                np.array_equal(st[:, 5], res["nrecs"][:cpu_gaps]) and
+                np.array_equal(rrecs, recs[:int(res["nrecs"][:cpu_gaps].sum())]))
+        out["cpu_baseline"] = {"value": round(cpu_gaps / secs, 1), "unit": "gaps/s", "cores": threads,
+                               "kind": "reference",
+                               "sample": f"the first {cpu_gaps} gaps, Dynprog_end5_gap / Dynprog_end3_gap of "
+                                         f"oracle/_ref, {secs:.2f} s on {threads} threads",
+                               "one_thread_gaps_per_s": round((cpu_gaps // 8) / secs1, 1),
+                               "same_results": bool(same)}
+    return out
+
 def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000,
                   workers=4):
     """The serving loop under Poisson load: single-pair requests of the
@@ -888,6 +1019,7 @@ def run_gdp(args):
     if rank == 0 and world == 1 and not args.no_per_pair:
         extra["endpoint_search"] = endpoint_search(lib, ctx, args.seed + 9)
         extra["single_gap"] = single_gap_batch(lib, ctx, args.seed + 10)
+        extra["end_gap"] = end_gap_batch(lib, ctx, args.seed + 11)
     if rank == 0 and world == 1 and not args.no_serving:
         extra["serving"] = serving_sweep(lib, local, args.seed + 8,
                                          [1e3, 1e4, 5e4, 1e5, 2e5, 3e5, 5e5, 1e6])

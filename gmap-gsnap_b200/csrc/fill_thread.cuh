@@ -446,11 +446,15 @@ fill_finish (const FillParams &P, int pi, gdp_meta_t *mp, const gdp_geom_t &g, b
     r->score = final_score;
     r->precision = W == 16 ? 16 : 8;
     r->rerun = (MODE == 1) ? 1 : 0;
-    /* only a traceback needs the final cell: an end-gap half, or the
-       lower fill of a gap with glength > rlength (a cDNA gap's lower
+    /* only a traceback from the final cell needs it: an end-gap half, or
+       the lower fill of a gap with glength > rlength (a cDNA gap's lower
        half), holds none and keeps GDP_OK with score NEG_INFINITY, the
-       cell the reference leaves unwritten */
-    if (!swept && eb == nullptr && (P.pairs[pi].flags & GDP_FLAG_TRACEBACK)) r->status = GDP_ERR_BAND;
+       cell the reference leaves unwritten.  A traceback from another cell
+       (an end gap's best cell) checks its own cells as it walks. */
+    const gdp_pair_t &pp = P.pairs[pi];
+    if (!swept && eb == nullptr && (pp.flags & GDP_FLAG_TRACEBACK) && pp.tb_r == pp.rlength &&
+        pp.tb_c == pp.glength)
+      r->status = GDP_ERR_BAND;
     if (eb != nullptr) {
       r->end_score = eb->score;
       r->end_r = eb->r;

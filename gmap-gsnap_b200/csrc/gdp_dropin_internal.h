@@ -31,14 +31,16 @@ int gdpi_traceback_one(gdp_ctx *ctx, gdpi_fill *f, const gdp_pair_t *p, const ch
 void gdpi_fill_free(gdpi_fill *f);
 int gdpi_set_tables(gdp_ctx *ctx, const gdp_tables_t *t);
 
-/* The single-gap layer's state in a context (single_gap.cu): the user
-   penalties of Dynprog_single_setup, and its working memory, kept between
-   calls: grow-only device buffers, pinned host staging and one plan whose
-   buffers are reused. */
+/* The gap solvers' state in a context (single_gap.cu, end_gap.cu): the
+   user penalties of Dynprog_single_setup and Dynprog_end_setup, and the
+   single gap's working memory, kept between calls: grow-only device
+   buffers, pinned host staging and one plan whose buffers are reused. */
 struct gdp_plan;
 struct gdpi_single_cfg {
   int user_open = 0, user_extend = 0;
   bool user_p = false;   /* user_dynprog_p */
+  int end_open = 0, end_extend = 0;
+  bool end_user_p = false;   /* Dynprog_end_setup's user_dynprog_p */
   static constexpr int NBUF = 16;
   void *dbuf[NBUF] = {};
   size_t dcap[NBUF] = {};

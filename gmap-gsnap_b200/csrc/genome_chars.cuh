@@ -47,14 +47,19 @@ genomic_char (const gdp_pair_t &p, int gp, const uint32_t *genome, const uint32_
  * The character Dynprog_single_gap's gsequence holds for genomic coordinate
  * gp (GDP_XFLAG_SEGMENT): Genome_get_segment_right on the plus strand ('*'
  * at and above chrhigh), the reverse complement of Genome_get_segment_left
- * on the minus strand ('*' below chroffset), src/genome.c:11022-11120.  The
- * positions it reads must be resident (the planner checks).
+ * on the minus strand ('*' below chroffset), src/genome.c:11022-11120; with
+ * GDP_XFLAG_SEGMENT_REV the mirrored segment Dynprog_end5_gap reads
+ * (segment_left on the plus strand, '*' below chroffset; the reverse
+ * complement of segment_right on the minus strand, '*' at and above
+ * chrhigh).  The positions it reads must be resident (the planner checks).
  */
 __device__ __forceinline__ char
 segment_char (const gdp_pair_t &p, int gp, const uint32_t *genome, const uint32_t *genomealt, uint64_t len,
               char *alt) {
   const int64_t pos = p.watsonp ? (int64_t) p.chroffset + gp : (int64_t) p.chrhigh - gp;
-  if (p.watsonp ? pos >= (int64_t) p.chrhigh : pos < (int64_t) p.chroffset) { *alt = '*'; return '*'; }
+  const bool rev = (p.xflags & GDP_XFLAG_SEGMENT_REV) != 0;
+  const bool below = pos < (int64_t) p.chroffset, above = pos >= (int64_t) p.chrhigh;
+  if (p.watsonp ? (rev ? below : above) : (rev ? above : below)) { *alt = '*'; return '*'; }
   if (genome == nullptr || pos < 0 || (uint64_t) pos >= len) { *alt = 'N'; return 'N'; }
   const uint32_t rp = (uint32_t) pos;
   const char c = gnt_decode(genome, rp, true);

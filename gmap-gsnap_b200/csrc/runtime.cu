@@ -711,7 +711,9 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
   if (p.mismatchtype < 0 || p.mismatchtype > 3) return GDP_ERR_PARAM;
   if (p.open < -127 || p.open > 0 || p.extend < -127 || p.extend > 0) return GDP_ERR_PARAM;
   if (p.genestrand < 0 || p.genestrand > 2) return GDP_ERR_PARAM;
-  if (p.xflags & ~GDP_XFLAG_SEGMENT) return GDP_ERR_PARAM;
+  if ((p.xflags & ~(GDP_XFLAG_SEGMENT | GDP_XFLAG_SEGMENT_REV)) ||
+      (p.xflags & (GDP_XFLAG_SEGMENT | GDP_XFLAG_SEGMENT_REV)) == (GDP_XFLAG_SEGMENT | GDP_XFLAG_SEGMENT_REV))
+    return GDP_ERR_PARAM;
   if (p.rlength <= 0 || p.glength <= 0 || p.rlength > (1 << 20) || p.glength > (1 << 20)) return GDP_ERR_LEN;
   if (p.lband < 0 || p.uband < 0) return GDP_ERR_BAND;
   if (arena_bytes >= 0) {
@@ -741,6 +743,10 @@ validate (const gdp_pair_t &p, int64_t arena_bytes, uint64_t genome_len) {
          Genome_get_segment_left those below chroffset */
       if (p.watsonp) hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
       else lo = std::max<int64_t>(lo, p.chroffset);
+    } else if (p.xflags & GDP_XFLAG_SEGMENT_REV) {
+      /* the mirrored segment: left on the plus strand, right on the minus */
+      if (p.watsonp) lo = std::max<int64_t>(lo, p.chroffset);
+      else hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);
     } else {
       lo = std::max<int64_t>(lo, p.chroffset);
       hi = std::min<int64_t>(hi, (int64_t) p.chrhigh - 1);

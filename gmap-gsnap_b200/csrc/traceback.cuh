@@ -97,7 +97,7 @@ window_kernel (const gdp_pair_t *pairs, const int32_t *status, int64_t n, char *
     const int g0 = (p.flags & GDP_FLAG_REVP) ? p.genomeoffset - (gl - 1) : p.genomeoffset;
     char *w = arena + p.gseq, *wa = arena + p.gseq_alt;
     const bool same = (p.gseq_alt == p.gseq);
-    const bool segment = (p.xflags & GDP_XFLAG_SEGMENT) != 0;
+    const bool segment = (p.xflags & (GDP_XFLAG_SEGMENT | GDP_XFLAG_SEGMENT_REV)) != 0;
     for (int j = threadIdx.x; j < gl; j += blockDim.x) {
       char a, c;
       if (segment) {

@@ -65,6 +65,20 @@ SINGLE_GAP_DTYPE = np.dtype([
 ])
 assert SINGLE_GAP_DTYPE.itemsize == 72
 SINGLE_NULL, SINGLE_SIMPLE, SINGLE_DP = 0, 1, 2
+XFLAG_SEGMENT_REV = 2
+
+# struct gdp_end_gap, 72 bytes: the arguments of Dynprog_end5_gap / _end3_gap
+END_GAP_DTYPE = np.dtype([
+    ("rseq", "<i8"), ("rseq_uc", "<i8"),
+    ("rlength", "<i4"), ("glength", "<i4"), ("roffset", "<i4"), ("goffset", "<i4"),
+    ("chroffset", "<u4"), ("chrhigh", "<u4"),
+    ("end", "i1"), ("endalign", "i1"), ("watsonp", "i1"), ("genestrand", "i1"), ("jump_late_p", "i1"),
+    ("require_pos_score_p", "i1"), ("pad", "<i2"),
+    ("extraband_end", "<i4"), ("max_rlength", "<i4"), ("max_glength", "<i4"), ("dynprogindex", "<i4"),
+    ("defect_rate", "<f8"),
+])
+assert END_GAP_DTYPE.itemsize == 72
+QUERYEND_GAP, QUERYEND_INDELS, QUERYEND_NOGAPS, BEST_LOCAL = 0, 1, 2, 3
 
 WL_FIXED, WL_SHORT, WL_CDNA, WL_MIX, WL_LONG = 1, 2, 3, 4, 5
 
@@ -135,6 +149,8 @@ def load(path=LIB_PATH):
     lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
     lib.gdp_single_setup.argtypes = [vp, i32, i32, i32, i32]
     lib.gdp_single_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_end_setup.argtypes = [vp, i32, i32, i32]
+    lib.gdp_end_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
     lib.gdp_gap_queue_create.argtypes = [i32, i32, i64, i64, vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
     lib.gdp_gap_queue_setup.argtypes = [vp, i32, i32, i32, i32]
     lib.gdp_gap_queue_align.argtypes = [vp, vp, vp, vp, vp, vp, vp, i64, ctypes.POINTER(i64)]
@@ -409,6 +425,24 @@ class Context:
         if rc != 0:
             raise RuntimeError(f"gdp_single_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
         return results, path, recs[:used.value]
+
+    def end_setup(self, user_open=0, user_extend=0, user_dynprog_p=False):
+        return self.lib.gdp_end_setup(self.h, user_open, user_extend, int(user_dynprog_p))
+
+    def end_gaps(self, gaps, arena, max_recs=None):
+        """Dynprog_end5_gap / Dynprog_end3_gap over a batch: (results, records)."""
+        n = gaps.size
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        if max_recs is None:
+            max_recs = int((np.maximum(gaps["rlength"], 0).astype(np.int64)
+                            + np.maximum(gaps["glength"], 0) + 2).sum())
+        recs = np.zeros(max(max_recs, 1), dtype=REC_DTYPE)
+        used = ctypes.c_int64(0)
+        rc = self.lib.gdp_end_gap_batch(self.h, _ptr(gaps), n, _ptr(arena), arena.size, _ptr(results),
+                                        _ptr(recs), max_recs, ctypes.byref(used))
+        if rc != 0:
+            raise RuntimeError(f"gdp_end_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
+        return results, recs[:used.value]
 
     def fill_dump(self, pairs, arena, scores=True):
         """Dense in-band scores and directions of every pair.  With

@@ -132,7 +132,12 @@ enum {
      down from chrhigh - genomeoffset, '*' below chroffset), src/genome.c:
      11022-11120.  The two differ from get_genomic_nt only on the minus
      strand at genomic coordinate 0, which reads position chrhigh. */
-  GDP_XFLAG_SEGMENT = 1
+  GDP_XFLAG_SEGMENT = 1,
+  /* the mirrored segment, as Dynprog_end5_gap reads its rev_gsequence:
+     Genome_get_segment_left on the plus strand ('*' below chroffset) and
+     the reverse complement of Genome_get_segment_right on the minus strand
+     ('*' at and above chrhigh) */
+  GDP_XFLAG_SEGMENT_REV = 2
 };
 
 /*
@@ -449,6 +454,83 @@ int gdp_single_setup(gdp_ctx *ctx, int user_open, int user_extend, int user_dynp
 int gdp_single_gap_batch(gdp_ctx *ctx, const gdp_single_gap_t *gaps, int64_t ngaps, const char *arena,
                          int64_t arena_bytes, gdp_result_t *results, int8_t *path, gdp_rec_t *recs,
                          int64_t max_recs, int64_t *nrecs_used);
+
+/*
+ * Dynprog_end5_gap / Dynprog_end3_gap (src/dynprog_end.c:1293-1650,
+ * :1923-2245) for a batch of end gaps: the alignment of a read end beyond
+ * its last aligned block, which GMAP's stage 3 runs for the 5' and 3' ends
+ * of every alignment.  Per gap, as the reference does:
+ *   - mismatch type ENDQ; open / extend by defect_rate (END_OPEN_* /
+ *     END_EXTEND_*: -10/-2 below DEFECT_HIGHQ, -8/-2 below DEFECT_MEDQ,
+ *     -6/-2 above) or gdp_end_setup's user penalties;
+ *   - rlength <= 0, glength <= 0, or (end 5) goffset < 0: no pairs, score
+ *     and counts 0; otherwise rlength and glength are cut to max_rlength /
+ *     max_glength (the caller's Dynprog_T sizes);
+ *   - the genome segment from the resident genome: end 3 as
+ *     Genome_get_segment_right (plus strand, from chroffset + goffset) or
+ *     the reverse complement of Genome_get_segment_left (minus strand, down
+ *     from chrhigh - goffset); end 5 as Genome_get_segment_left (plus
+ *     strand, ending at chroffset + goffset) or the reverse complement of
+ *     Genome_get_segment_right (minus strand, from chrhigh - goffset), read
+ *     backwards (src/genome.c:11022-11120);
+ *   - GDP_QUERYEND_GAP and GDP_BEST_LOCAL: wide bands (Dynprog_compute_bands
+ *     with extraband_end), an upper and a lower fill, the best cell of the
+ *     band (find_best_endpoint_*); GDP_QUERYEND_INDELS: narrow bands and the
+ *     best cell of the last query row (find_best_endpoint_to_queryend_
+ *     indels_*); 8-bit fills when rlength or glength is below 24
+ *     (use8p_size[ENDQ], the || rule), else 16-bit; end 5 fills backwards
+ *     with the tie rule reversed (!jump_late_p), end 3 forwards;
+ *   - the traceback from the best cell, through the upper fill when
+ *     bestc >= bestr, else the lower; none with require_pos_score_p;
+ *   - GDP_QUERYEND_GAP / GDP_BEST_LOCAL: a traceback with nmatches + 1 <
+ *     nmismatches returns no pairs and score 0 (the counts stay); otherwise
+ *     the pairs come in the order of the reference's returned List (head
+ *     first), without its leading indel pairs.
+ * GDP_QUERYEND_NOGAPS gaps and gaps with an end other than 5 or 3 get
+ * GDP_ERR_PARAM (not built).  results[i]: status, tb_score (the traceback
+ * score), the counts, nrecs records at rec_offset in `recs`, precision, and
+ * in end_score / end_r / end_c the best cell the search found (all 0 for a
+ * gap that ran no search: no pairs by the length checks, or
+ * require_pos_score_p).  When the records do not fit into max_recs, the
+ * first gap whose records pass it and every later gap with records get
+ * GDP_ERR_RECS (and no records).  The reference advances dynprogindex away
+ * from zero once per gap that passes the length checks (rlength > 0,
+ * glength > 0, end 5 goffset >= 0); the caller does the same.  Queries more
+ * than one base longer than their genome stretch (after the cuts) have no
+ * defined reference result: its endpoint scan then reads lower-matrix cells
+ * beyond glength that no fill wrote; here those cells do not exist.  The
+ * fills read rseq: the substitution tables score a lower-case query letter
+ * as its upper-case letter, so this equals the reference's fill with
+ * rsequenceuc when rseq_uc holds rseq upper-cased.  Calls on one context
+ * must not overlap.
+ */
+typedef struct gdp_end_gap {
+  int64_t rseq;          /* the reference's sequence pointer as an arena offset: end 5, rev_rsequence (the
+                            query's last character, read backwards); end 3, rsequence (its first) */
+  int64_t rseq_uc;       /* rev_rsequenceuc / rsequenceuc, the same way */
+  int32_t rlength, glength;
+  int32_t roffset, goffset;       /* rev_roffset, rev_goffset (end 5); roffset, goffset (end 3) */
+  uint32_t chroffset, chrhigh;
+  int8_t end;                     /* 5 or 3 */
+  int8_t endalign;                /* GDP_QUERYEND_GAP, GDP_QUERYEND_INDELS, GDP_QUERYEND_NOGAPS, GDP_BEST_LOCAL */
+  int8_t watsonp, genestrand, jump_late_p, require_pos_score_p;
+  int16_t pad;
+  int32_t extraband_end;
+  int32_t max_rlength, max_glength;   /* dynprog->max_rlength, dynprog->max_glength */
+  int32_t dynprogindex;
+  double defect_rate;
+} gdp_end_gap_t;
+
+/* Endalign_T (src/dynprog.h:24) */
+enum { GDP_QUERYEND_GAP = 0, GDP_QUERYEND_INDELS = 1, GDP_QUERYEND_NOGAPS = 2, GDP_BEST_LOCAL = 3 };
+
+/* Dynprog_end_setup (src/dynprog_end.c:118): user gap penalties for later
+   gdp_end_gap_batch calls on the context. */
+int gdp_end_setup(gdp_ctx *ctx, int user_open, int user_extend, int user_dynprog_p);
+
+int gdp_end_gap_batch(gdp_ctx *ctx, const gdp_end_gap_t *gaps, int64_t ngaps, const char *arena,
+                      int64_t arena_bytes, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                      int64_t *nrecs_used);
 
 /*
  * Stage-3 batching adapter.  GMAP's stage 3 calls Dynprog_single_gap once

@@ -288,6 +288,179 @@ def single_gap_restated(orc, gaps, arena, g, galt, user=None):
     return stats, off, recs
 
 
+
+class ReferenceEndGap:
+    """The reference's own Dynprog_end5_gap / Dynprog_end3_gap
+    (oracle/ref_end.c) over a batch of end gaps, in a reference library
+    (shares its genome and tables)."""
+
+    def __init__(self, ref, maxlookback, extraquerygap):
+        lib = ref.lib
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        lib.ref_end_init.argtypes = [i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        lib.ref_end_setup.argtypes = [i32, i32, i32]
+        lib.ref_end_gap_batch.argtypes = [vp, i32, vp, vp, vp, i64, vp]
+        lib.ref_end_gap_batch.restype = i64
+        mr, mg = ctypes.c_int(0), ctypes.c_int(0)
+        lib.ref_end_init(maxlookback, extraquerygap, ctypes.byref(mr), ctypes.byref(mg))
+        self.lib = lib
+        self.max_rlength, self.max_glength = mr.value, mg.value
+
+    def setup(self, user_open=0, user_extend=0, user_dynprog_p=False):
+        self.lib.ref_end_setup(user_open, user_extend, int(user_dynprog_p))
+
+    def bench(self, gaps, arena, nthreads, maxlookback, extraquerygap):
+        """Wall seconds and a checksum of the end-gap solvers over every gap
+        once on nthreads threads, each with its own Dynprog_T (sized by
+        maxlookback / extraquerygap) and Pairpool_T."""
+        lib = self.lib
+        lib.ref_end_gap_bench.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+        lib.ref_end_gap_bench.restype = ctypes.c_double
+        cs = ctypes.c_int64(0)
+        secs = lib.ref_end_gap_bench(_ptr(gaps), gaps.size, _ptr(arena), nthreads, maxlookback, extraquerygap,
+                                     ctypes.byref(cs))
+        return secs, cs.value
+
+    def run(self, gaps, arena):
+        """Per gap: stats (traceback_score, nmatches, nmismatches, nopens,
+        nindels, npairs, list is NULL, dynprogindex after), record offsets,
+        and the records (the returned List, head first)."""
+        n = gaps.size
+        stats = np.zeros((n, 8), np.int32)
+        off = np.zeros(n, np.int64)
+        cap = int((np.maximum(gaps["rlength"], 0).astype(np.int64) + np.maximum(gaps["glength"], 0) + 2).sum()) + 1
+        recs = np.zeros(cap, dtype=_rec_dtype())
+        used = self.lib.ref_end_gap_batch(_ptr(gaps), n, _ptr(arena), _ptr(stats), _ptr(recs), cap, _ptr(off))
+        assert used <= cap
+        return stats, off, recs[:used]
+
+
+def _segment_end(g, galt, chroffset, chrhigh, goffset, glength, watsonp, end):
+    """The genome segment of an end gap, stored forward: end 3 is
+    Dynprog_end3_gap's gsequence (Genome_get_segment_right from chroffset +
+    goffset on the plus strand, the reverse complement of Genome_get_
+    segment_left down from chrhigh - goffset on the minus strand; '*' at and
+    above chrhigh, or below chroffset); end 5 is Dynprog_end5_gap's
+    rev_gsequence (src/dynprog_end.c:1384-1390): Genome_get_segment_left
+    ending at chroffset + goffset ('*' below chroffset) or the reverse
+    complement of Genome_get_segment_right from chrhigh - goffset ('*' at
+    and above chrhigh).  Character j is genomic coordinate goffset + j (end
+    3) or goffset - (glength - 1) + j (end 5)."""
+    compl = {65: 84, 67: 71, 71: 67, 84: 65}
+    seg = np.empty(glength, np.uint8)
+    alt = np.empty(glength, np.uint8)
+    g0 = goffset - (glength - 1) if end == 5 else goffset
+    for j in range(glength):
+        pos = chroffset + g0 + j if watsonp else chrhigh - (g0 + j)
+        if end == 5:
+            star = pos < chroffset if watsonp else pos >= chrhigh
+        else:
+            star = pos >= chrhigh if watsonp else pos < chroffset
+        if star:
+            seg[j] = alt[j] = 42
+            continue
+        c = int(g[pos])
+        a = c if c == 78 else int(galt[pos])
+        seg[j], alt[j] = (c, a) if watsonp else (compl.get(c, c), compl.get(a, a))
+    return seg, alt
+
+
+def end_gap_restated(orc, gaps, arena, g, galt, user=None):
+    """Dynprog_end5_gap / Dynprog_end3_gap (src/dynprog_end.c:1293-1650,
+    :1923-2245) restated over a CPU oracle's fills and traceback (orc:
+    restatement() or reference(), tables and genome set): ENDQ penalties by
+    defect rate (:88-94), the length checks and cuts, Dynprog_compute_bands
+    (src/dynprog.c:1246), 8-bit fills when either length is below 24
+    (use8p_size[ENDQ], the || rule), the upper and lower fills (end 5 with
+    revp and !jump_late_p), the endpoint scan (find_best_endpoint), the
+    traceback from the best cell through the upper fill when bestc >= bestr,
+    the nmatches + 1 < nmismatches rejection, and the List_reverse and
+    indel trimming (end 5 reversed once more).  Returns the same (stats,
+    offsets, records) as ReferenceEndGap.run, without the dynprogindex
+    column's update.  NOGAPS gaps are not restated (stats all 0)."""
+    n = gaps.size
+    stats = np.zeros((n, 8), np.int32)
+    off = np.zeros(n, np.int64)
+    out = []
+    used = 0
+    for i in range(n):
+        x = gaps[i]
+        off[i] = used
+        stats[i, 7] = int(x["dynprogindex"])
+        stats[i, 6] = 1
+        end, endalign = int(x["end"]), int(x["endalign"])
+        rl, gl = int(x["rlength"]), int(x["glength"])
+        if rl <= 0 or endalign == 2:
+            continue
+        rl = min(rl, int(x["max_rlength"]))
+        if end == 5 and int(x["goffset"]) < 0:
+            continue
+        if gl <= 0:
+            continue
+        gl = min(gl, int(x["max_glength"]))
+        if user is not None:
+            op, ex = user
+        else:
+            d = float(x["defect_rate"])
+            op, ex = (-10 if d < 0.003 else -8 if d < 0.014 else -6), -2
+        xb = int(x["extraband_end"])
+        qend = endalign == 1
+        if qend:
+            lb = ub = xb
+        elif gl >= rl:
+            lb, ub = xb, gl - rl + xb
+        else:
+            lb, ub = rl - gl + xb, xb
+        prec = 8 if (rl < 24 or gl < 24) else 16
+        seg, alt = _segment_end(g, galt, int(x["chroffset"]), int(x["chrhigh"]), int(x["goffset"]), gl,
+                                bool(x["watsonp"]), end)
+        r0 = int(x["rseq"]) - (rl - 1) if end == 5 else int(x["rseq"])
+        u0 = int(x["rseq_uc"]) - (rl - 1) if end == 5 else int(x["rseq_uc"])
+        rs, ru = arena[r0:r0 + rl], arena[u0:u0 + rl]
+        late = (not x["jump_late_p"]) if end == 5 else bool(x["jump_late_p"])
+        local = np.concatenate([rs, ru, seg, alt])
+        p = np.zeros(1, dtype=_pair_dtype())
+        p["rseq"], p["rseq_uc"], p["gseq"], p["gseq_alt"] = 0, rl, 2 * rl, 2 * rl + gl
+        p["rlength"], p["glength"] = rl, gl
+        p["precision"], p["mismatchtype"] = prec, 3
+        p["open"], p["extend"] = op, ex
+        p["flags"] = (1 if late else 0) | (2 if end == 5 else 0)
+        p["queryoffset"], p["genomeoffset"] = int(x["roffset"]), int(x["goffset"])
+        p["chroffset"], p["chrhigh"] = int(x["chroffset"]), int(x["chrhigh"])
+        p["watsonp"], p["genestrand"] = int(x["watsonp"]), int(x["genestrand"])
+        p["dynprogindex"] = int(x["dynprogindex"])
+        up, lo = p.copy(), p.copy()
+        up["variant"], up["uband"] = 1, ub
+        lo["variant"], lo["lband"] = 2, lb
+        if x["require_pos_score_p"]:
+            continue
+        Hu = orc.align(up, 0, local)["H"].reshape(gl + 1, rl + 1)
+        Hl = orc.align(lo, 0, local)["H"].reshape(gl + 1, rl + 1)
+        _, br, bc, _ = find_best_endpoint(Hu, Hl, rl, gl, lb, ub, late, qend, prec)
+        t = (up if bc >= br else lo).copy()
+        t["flags"] |= 4
+        t["tb_r"], t["tb_c"] = br, bc
+        r = orc.align(t, 0, local, want_matrix=False)
+        st = r["stats"]
+        score, nmatch, nmis, nopen, nindel = (int(v) for v in st[:5])
+        if endalign in (0, 3) and nmatch + 1 < nmis:
+            stats[i, :7] = (0, nmatch, nmis, nopen, nindel, 0, 1)
+            continue
+        recs = [tuple(rec) for rec in r["recs"]]
+        k = 0
+        while k < len(recs) and recs[k][3] == b"-":
+            k += 1
+        recs = recs[k:]
+        if end == 5:
+            recs.reverse()
+        stats[i, :7] = (score, nmatch, nmis, nopen, nindel, len(recs), 0 if recs else 1)
+        out.extend(recs)
+        used += len(recs)
+    recs = np.array(out, dtype=_rec_dtype()) if out else np.zeros(0, dtype=_rec_dtype())
+    return stats, off, recs
+
+
 def _pair_dtype():
     """struct gdp_pair (include/gdp.h), 88 bytes."""
     return np.dtype([

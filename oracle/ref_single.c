@@ -74,18 +74,21 @@ reverse_complement (char *s, Chrpos_T length) {
   if (length % 2 == 1) s[length / 2] = compl_nt(s[length / 2]);
 }
 
-/* segment[i] = the genome at first + i, '*' where star(first + i) */
+/* segment[i] = the genome at first + i, '*' where first + i lies outside
+   [lo_ok, hi_ok).  Positions are signed: the left segment of a window that
+   starts before coordinate 0 (right < length) reads '*' there, as the
+   reference's out_of_bounds count does. */
 static void
-fill_segment (char *segment, char *segmentalt, Genome_T genome, Genome_T genomealt, Univcoord_T first,
-              Chrpos_T length, Univcoord_T lo_ok, Univcoord_T hi_ok, bool revcomp) {
+fill_segment (char *segment, char *segmentalt, Genome_T genome, Genome_T genomealt, int64_t first,
+              Chrpos_T length, int64_t lo_ok, int64_t hi_ok, bool revcomp) {
   Chrpos_T i;
   for (i = 0; i < length; i++) {
-    const Univcoord_T pos = first + i;
+    const int64_t pos = first + (int64_t) i;
     if (pos < lo_ok || pos >= hi_ok) {
       segment[i] = segmentalt[i] = '*';
     } else {
-      segment[i] = nt_at(genome->blocks, genome->blocks, pos);
-      segmentalt[i] = nt_at(genomealt->blocks, genome->blocks, pos);
+      segment[i] = nt_at(genome->blocks, genome->blocks, (Univcoord_T) pos);
+      segmentalt[i] = nt_at(genomealt->blocks, genome->blocks, (Univcoord_T) pos);
     }
   }
   segment[length] = segmentalt[length] = '\0';
@@ -99,15 +102,15 @@ void
 Genome_get_segment_right (char *segment, char *segmentalt, Genome_T genome, Genome_T genomealt,
                           Univcoord_T left, Chrpos_T length, Univcoord_T chrhigh, bool revcomp) {
   if (length == 0) { segment[0] = segmentalt[0] = '\0'; return; }
-  fill_segment(segment, segmentalt, genome, genomealt, left, length, 0, chrhigh, revcomp);
+  fill_segment(segment, segmentalt, genome, genomealt, (int64_t) left, length, 0, (int64_t) chrhigh, revcomp);
 }
 
 void
 Genome_get_segment_left (char *segment, char *segmentalt, Genome_T genome, Genome_T genomealt,
                          Univcoord_T right, Chrpos_T length, Univcoord_T chroffset, bool revcomp) {
   if (length == 0) { segment[0] = segmentalt[0] = '\0'; return; }
-  fill_segment(segment, segmentalt, genome, genomealt, right - length, length, chroffset, (Univcoord_T) -1,
-               revcomp);
+  fill_segment(segment, segmentalt, genome, genomealt, (int64_t) right - (int64_t) length, length,
+               (int64_t) chroffset, INT64_MAX, revcomp);
 }
 
 static Dynprog_T single_dynprog = NULL;
