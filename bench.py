@@ -609,17 +609,24 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
     pool, arena = gdp.make_resident_pairs(lib, gdp.WL_MIX, seed, genome, pool_size)
     cells = gdp.band_cells(pool)
     srv = gdp.Server(lib, device=device, workers=workers, budget=40 << 30, blocks=blocks, length=genome.size)
+    cls = srv.classes(pool)                                  # 0 short, 1 long (longest stretch > 512)
     srv.drive(pool, arena, 300_000, rate=1e6, seed=1)       # warm-up: every worker's buffers reach working size
     rows = []
     for k, rate in enumerate(rates):
         n = int(min(max_requests, max(200, rate * seconds_per_rate)))
         lat, elapsed, _ = srv.drive(pool, arena, n, rate=rate, seed=100 + k)
         served = cells[np.arange(n) % pool.size].sum()
-        rows.append({"offered_per_s": rate, "requests": n,
-                     "sustained_per_s": round(n / elapsed, 1),
-                     "p50_ms": round(float(np.percentile(lat, 50)), 3),
-                     "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                     "gcups": round(float(served) / elapsed / 1e9, 2)})
+        c = cls[np.arange(n) % pool.size]
+        row = {"offered_per_s": rate, "requests": n,
+               "sustained_per_s": round(n / elapsed, 1),
+               "p50_ms": round(float(np.percentile(lat, 50)), 3),
+               "p99_ms": round(float(np.percentile(lat, 99)), 3),
+               "gcups": round(float(served) / elapsed / 1e9, 2)}
+        for k, label in ((0, "short"), (1, "long")):
+            if (c == k).any():
+                row[f"{label}_p50_ms"] = round(float(np.percentile(lat[c == k], 50)), 3)
+                row[f"{label}_p99_ms"] = round(float(np.percentile(lat[c == k], 99)), 3)
+        rows.append(row)
     st = srv.stats()
     srv.close()
     knee = max((r["offered_per_s"] for r in rows if r["sustained_per_s"] >= 0.95 * r["offered_per_s"]),
@@ -627,6 +634,10 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
     return {"genome": "100 Mbp seeded random, resident (genomecomp, 2-bit + N flags)",
             "requests": "single pairs of the 70/25/5 short/long/cDNA mix, device-extracted windows",
             "workers": workers, "dir_budget_gb": 40, "sweep": rows, "knee_offered_per_s": knee,
+            "classes": {"short": "longest stretch <= 512 nt, batched apart on the higher stream priority, "
+                                 "served by half the workers (and by the others when no long request waits)",
+                        "short_share": round(float((cls == 0).mean()), 3),
+                        "class_batches": st["class_batches"], "class_pairs": st["class_pairs"]},
             "batches": st["batches"], "max_batch_pairs": st["max_batch_pairs"],
             "peak_admitted_dir_gb": round(st["peak_reserved_bytes"] / 2**30, 3)}
 
@@ -853,6 +864,8 @@ def kernel_cells(pairs, kernel, ctx):
     the 16-bit pass of every rerun pair); pairs with fewer lanes (query
     rows; lower: genome columns) than warp_min_x go one thread per pair
     (fill_thread), the others to lane groups or CTAs."""
+    if "," not in kernel:
+        return int(gdp.band_cells(pairs).sum())
     variant = {"full": gdp.FULL, "upper": gdp.UPPER, "lower": gdp.LOWER}[kernel.split(",")[1]]
     rerun = ((pairs["precision"] == 8) & ((pairs["flags"] & gdp.FLAG_RERUN16) != 0))
     if "W16" in kernel:
@@ -957,7 +970,10 @@ def run_gdp(args):
         g = k.replace(",early,", ",*,").replace(",late,", ",*,")
         tot, n_launch, members = groups.get(g, (0.0, 0, []))
         groups[g] = (tot + kms, n_launch + kn, members + [k])
-    top_name, (top_ms, top_n, top_members) = max(groups.items(), key=lambda kv: kv[1][0])
+    # the dominant fill group (the roofline counts fill lane-ops; a profiler
+    # that serialises launches can make the traceback look larger)
+    fills = {g: v for g, v in groups.items() if g.startswith("fill_")} or groups
+    top_name, (top_ms, top_n, top_members) = max(fills.items(), key=lambda kv: kv[1][0])
     avg_launch_ms = top_ms / args.steps          # the group's device time per step
     int_peak = ctx.int_peak()
     top_cells = kernel_cells(pairs, top_name, ctx)
@@ -1028,15 +1044,16 @@ def run_gdp(args):
     if os.path.exists(peaks_path):
         hbm = json.load(open(peaks_path)).get("hbm_gbs")
     # DRAM bytes of the dominant kernel per launch: one ncu capture of the same
-    # kernel on 50,000 pairs of this workload (dram__bytes_read.sum +
-    # dram__bytes_write.sum = 123.70 + 266.46 MB over 300,657,762 in-band
-    # cells), scaled to this launch by its in-band cells; the kernel's bytes
-    # grow with the cells (directions and carries per swept cell)
+    # kernel on 300,000 pairs of this workload (its first launch, the 150,000
+    # jump-early pairs: dram__bytes_read.sum + dram__bytes_write.sum =
+    # 357.99 + 832.93 MB over 902,385,535 in-band cells), scaled to this
+    # step's launches by their in-band cells; the kernel's bytes grow with the
+    # cells (directions and carries per swept cell)
     traffic, traffic_src = None, None
     if name == "short" and top_name.startswith("fill_packed<W16,full"):
-        traffic = int(round((123.696896e6 + 266.455296e6) / 300657762 * top_cells))
-        traffic_src = ("ncu capture of this kernel on 50,000 pairs (390.2 MB), scaled by in-band cells "
-                       "to one step's launches")
+        traffic = int(round((357.993728e6 + 832.926208e6) / 902385535 * top_cells))
+        traffic_src = ("ncu capture of this kernel on 300,000 pairs (1,190.9 MB for 902,385,535 in-band cells), "
+                       "scaled by in-band cells to one step's launches")
     if rank == 0:
         line = {
             "metric": "GCUPS (in-band cells, fill + traceback), batched",

@@ -284,6 +284,8 @@ struct gdp_ctx {
   int device = 0;
   cudaStream_t wave_stream[GDP_MAX_WAVE_STREAMS] = {};   /* gdp_align_batch's compute, highest priority first */
   int nwave = 0;
+  int wave_prio = 0;     /* first wave stream of a batch: 0 = the highest priority */
+  int grid_limit = 0;    /* fill and traceback grids: at most this many blocks per SM (0: no limit) */
   int nsm = 148;
   cudaStream_t stream = nullptr;        /* compute */
   cudaStream_t h2d = nullptr, d2h = nullptr;
@@ -1160,16 +1162,25 @@ launch_kind (int k, FillParams P, int grid, cudaStream_t s, int max_min_len) {
   return 0;
 }
 
+/* Grid cap of the fill and traceback kernels: k blocks per SM, or fewer
+   under the context's grid_limit (a footprint cap that leaves SMs' block
+   slots to other contexts' kernels: the grid-stride kernels then take more
+   items per block). */
+static inline int64_t
+grid_cap (const gdp_ctx *ctx, int k) {
+  return (int64_t) ctx->nsm * (ctx->grid_limit > 0 ? std::min(k, ctx->grid_limit) : k);
+}
+
 static inline int
 fill_grid (gdp_ctx *ctx, int64_t count) {
-  return (int) std::max<int64_t>(1, std::min<int64_t>((count + 127) / 128, (int64_t) ctx->nsm * 16));
+  return (int) std::max<int64_t>(1, std::min<int64_t>((count + 127) / 128, grid_cap(ctx, 16)));
 }
 
 /* warp kinds: K lanes per pair, 128 / K pairs per block of 128 */
 static inline int
 warp_grid (gdp_ctx *ctx, int64_t count, int K) {
   const int per_block = 128 / K;
-  return (int) std::max<int64_t>(1, std::min<int64_t>((count + per_block - 1) / per_block, (int64_t) ctx->nsm * 16));
+  return (int) std::max<int64_t>(1, std::min<int64_t>((count + per_block - 1) / per_block, grid_cap(ctx, 16)));
 }
 
 template <int V, bool L>
@@ -1251,7 +1262,7 @@ launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_
   cudaEvent_t ev = nullptr;
   prof_begin(ctx, &ev, ks);
   if (ctx->tb_warp) {
-    const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, (int64_t) ctx->nsm * 16));
+    const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, grid_cap(ctx, 16)));
     traceback_warp_kernel<<<g, 128, 0, ks>>>(T);
   } else {
     traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, ks>>>(T);
@@ -1327,7 +1338,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       const int w32 = thread ? (k >> 2) / 3 : 0, pass = thread ? (k & 1) : 0;
       const bool second = (w32 == 1 && pass == 1) || warp8;
       if ((round == 0) == second || !ph.counts[k]) continue;
-      const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], (int64_t) ctx->nsm * 8))
+      const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], grid_cap(ctx, 8)))
                      : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
                      : warp8 ? warp_grid(ctx, ph.counts[k], WARP8_K[(k - FIRST_WARP8) % 3])
                              : fill_grid(ctx, ph.counts[k]);
@@ -1498,6 +1509,9 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "check_min_x") && value >= 1) ctx->check_min_x = (int) std::min<int64_t>(value, 1 << 30);
   else if (!strcmp(name, "wave_pairs") && value >= 1) ctx->wave = value;
   else if (!strcmp(name, "first_wave_pairs") && value >= 0) ctx->first_wave = value;
+  else if (!strcmp(name, "wave_priority") && value >= 0)
+    ctx->wave_prio = (int) std::min<int64_t>(value, std::max(ctx->nwave - 1, 0));
+  else if (!strcmp(name, "grid_blocks_per_sm") && value >= 0) ctx->grid_limit = (int) std::min<int64_t>(value, 64);
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1514,6 +1528,8 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "check_min_x")) *value = ctx->check_min_x;
   else if (!strcmp(name, "wave_pairs")) *value = ctx->wave;
   else if (!strcmp(name, "first_wave_pairs")) *value = ctx->first_wave;
+  else if (!strcmp(name, "wave_priority")) *value = ctx->wave_prio;
+  else if (!strcmp(name, "grid_blocks_per_sm")) *value = ctx->grid_limit;
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1630,7 +1646,7 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   if (rc != GDP_OK) return rc;
   CK(ctx, cudaEventRecord(sl.h2d_done, ctx->h2d));
   GDP_TEV(ctx->h2d, "h2d_end %lld", first);
-  sl.cs = ctx->wave_stream[std::min(wave_index, ctx->nwave - 1)];
+  sl.cs = ctx->wave_stream[std::min(ctx->wave_prio + wave_index, ctx->nwave - 1)];
   CK(ctx, cudaStreamWaitEvent(sl.cs, sl.h2d_done, 0));
   if (arena_ready) CK(ctx, cudaStreamWaitEvent(sl.cs, arena_ready, 0));
   GDP_TEV(sl.cs, "comp_begin %lld", first);

@@ -4,13 +4,18 @@
  * Requests (one or more alignment pairs each) arrive at any time from any
  * thread.  A request is admitted when the direction-matrix memory it needs
  * (the device words of its fills) fits into what the admitted, unfinished
- * requests leave of the budget; admitted requests that are waiting are
- * batched together in arrival order.  Each worker owns a context (its own
- * CUDA streams and buffers, the resident genome) and runs one batch at a
- * time, so with two or more workers a new batch is copied in, planned and
- * filled while the previous one traces back and copies out: requests that
- * arrive while others are on the GPU are admitted as memory frees up and
- * their work overlaps on the device.  Every pair is independent, so a
+ * requests leave of the budget.  Requests fall into two size classes by
+ * their longest stretch -- short reads and long ones (long reads, cDNA
+ * gaps) -- with
+ * one arrival-order queue each, and a batch takes the admissible waiting
+ * requests of one class: a lone long read needs ten times the time of a
+ * short one, and a short request batched with it would wait for it.  Each
+ * worker owns a context (its own CUDA streams and buffers, the resident
+ * genome) and runs one batch at a time; some workers take short batches
+ * only, the others long batches first and short ones when no long request
+ * waits, and short batches compute on a higher stream priority.  With two
+ * or more workers a new batch is copied in, planned and filled while
+ * another traces back and copies out.  Every pair is independent, so a
  * request's results do not depend on what it was batched with.
  *
  * A load generator (gdp_server_drive) submits single-pair requests at
@@ -69,6 +74,7 @@ struct Request {
   const char *arena = nullptr;
   int64_t n = 0;
   int64_t dir_bytes = 0;   /* direction-matrix bytes the request's fills hold */
+  int cls = 0;             /* size class: 0 short, 1 long */
   int64_t rec_slots = 0;   /* traceback record capacity it needs */
   clk::time_point t_submit;
   double latency_ms = 0;
@@ -113,7 +119,11 @@ struct gdp_server {
   int64_t max_batch_rec_bytes = (int64_t) 1 << 30;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<Request *> queue;
+  std::deque<Request *> queue[2];   /* waiting requests per size class, in arrival order */
+  int64_t short_max_length = 512;
+  int short_workers = 0;          /* workers 0 .. short_workers-1 take short batches only */
+  bool started = false;           /* a request was enqueued: the classes are fixed */
+  int long_blocks_per_sm = 2;     /* grid cap of long batches (0: none) */
   std::unordered_map<int64_t, Request *> owned;   /* submitted through the public API */
   int64_t next_id = 0;
   int64_t reserved = 0;           /* bytes of admitted, unfinished requests */
@@ -121,9 +131,23 @@ struct gdp_server {
   bool stop = false;
   /* statistics */
   int64_t st_batches = 0, st_pairs = 0, st_peak_reserved = 0, st_max_batch = 0;
+  int64_t st_cls_batches[2] = {0, 0}, st_cls_pairs[2] = {0, 0};
   double st_busy_s = 0;
 
   void worker (int w);
+  int class_of (const gdp_pair_t *p, int64_t n) const {
+    for (int64_t i = 0; i < n; i++)
+      if (p[i].rlength > short_max_length || p[i].glength > short_max_length) return 1;
+    return 0;
+  }
+  /* the class worker w takes a batch of now, or -1 (caller holds mu) */
+  int pick (int w) const {
+    auto ready = [&](int c) { return !queue[c].empty() && reserved + queue[c].front()->dir_bytes <= budget; };
+    if (short_workers > 0 && w < short_workers) return ready(0) ? 0 : -1;
+    if (short_workers > 0 && ready(1)) return 1;
+    if (ready(0)) return 0;
+    return ready(1) ? 1 : -1;
+  }
 };
 
 /* One worker: take the admitted head of the queue as a batch, align it on
@@ -139,19 +163,22 @@ gdp_server::worker (int w) {
   for (;;) {
     batch.clear();
     int64_t bytes = 0, npairs = 0, rec_slots = 0;
+    int cls = -1;
     {
       std::unique_lock<std::mutex> lk(mu);
-      cv_work.wait(lk, [&] {
-        return stop || (!queue.empty() && reserved + queue.front()->dir_bytes <= budget);
-      });
-      if (stop && queue.empty()) return;
-      if (queue.empty() || reserved + queue.front()->dir_bytes > budget) continue;
-      while (!queue.empty()) {
-        Request *r = queue.front();
+      cv_work.wait(lk, [&] { return stop || pick(w) >= 0; });
+      cls = pick(w);
+      if (cls < 0) {
+        if (stop) return;
+        continue;
+      }
+      std::deque<Request *> &q = queue[cls];
+      while (!q.empty()) {
+        Request *r = q.front();
         if (!batch.empty() && (npairs + r->n > max_batch_pairs || reserved + bytes + r->dir_bytes > budget ||
                                (rec_slots + r->rec_slots) * (int64_t) sizeof(gdp_rec_t) > max_batch_rec_bytes))
           break;
-        queue.pop_front();
+        q.pop_front();
         batch.push_back(r);
         bytes += r->dir_bytes;
         npairs += r->n;
@@ -202,7 +229,11 @@ gdp_server::worker (int w) {
         }
       }
       int64_t used = 0;
-      rc = gdp_align_batch(c, bpairs.data(), npairs, a, off, results.as<gdp_result_t>(), recs.as<gdp_rec_t>(),
+      /* long batches below short ones on the device, and on part of each SM */
+      rc = gdp_ctx_set_param(c, "wave_priority", cls == 0 ? 0 : (int64_t) 1 << 20);
+      if (rc == GDP_OK) rc = gdp_ctx_set_param(c, "grid_blocks_per_sm", cls == 0 ? 0 : long_blocks_per_sm);
+      if (rc == GDP_OK)
+        rc = gdp_align_batch(c, bpairs.data(), npairs, a, off, results.as<gdp_result_t>(), recs.as<gdp_rec_t>(),
                            std::max<int64_t>(rec_slots, 1), &used);
     }
     const gdp_result_t *res = results.as<gdp_result_t>();
@@ -247,6 +278,8 @@ gdp_server::worker (int w) {
       st_batches++;
       st_pairs += npairs;
       st_max_batch = std::max(st_max_batch, npairs);
+      st_cls_batches[cls]++;
+      st_cls_pairs[cls] += npairs;
       st_busy_s += std::chrono::duration<double>(t1 - t0).count();
     }
     cv_done.notify_all();
@@ -259,10 +292,13 @@ server_enqueue (gdp_server *s, Request *r) {
   {
     std::lock_guard<std::mutex> lk(s->mu);
     r->t_submit = clk::now();
-    s->queue.push_back(r);
+    r->cls = s->class_of(r->pairs, r->n);
+    s->started = true;
+    s->queue[r->cls].push_back(r);
     s->outstanding++;
   }
-  s->cv_work.notify_one();
+  /* the worker that takes this class may be any of them */
+  s->cv_work.notify_all();
 }
 
 extern "C" int
@@ -292,6 +328,7 @@ gdp_server_create (int device, int mode, int nworkers, int64_t dir_budget_bytes,
     }
     s->ctx.push_back(c);
   }
+  s->short_workers = nworkers >= 2 ? std::min((nworkers + 1) / 2, nworkers - 1) : 0;
   for (int w = 0; w < nworkers; w++) s->workers.emplace_back(&gdp_server::worker, s, w);
   *out = s;
   return GDP_OK;
@@ -433,4 +470,34 @@ gdp_server_destroy (gdp_server *s) {
   for (auto &kv : s->owned) delete kv.second;
   for (gdp_ctx *c : s->ctx) gdp_ctx_destroy(c);
   delete s;
+}
+
+extern "C" int
+gdp_server_set_classes (gdp_server *s, int64_t short_max_length, int short_workers) {
+  if (s == nullptr || short_max_length < 0 || short_workers < 0) return GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const int nw = (int) s->ctx.size();
+  /* before the first request: a request keeps the class it got */
+  if (s->started || (nw > 1 && short_workers >= nw)) return GDP_ERR_PARAM;
+  s->short_max_length = short_max_length;
+  s->short_workers = nw >= 2 ? short_workers : 0;
+  return GDP_OK;
+}
+
+extern "C" int
+gdp_server_class_of (gdp_server *s, const gdp_pair_t *pairs, int64_t npairs) {
+  if (s == nullptr || pairs == nullptr || npairs <= 0) return -GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(s->mu);
+  return s->class_of(pairs, npairs);
+}
+
+extern "C" int
+gdp_server_class_stats (gdp_server *s, int64_t *batches, int64_t *pairs) {
+  if (s == nullptr) return GDP_ERR_PARAM;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (int c = 0; c < 2; c++) {
+    if (batches) batches[c] = s->st_cls_batches[c];
+    if (pairs) pairs[c] = s->st_cls_pairs[c];
+  }
+  return GDP_OK;
 }

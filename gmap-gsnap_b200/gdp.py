@@ -145,6 +145,9 @@ def load(path=LIB_PATH):
     lib.gdp_server_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
                                      ctypes.POINTER(i64), dp]
     lib.gdp_server_destroy.argtypes = [vp]
+    lib.gdp_server_set_classes.argtypes = [vp, i64, i32]
+    lib.gdp_server_class_of.argtypes = [vp, vp, i64]
+    lib.gdp_server_class_stats.argtypes = [vp, vp, vp]
     ip = ctypes.POINTER(i32)
     lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
     lib.gdp_single_setup.argtypes = [vp, i32, i32, i32, i32]
@@ -526,8 +529,19 @@ class Server:
         busy = ctypes.c_double(0)
         self.lib.gdp_server_stats(self.h, ctypes.byref(b), ctypes.byref(p), ctypes.byref(m), ctypes.byref(pk),
                                   ctypes.byref(busy))
+        cb, cp = np.zeros(2, np.int64), np.zeros(2, np.int64)
+        self.lib.gdp_server_class_stats(self.h, _ptr(cb), _ptr(cp))
         return {"batches": b.value, "pairs": p.value, "max_batch_pairs": m.value,
-                "peak_reserved_bytes": pk.value, "busy_s": busy.value}
+                "peak_reserved_bytes": pk.value, "busy_s": busy.value,
+                "class_batches": cb.tolist(), "class_pairs": cp.tolist()}
+
+    def set_classes(self, short_max_length=512, short_workers=1):
+        return self.lib.gdp_server_set_classes(self.h, short_max_length, short_workers)
+
+    def classes(self, pairs):
+        """The size class (0 short, 1 long) of each pair as a one-pair request."""
+        return np.array([self.lib.gdp_server_class_of(self.h, _ptr(pairs[i:i + 1]), 1) for i in range(pairs.size)],
+                        dtype=np.int8)
 
 
 class GapQueue:

@@ -267,6 +267,13 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *   "first_wave_pairs" pairs of its first wave (0: wave_pairs / 16, at least
  *                    16,384); each next wave holds twice the one before,
  *                    up to wave_pairs
+ *   "wave_priority"  stream priority of a batch's first wave, 0 the highest
+ *                    (later waves step down from it); the serving loop
+ *                    runs its long-request batches below its short ones
+ *   "grid_blocks_per_sm" at most this many blocks per SM in the fill and
+ *                    traceback grids (0: no limit); the serving loop's long
+ *                    batches keep to part of each SM, so that short batches
+ *                    find block slots free
  * gdp_autotune times plan executions of a sample batch (device-resident
  * copies, the caller's pairs and arena) under candidate values of the first
  * six, one parameter at a time, and keeps the fastest; *best_ms gets the
@@ -362,11 +369,24 @@ int gdp_fill16_noalloc(int device, int mode, const gdp_pair_t *d_pairs, int64_t 
  * Serving loop (continuous batching).  A server owns `nworkers` contexts
  * on `device` (tables of `mode`), each holding the resident genome (may be
  * NULL).  Requests of one or more pairs are submitted from any thread and
- * admitted in arrival order while the direction-matrix memory of the
- * admitted, unfinished requests stays within `dir_budget_bytes` (0: 40 GB);
- * a worker takes every admitted waiting request (up to `max_batch_pairs`
- * pairs; 0: 131,072) as one batch.  With two or more workers, batches
- * overlap on the device.  Results do not depend on the batching.
+ * admitted while the direction-matrix memory of the admitted, unfinished
+ * requests stays within `dir_budget_bytes` (0: 40 GB).
+ *
+ * Size classes.  A request is short (class 0) when none of its pairs has
+ * a query or genome stretch longer than `short_max_length` (default 512
+ * bases), else long (class 1): a lone pair's time on the device follows
+ * its longest stretch (the fill's column steps run one after another).
+ * Each class has its own arrival-
+ * order queue, and a batch holds requests of one class only, so a short
+ * request never waits for a long one in its batch.  With two or more
+ * workers, the first `short_workers` (default: half, rounded up) take short
+ * batches only; the others take long batches and, when no long request is
+ * admissible, short ones.  Short batches compute on the highest stream
+ * priority, long batches on the lowest.  A worker takes every admissible
+ * waiting request of its class (up to `max_batch_pairs` pairs; 0: 131,072)
+ * as one batch.  gdp_server_set_classes changes the threshold and the
+ * split before the first submission.  Results do not depend on the
+ * batching.
  *
  * gdp_server_submit copies the request and returns its id (>= 0), or
  * -GDP_ERR_* when it is malformed; a request larger than the budget
@@ -394,6 +414,11 @@ int gdp_server_drive(gdp_server *server, const gdp_pair_t *pool, int64_t npool, 
                      double *latency_ms, double *elapsed_s);
 int gdp_server_stats(gdp_server *server, int64_t *batches, int64_t *pairs, int64_t *max_batch_pairs,
                      int64_t *peak_reserved_bytes, double *busy_s);
+int gdp_server_set_classes(gdp_server *server, int64_t short_max_length, int short_workers);
+/* The size class (0 short, 1 long) of a request of these pairs, or -GDP_ERR_PARAM. */
+int gdp_server_class_of(gdp_server *server, const gdp_pair_t *pairs, int64_t npairs);
+/* Batches and pairs run per class (arrays of 2). */
+int gdp_server_class_stats(gdp_server *server, int64_t *batches, int64_t *pairs);
 void gdp_server_destroy(gdp_server *server);
 
 /*

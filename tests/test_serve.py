@@ -192,3 +192,33 @@ def test_admission_respects_the_budget(gdplib, genome):
     assert all((r["status"] == 0).all() for r, _, _ in out)
     assert (rbig["status"] == 4).all()              # GDP_ERR_BUDGET
     assert 0 < st["peak_reserved_bytes"] <= budget
+
+
+def test_size_classes_batch_apart(gdplib, genome):
+    """Short and long requests are batched apart (gdp_server_class_stats):
+    every batch holds one class, short batches serve short requests only
+    when long workers exist, results equal one direct batch, and short
+    requests wait less than long ones under the same load."""
+    g, blocks = genome
+    pool, arena = gdp.make_resident_pairs(gdplib, gdp.WL_MIX, 61, g, 600)
+    srv = gdp.Server(gdplib, workers=4, blocks=blocks, length=GENOME_LEN)
+    assert srv.set_classes(512, 2) == 0
+    cls = srv.classes(pool)
+    longest = np.maximum(pool["rlength"], pool["glength"])
+    assert np.array_equal(cls, (longest > 512).astype(np.int8))
+    assert 50 < int((cls == 1).sum()) < 550
+    lat, elapsed, res = srv.drive(pool, arena, 3000, rate=20000.0, seed=5, want_results=True)
+    assert srv.set_classes(512, 1) == 3        # not after requests were submitted
+    st = srv.stats()
+    srv.close()
+    assert st["class_pairs"][0] + st["class_pairs"][1] == st["pairs"] == 3000
+    assert st["class_pairs"][1] == int((cls[np.arange(3000) % pool.size] == 1).sum())
+    assert min(st["class_batches"]) > 0 and sum(st["class_batches"]) == st["batches"]
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, None, GENOME_LEN)
+    rd, _ = ctx.align(pool, arena)
+    ctx.close()
+    for k in range(0, 3000, pool.size):
+        assert _same(res[k:k + pool.size], rd[:min(pool.size, 3000 - k)]), k
+    c = cls[np.arange(3000) % pool.size]
+    assert np.median(lat[c == 0]) < np.median(lat[c == 1])
