@@ -1011,7 +1011,10 @@ def run_gdp(args):
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / e2e_steps)
     e2e_value = total_cells / (e2e_ms * 1e-3) / 1e9
     h2d = pairs.nbytes + arena.nbytes
-    d2h = results.nbytes + int(used.value) * gdp.REC_DTYPE.itemsize
+    # what the call copied device to host: the results and the records as
+    # runs (the host rebuilds the 12-byte records from them)
+    d2h = ctx.get_param("last_d2h_bytes")
+    records_bytes = int(used.value) * gdp.REC_DTYPE.itemsize
     e2e_bad = int((results["status"] != 0).sum())
 
     cpu = None
@@ -1068,7 +1071,9 @@ def run_gdp(args):
                        "graph": True, "autotune": tuned},
             "alignments_per_s": round(total_pairs * args.steps / (ms_max * 1e-3), 1),
             "e2e": {"value": round(e2e_value, 3), "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3), "steps": e2e_steps,
+                    "d2h_bytes_per_step": int(d2h), "records_rebuilt_bytes": records_bytes,
+                    "record_transport": "runs" if ctx.get_param("record_runs") else "records",
+                    "ms_per_step": round(e2e_ms, 3), "steps": e2e_steps,
                     "host_buffers": "pinned", "bad_status_pairs": e2e_bad},
             "roofline": {"bound": "int", "kernel": top_name, "instantiations": top_members,
                          "cells_per_step": int(top_cells),

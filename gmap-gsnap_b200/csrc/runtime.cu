@@ -47,6 +47,7 @@
 #include "fill_thread.cuh"
 #include "traceback.cuh"
 #include "traceback_warp.cuh"
+#include "rec_runs.h"
 
 #define GDP_VERSION "gdp-b200 0.2"
 
@@ -274,6 +275,11 @@ struct Slot {
   cudaStream_t cs = nullptr;
   DevBuf scratch, scratch8;
   HostBuf total;           /* pinned int64: records of the wave */
+  /* the record-run transport (rec_runs.h): the wave's encoded records, each
+     pair's stream offset, and their pinned host copies */
+  DevBuf enc, enc_off;
+  HostBuf h_enc, h_encoff, enc_total;
+  bool runs = false;       /* the wave's records leave as runs */
   cudaEvent_t h2d_done = nullptr, comp_done = nullptr, out_done = nullptr, total_ready = nullptr;
   int64_t first = 0, count = 0, rec_base = 0;
   bool busy = false;
@@ -313,6 +319,9 @@ struct gdp_ctx {
   DevBuf arena, scratch, scratch8;
   Slot slot[NSLOTS];
   WorkPool pool;            /* the planner's host threads */
+  WorkPool xpool;           /* the copy-out side's host threads (record-run expansion) */
+  bool record_runs = true;  /* gdp_align_batch's records leave the device as runs */
+  int64_t last_d2h = 0;     /* bytes the last gdp_align_batch copied device to host */
   std::atomic<int64_t> launches{0};
   std::string err;
   std::mutex mu;
@@ -440,6 +449,7 @@ slot_release (Slot &sl) {
   sl.d.release();
   sl.h.release();
   sl.pairs.release(); sl.results.release(); sl.recs.release(); sl.total.release();
+  sl.enc.release(); sl.enc_off.release(); sl.h_enc.release(); sl.h_encoff.release(); sl.enc_total.release();
   if (sl.h2d_done) cudaEventDestroy(sl.h2d_done);
   if (sl.comp_done) cudaEventDestroy(sl.comp_done);
   if (sl.out_done) cudaEventDestroy(sl.out_done);
@@ -1451,6 +1461,73 @@ compact_records (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, gdp_result_t *d_
   return GDP_OK;
 }
 
+/* The record-run stream length of each pair of a wave (one thread per
+   pair, its records as compacted); len[n] = 0, so that the exclusive scan's
+   last entry is the total. */
+__global__ void __launch_bounds__(128)
+run_size_kernel (const gdp_result_t *res, const gdp_pair_t *pairs, const char *arena, const gdp_rec_t *recs,
+                 int64_t n, int64_t *len) {
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t) gridDim.x * blockDim.x) {
+    int64_t l = 0;
+    if (i < n) {
+      const int nr = res[i].nrecs;
+      if (nr > 0) {
+        const gdp_pair_t p = pairs[i];
+        l = rec_encode(run_seqs(p, arena), recs + res[i].rec_offset, nr, (p.flags & GDP_FLAG_GWINDOW) != 0,
+                       nullptr);
+      }
+    }
+    len[i] = l;
+  }
+}
+
+/* Writes each pair's stream at off[i]; the total goes to a mapped host
+   word. */
+__global__ void __launch_bounds__(128)
+run_write_kernel (const gdp_result_t *res, const gdp_pair_t *pairs, const char *arena, const gdp_rec_t *recs,
+                  int64_t n, const int64_t *off, uint8_t *out, int64_t *total_host) {
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+    const int nr = res[i].nrecs;
+    if (nr > 0) {
+      const gdp_pair_t p = pairs[i];
+      rec_encode(run_seqs(p, arena), recs + res[i].rec_offset, nr, (p.flags & GDP_FLAG_GWINDOW) != 0, out + off[i]);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *(volatile int64_t *) total_host = off[n];
+    __threadfence_system();
+  }
+}
+
+/* Encodes a wave's compacted records as runs, on its compute stream. */
+static int
+encode_runs (gdp_ctx *ctx, Slot &sl, const char *d_arena) {
+  const int64_t n = sl.count;
+  cudaStream_t s = sl.cs;
+  CK(ctx, sl.enc_off.ensure((2 * n + 2) * sizeof(int64_t)));
+  CK(ctx, sl.enc.ensure(std::max<int64_t>(sl.h.total_recs, 1) * (1 + (int64_t) sizeof(gdp_rec_t))));
+  CK(ctx, sl.enc_total.ensure(sizeof(int64_t)));
+  *(volatile int64_t *) sl.enc_total.p = 0;
+  int64_t *total_dev = nullptr;
+  CK(ctx, cudaHostGetDevicePointer((void **) &total_dev, sl.enc_total.p, 0));
+  int64_t *len = sl.enc_off.as<int64_t>() + n + 1, *off = sl.enc_off.as<int64_t>();
+  const gdp_result_t *res = sl.results.as<gdp_result_t>();
+  const gdp_pair_t *pairs = sl.pairs.as<gdp_pair_t>();
+  const gdp_rec_t *recs = sl.recs.as<gdp_rec_t>();
+  const int grid = (int) std::max<int64_t>(1, std::min<int64_t>((n + 128) / 128, (int64_t) ctx->nsm * 16));
+  run_size_kernel<<<grid, 128, 0, s>>>(res, pairs, d_arena, recs, n, len);
+  ctx->launches++;
+  size_t tmp = 0;
+  CK(ctx, cub::DeviceScan::ExclusiveSum(nullptr, tmp, len, off, (int) (n + 1), s));
+  CK(ctx, sl.d.cub_tmp.ensure(std::max<size_t>(tmp, 16)));
+  CK(ctx, cub::DeviceScan::ExclusiveSum(sl.d.cub_tmp.p, tmp, len, off, (int) (n + 1), s));
+  ctx->launches++;
+  run_write_kernel<<<grid, 128, 0, s>>>(res, pairs, d_arena, recs, n, off, sl.enc.as<uint8_t>(), total_dev);
+  ctx->launches++;
+  CK(ctx, cudaGetLastError());
+  return GDP_OK;
+}
+
 extern "C" int
 gdp_plan_execute (gdp_ctx *ctx, gdp_plan *pl, const gdp_pair_t *d_pairs, const char *d_arena,
                   gdp_result_t *d_results, gdp_rec_t *d_recs) {
@@ -1497,6 +1574,23 @@ gdp_plan_use_graph (gdp_plan *pl, int on) {
 /* Tunable routing parameters and the autotuner                        */
 /* ------------------------------------------------------------------ */
 
+/* The record-run codec on the host (rec_runs.h), for callers that move
+   records elsewhere and for tests. */
+extern "C" int64_t
+gdp_runs_encode (const gdp_pair_t *pair, const char *arena, const gdp_rec_t *recs, int32_t nrecs, uint8_t *out) {
+  if (pair == nullptr || arena == nullptr || nrecs < 0 || (nrecs > 0 && recs == nullptr)) return -GDP_ERR_PARAM;
+  return rec_encode(run_seqs(*pair, arena), recs, nrecs, (pair->flags & GDP_FLAG_GWINDOW) != 0, out);
+}
+
+extern "C" int
+gdp_runs_decode (const gdp_pair_t *pair, const char *arena, const uint8_t *in, int64_t len, gdp_rec_t *recs,
+                 int32_t nrecs) {
+  if (pair == nullptr || arena == nullptr || nrecs < 0 || len < 0 || (len > 0 && in == nullptr) ||
+      (nrecs > 0 && recs == nullptr))
+    return GDP_ERR_PARAM;
+  return rec_decode(run_seqs(*pair, arena), in, len, recs, nrecs) ? GDP_OK : GDP_ERR_PARAM;
+}
+
 extern "C" int
 gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   if (ctx == nullptr || name == nullptr) return GDP_ERR_PARAM;
@@ -1512,6 +1606,7 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "wave_priority") && value >= 0)
     ctx->wave_prio = (int) std::min<int64_t>(value, std::max(ctx->nwave - 1, 0));
   else if (!strcmp(name, "grid_blocks_per_sm") && value >= 0) ctx->grid_limit = (int) std::min<int64_t>(value, 64);
+  else if (!strcmp(name, "record_runs")) ctx->record_runs = value != 0;
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1530,6 +1625,8 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "first_wave_pairs")) *value = ctx->first_wave;
   else if (!strcmp(name, "wave_priority")) *value = ctx->wave_prio;
   else if (!strcmp(name, "grid_blocks_per_sm")) *value = ctx->grid_limit;
+  else if (!strcmp(name, "record_runs")) *value = ctx->record_runs ? 1 : 0;
+  else if (!strcmp(name, "last_d2h_bytes")) *value = ctx->last_d2h;
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1662,6 +1759,15 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   rc = compact_records(ctx, sl.h, sl.d, sl.results.as<gdp_result_t>(), sl.d.slots.as<gdp_rec_t>(),
                        sl.recs.as<gdp_rec_t>(), total_dev, sl.cs);
   if (rc != GDP_OK) return rc;
+  /* runs only pay where the host holds the genome characters: not for a
+     wave whose every pair has its window written on the device */
+  sl.runs = false;
+  if (ctx->record_runs)
+    for (int64_t i = first; i < first + count && !sl.runs; i++) sl.runs = !(pairs[i].flags & GDP_FLAG_GWINDOW);
+  if (sl.runs) {
+    rc = encode_runs(ctx, sl, ctx->arena.as<char>());
+    if (rc != GDP_OK) return rc;
+  }
   GDP_TEV(sl.cs, "comp_end %lld", first);
   CK(ctx, cudaEventRecord(sl.total_ready, sl.cs));
   CK(ctx, cudaEventRecord(sl.comp_done, sl.cs));
@@ -1678,10 +1784,13 @@ add_rec_base_kernel (gdp_result_t *res, int64_t n, int64_t base) {
 
 /* Waits for the wave's record count and queues its results and records
    out (records at *base).  The copy stream takes waves in order, so a wave
-   still computing never holds up the copies of an earlier one. */
+   still computing never holds up the copies of an earlier one.  A wave
+   whose records travel as runs (rec_runs.h) copies its streams out instead
+   and rebuilds the records into recs on the context's host threads before
+   the slot is free again. */
 static int
-slot_finish (gdp_ctx *ctx, Slot &sl, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs, int64_t *base,
-             bool *overflow) {
+slot_finish (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, const char *arena, gdp_result_t *results,
+             gdp_rec_t *recs, int64_t max_recs, int64_t *base, bool *overflow) {
   GDP_TRACE_BEGIN(t0);
   CK(ctx, cudaEventSynchronize(sl.total_ready));
   GDP_TRACE_END(t0, "wait_total");
@@ -1694,19 +1803,57 @@ slot_finish (gdp_ctx *ctx, Slot &sl, gdp_result_t *results, gdp_rec_t *recs, int
   }
   CK(ctx, cudaMemcpyAsync(results + sl.first, sl.results.p, sl.count * sizeof(gdp_result_t), cudaMemcpyDeviceToHost,
                           ctx->d2h));
+  ctx->last_d2h += sl.count * (int64_t) sizeof(gdp_result_t);
   const int64_t total = sl.h.n > 0 ? *(volatile int64_t *) sl.total.p : 0;
+  bool expand = false;
   if (total > 0) {
     if (recs == nullptr || *base + total > max_recs) {
       *overflow = true;
+    } else if (sl.runs) {
+      const int64_t bytes = *(volatile int64_t *) sl.enc_total.p;
+      CK(ctx, sl.h_enc.ensure(std::max<int64_t>(bytes, 16)));
+      CK(ctx, sl.h_encoff.ensure((sl.count + 1) * sizeof(int64_t)));
+      GDP_TEV(ctx->d2h, "runs_begin %lld", sl.first);
+      CK(ctx, cudaMemcpyAsync(sl.h_enc.p, sl.enc.p, bytes, cudaMemcpyDeviceToHost, ctx->d2h));
+      CK(ctx, cudaMemcpyAsync(sl.h_encoff.p, sl.enc_off.p, (sl.count + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                              ctx->d2h));
+      GDP_TEV(ctx->d2h, "runs_end %lld", sl.first);
+      ctx->last_d2h += bytes + (sl.count + 1) * (int64_t) sizeof(int64_t);
+      expand = true;
     } else {
       GDP_TEV(ctx->d2h, "recs_begin %lld", sl.first);
       CK(ctx, cudaMemcpyAsync(recs + *base, sl.recs.p, total * sizeof(gdp_rec_t), cudaMemcpyDeviceToHost, ctx->d2h));
       GDP_TEV(ctx->d2h, "recs_end %lld", sl.first);
+      ctx->last_d2h += total * (int64_t) sizeof(gdp_rec_t);
     }
   }
   CK(ctx, cudaEventRecord(sl.out_done, ctx->d2h));
   sl.rec_base = *base;
   *base += total;
+  if (expand) {
+    /* the records of each pair from its stream, on the copy-out side's
+       threads; the results (with batch-wide record offsets) are on the host
+       once the copies above are done */
+    GDP_TRACE_BEGIN(t1);
+    CK(ctx, cudaEventSynchronize(sl.out_done));
+    const gdp_pair_t *wp = pairs + sl.first;
+    const gdp_result_t *wr = results + sl.first;
+    const uint8_t *enc = sl.h_enc.as<uint8_t>();
+    const int64_t *off = sl.h_encoff.as<int64_t>();
+    const int64_t n = sl.count;
+    const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, n / 4096));
+    std::atomic<int> bad{0};
+    parallel_chunks(ctx->xpool, n, nt, [&](int64_t lo, int64_t hi, int) {
+      for (int64_t i = lo; i < hi; i++) {
+        const int nr = wr[i].nrecs;
+        if (nr <= 0) continue;
+        if (!rec_decode(run_seqs(wp[i], arena), enc + off[i], off[i + 1] - off[i], recs + wr[i].rec_offset, nr))
+          bad.store(1);
+      }
+    });
+    GDP_TRACE_END(t1, "expand");
+    if (bad.load()) return set_err(ctx, "record runs: a stream did not rebuild its records", cudaErrorUnknown);
+  }
   return GDP_OK;
 }
 
@@ -1716,6 +1863,7 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
   if (nrecs_used) *nrecs_used = 0;
+  ctx->last_d2h = 0;
   if (n <= 0) return GDP_OK;
   /* the previous batch may still be reading the arena */
   for (int s = 0; s < NSLOTS; s++) CK(ctx, cudaEventSynchronize(ctx->slot[s].out_done));
@@ -1815,7 +1963,8 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   int out_rc = GDP_OK;
   auto hand_out = [&](int k) {
     Slot &o = ctx->slot[k];
-    const int r = out_rc == GDP_OK ? slot_finish(ctx, o, results, recs, max_recs, &base, &overflow) : out_rc;
+    const int r = out_rc == GDP_OK ? slot_finish(ctx, o, pairs, arena, results, recs, max_recs, &base, &overflow)
+                                   : out_rc;
     std::lock_guard<std::mutex> g(m);
     if (r != GDP_OK) out_rc = r;
     o.busy = false;

@@ -152,6 +152,9 @@ def load(path=LIB_PATH):
     lib.gdp_endpoint_combine.argtypes = [vp, vp, i32, i32, i32, i32, ip, ip, ip]
     lib.gdp_single_setup.argtypes = [vp, i32, i32, i32, i32]
     lib.gdp_single_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_runs_encode.argtypes = [vp, vp, vp, i32, vp]
+    lib.gdp_runs_encode.restype = i64
+    lib.gdp_runs_decode.argtypes = [vp, vp, vp, i64, vp, i32]
     lib.gdp_end_setup.argtypes = [vp, i32, i32, i32]
     lib.gdp_end_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
     lib.gdp_gap_queue_create.argtypes = [i32, i32, i64, i64, vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
@@ -221,6 +224,27 @@ def endpoint_combine(lib, upper, lower, jump_late, qend, precision, rlength):
     if rc != 0:
         raise RuntimeError(f"gdp_endpoint_combine: {STATUS.get(rc, rc)}")
     return fs.value, br.value, bc.value
+
+
+def runs_encode(lib, pair, arena, recs):
+    """The record-run stream of one pair's records (gdp_runs_encode)."""
+    p = np.ascontiguousarray(pair, dtype=PAIR_DTYPE).reshape(1)
+    r = np.ascontiguousarray(recs, dtype=REC_DTYPE)
+    n = lib.gdp_runs_encode(_ptr(p), _ptr(arena), _ptr(r), r.size, None)
+    if n < 0:
+        raise RuntimeError("gdp_runs_encode: bad arguments")
+    out = np.zeros(max(n, 1), np.uint8)
+    lib.gdp_runs_encode(_ptr(p), _ptr(arena), _ptr(r), r.size, _ptr(out))
+    return out[:n]
+
+
+def runs_decode(lib, pair, arena, stream, nrecs):
+    """The records a run stream rebuilds (gdp_runs_decode), or None."""
+    p = np.ascontiguousarray(pair, dtype=PAIR_DTYPE).reshape(1)
+    out = np.zeros(max(nrecs, 1), dtype=REC_DTYPE)
+    st = np.ascontiguousarray(stream, dtype=np.uint8)
+    rc = lib.gdp_runs_decode(_ptr(p), _ptr(arena), _ptr(st), st.size, _ptr(out), nrecs)
+    return out[:nrecs] if rc == 0 else None
 
 
 def tables(lib, mode=0):

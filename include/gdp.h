@@ -186,6 +186,21 @@ typedef struct gdp_result {
 int gdp_endpoint_combine(const gdp_result_t *upper, const gdp_result_t *lower, int jump_late, int qend,
                          int precision, int rlength, int *finalscore, int *bestr, int *bestc);
 
+/*
+ * The record-run codec: the records of one pair (push order) as a byte
+ * stream, one byte for most records -- each follows from the record before
+ * it and the pair's sequences in `arena` -- and 13 bytes for the others.
+ * gdp_runs_encode returns the stream's length (out may be NULL to size
+ * it), or -GDP_ERR_PARAM; gdp_runs_decode rebuilds the records byte for
+ * byte from the same pair and arena (GDP_ERR_PARAM for a malformed
+ * stream).  Pairs with GDP_FLAG_GWINDOW encode every record whole.
+ * gdp_align_batch uses the same codec to bring records to the host.
+ */
+int64_t gdp_runs_encode(const gdp_pair_t *pair, const char *arena, const gdp_rec_t *recs, int32_t nrecs,
+                        uint8_t *out);
+int gdp_runs_decode(const gdp_pair_t *pair, const char *arena, const uint8_t *in, int64_t len, gdp_rec_t *recs,
+                    int32_t nrecs);
+
 typedef struct gdp_ctx gdp_ctx;
 
 /* Library version string. */
@@ -274,6 +289,12 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *                    traceback grids (0: no limit); the serving loop's long
  *                    batches keep to part of each SM, so that short batches
  *                    find block slots free
+ *   "record_runs"    1 (default): gdp_align_batch's records leave the device
+ *                    as runs -- one byte for most records, which follow from
+ *                    the one before and the pair's sequences -- and are
+ *                    rebuilt byte for byte on the host; 0: as 12-byte records
+ * gdp_ctx_get_param also reads "last_d2h_bytes": the bytes the last
+ * gdp_align_batch copied from the device to the host.
  * gdp_autotune times plan executions of a sample batch (device-resident
  * copies, the caller's pairs and arena) under candidate values of the first
  * six, one parameter at a time, and keeps the fastest; *best_ms gets the

@@ -207,7 +207,7 @@ def test_size_classes_batch_apart(gdplib, genome):
     longest = np.maximum(pool["rlength"], pool["glength"])
     assert np.array_equal(cls, (longest > 512).astype(np.int8))
     assert 50 < int((cls == 1).sum()) < 550
-    lat, elapsed, res = srv.drive(pool, arena, 3000, rate=20000.0, seed=5, want_results=True)
+    lat, elapsed, res = srv.drive(pool, arena, 3000, rate=5000.0, seed=5, want_results=True)
     assert srv.set_classes(512, 1) == 3        # not after requests were submitted
     st = srv.stats()
     srv.close()
