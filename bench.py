@@ -635,7 +635,7 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=4
             "requests": "single pairs of the 70/25/5 short/long/cDNA mix, device-extracted windows",
             "workers": workers, "dir_budget_gb": 40, "sweep": rows, "knee_offered_per_s": knee,
             "classes": {"short": "longest stretch <= 512 nt, batched apart on the higher stream priority, "
-                                 "served by half the workers (and by the others when no long request waits)",
+                                 "served by three workers in four (and by the others when no long request waits)",
                         "short_share": round(float((cls == 0).mean()), 3),
                         "class_batches": st["class_batches"], "class_pairs": st["class_pairs"]},
             "batches": st["batches"], "max_batch_pairs": st["max_batch_pairs"],

@@ -17,6 +17,7 @@
  *
  * Stream of one pair, byte by byte:
  *   0xFF          escape: the next 12 bytes are the record as it is;
+ *   (t << 4) | 12 token t (0..11) c + 1 times, c the next byte (1..256);
  *   (r << 4) | t  token t (0..11) r + 1 times (1..16).
  * Token t: move t >> 2 (0: both positions step, 1: querypos steps, 2:
  * genomepos steps), kind t & 3 (0 '*', 1 ':', 2 ' ' with the three
@@ -40,7 +41,25 @@
 #define GDP_HD inline
 #endif
 
-enum { RUN_ESCAPE = 0xFF, RUN_TOKENS = 12, RUN_MAX_REPEAT = 16 };
+/* a 32-bit word of a record, which may alias the record's fields */
+typedef uint32_t __attribute__((__may_alias__)) run_word;
+
+enum { RUN_ESCAPE = 0xFF, RUN_TOKENS = 12, RUN_LONG = 12, RUN_SHORT_REPEAT = 16, RUN_MAX_REPEAT = 256 };
+
+/* Writes token t repeated reps times (1..RUN_MAX_REPEAT) at out[len] when
+   out is not NULL; returns the bytes it takes. */
+GDP_HD int
+run_put (uint8_t *out, int64_t len, int t, int reps) {
+  if (reps <= RUN_SHORT_REPEAT) {
+    if (out) out[len] = (uint8_t) (((reps - 1) << 4) | t);
+    return 1;
+  }
+  if (out) {
+    out[len] = (uint8_t) ((t << 4) | RUN_LONG);
+    out[len + 1] = (uint8_t) (reps - 1);
+  }
+  return 2;
+}
 
 /* The sequences of one pair, as forward arena bytes. */
 struct RunSeqs {
@@ -146,10 +165,7 @@ rec_encode (const RunSeqs &s, const gdp_rec_t *recs, int n, bool whole, uint8_t 
     if (t >= 0 && t == pend && reps < RUN_MAX_REPEAT) {
       reps++;
     } else {
-      if (pend >= 0) {
-        if (out) out[len] = (uint8_t) (((reps - 1) << 4) | pend);
-        len++;
-      }
+      if (pend >= 0) len += run_put(out, len, pend, reps);
       pend = -1;
       reps = 0;
       if (t >= 0) {
@@ -165,10 +181,7 @@ rec_encode (const RunSeqs &s, const gdp_rec_t *recs, int n, bool whole, uint8_t 
     }
     prev = rec;
   }
-  if (pend >= 0) {
-    if (out) out[len] = (uint8_t) (((reps - 1) << 4) | pend);
-    len++;
-  }
+  if (pend >= 0) len += run_put(out, len, pend, reps);
   return len;
 }
 
@@ -190,7 +203,12 @@ rec_decode (const RunSeqs &s, const uint8_t *in, int64_t len, gdp_rec_t *recs, i
       recs[k++] = prev;
       continue;
     }
-    const int t = b & 15, reps = (b >> 4) + 1;
+    int t = b & 15, reps = (b >> 4) + 1;
+    if (t == RUN_LONG) {
+      if (at >= len) return false;
+      t = b >> 4;
+      reps = in[at++] + 1;
+    }
     if (t >= RUN_TOKENS || k + reps > n) return false;
     /* rec_predict reps times: positions move by (dq, dg) a step, and so do
        their arena indices; they are monotonic, so the first and the last
@@ -216,14 +234,27 @@ rec_decode (const RunSeqs &s, const uint8_t *in, int64_t len, gdp_rec_t *recs, i
       int32_t gi = run_index(prev.genomepos + dg, s.genomeoffset, s.glength, s.revp);
       if (gi < 0 || run_index(prev.genomepos + reps * dg, s.genomeoffset, s.glength, s.revp) < 0) return false;
       x.comp = kind == 0 ? '*' : kind == 1 ? ':' : ' ';
-      for (int r = 0; r < reps; r++, qi += dq, gi += dg) {
-        x.querypos += dq;
-        x.genomepos += dg;
-        x.cdna = s.rseq[qi];
-        x.genome = s.gseq[gi];
-        x.genomealt = s.galt[gi];
-        recs[k++] = x;
+      /* the records as 32-bit words: two positions, then the four
+         characters (cdna, comp, genome, genomealt in memory order) */
+      const uint32_t cmp = (uint32_t) (uint8_t) x.comp << 8;
+      run_word *w = reinterpret_cast<run_word *>(recs + k);
+      const uint8_t *rq = reinterpret_cast<const uint8_t *>(s.rseq) + qi;
+      const uint8_t *gg = reinterpret_cast<const uint8_t *>(s.gseq) + gi;
+      const uint8_t *ga = reinterpret_cast<const uint8_t *>(s.galt) + gi;
+      uint32_t qp = (uint32_t) x.querypos, gp = (uint32_t) x.genomepos;
+      for (int r = 0; r < reps; r++, w += 3) {
+        qp += (uint32_t) dq;
+        gp += (uint32_t) dg;
+        w[0] = qp;
+        w[1] = gp;
+        w[2] = (uint32_t) rq[r * dq] | cmp | (uint32_t) gg[r * dg] << 16 | (uint32_t) ga[r * dg] << 24;
       }
+      k += reps;
+      x.querypos = (int32_t) qp;
+      x.genomepos = (int32_t) gp;
+      x.cdna = (char) rq[(reps - 1) * dq];
+      x.genome = (char) gg[(reps - 1) * dg];
+      x.genomealt = (char) ga[(reps - 1) * dg];
     }
     prev = x;
   }

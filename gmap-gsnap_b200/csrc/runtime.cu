@@ -280,6 +280,7 @@ struct Slot {
   DevBuf enc, enc_off;
   HostBuf h_enc, h_encoff, enc_total;
   bool runs = false;       /* the wave's records leave as runs */
+  bool expand = false;     /* its runs are on their way to the host, not yet rebuilt */
   cudaEvent_t h2d_done = nullptr, comp_done = nullptr, out_done = nullptr, total_ready = nullptr;
   int64_t first = 0, count = 0, rec_base = 0;
   bool busy = false;
@@ -297,6 +298,11 @@ struct gdp_ctx {
   cudaStream_t h2d = nullptr, d2h = nullptr;
   /* the one-warp/one-CTA-per-pair fill kinds run beside the thread kinds */
   cudaStream_t side[2] = {nullptr, nullptr};
+  /* the side streams of the wave streams, each at its wave stream's
+     priority: a wave's lane-group, CTA and early 8-bit kinds run beside its
+     thread kinds with the same priority, and waves on different streams do
+     not queue behind one another's side kernels */
+  cudaStream_t wave_side[GDP_MAX_WAVE_STREAMS][2] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
@@ -320,7 +326,8 @@ struct gdp_ctx {
   Slot slot[NSLOTS];
   WorkPool pool;            /* the planner's host threads */
   WorkPool xpool;           /* the copy-out side's host threads (record-run expansion) */
-  bool record_runs = true;  /* gdp_align_batch's records leave the device as runs */
+  int record_runs = 0;      /* gdp_align_batch's records as runs: 0 never, 1 every wave, 2 the later waves */
+  int runs_from_wave = 5;   /* record_runs 2: the first wave whose records leave as runs */
   int64_t last_d2h = 0;     /* bytes the last gdp_align_batch copied device to host */
   std::atomic<int64_t> launches{0};
   std::string err;
@@ -486,6 +493,9 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
     if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
+  for (int w = 0; w < GDP_MAX_WAVE_STREAMS; w++)
+    for (int k = 0; k < 2; k++)
+      if (ctx->wave_side[w][k]) cudaStreamDestroy(ctx->wave_side[w][k]);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   free(ctx->h_tab);
   delete ctx;
@@ -518,8 +528,9 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
   ctx->nwave = std::max(1, std::min(GDP_MAX_WAVE_STREAMS, least - greatest + 1));
   for (int k = 0; k < ctx->nwave; k++) {
-    if (cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
-      ctx->wave_stream[k] = nullptr;
+    if (cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->wave_side[k][0], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->wave_side[k][1], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
       gdp_ctx_destroy(ctx);
       return GDP_ERR_CUDA;
     }
@@ -1290,6 +1301,9 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
           gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t stream = nullptr, DevBuf *scratch_buf = nullptr,
           DevBuf *scratch8_buf = nullptr) {
   cudaStream_t s = stream ? stream : ctx->stream;
+  cudaStream_t *side_s = ctx->side;
+  for (int w = 0; w < ctx->nwave; w++)
+    if (s == ctx->wave_stream[w]) side_s = ctx->wave_side[w];
   DevBuf &scratch = scratch_buf ? *scratch_buf : ctx->scratch;
   DevBuf &scratch8 = scratch8_buf ? *scratch8_buf : ctx->scratch8;   /* the early 8-bit kinds' own */
   const int64_t n = ph.n;
@@ -1334,7 +1348,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   for (int round = 0; round < 2; round++) {
     if (round == 1 && forked) {
       for (int q = 0; q < 2; q++) {
-        CK(ctx, cudaEventRecord(ctx->join_ev[q], ctx->side[q]));
+        CK(ctx, cudaEventRecord(ctx->join_ev[q], side_s[q]));
         CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
       }
     }
@@ -1392,15 +1406,15 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       cudaStream_t ks = s;
       if (warp || cta || early8) {
         if (!forked) {
-          for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(ctx->side[q], ctx->fork_ev, 0));
+          for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(side_s[q], ctx->fork_ev, 0));
           forked = true;
         }
         if (early8) {
           /* the early 8-bit kinds share one scratch: they stay in order on
              one side stream */
-          ks = ctx->side[0];
+          ks = side_s[0];
         } else {
-          ks = ctx->side[side];
+          ks = side_s[side];
           side ^= 1;
         }
       }
@@ -1606,7 +1620,8 @@ gdp_ctx_set_param (gdp_ctx *ctx, const char *name, int64_t value) {
   else if (!strcmp(name, "wave_priority") && value >= 0)
     ctx->wave_prio = (int) std::min<int64_t>(value, std::max(ctx->nwave - 1, 0));
   else if (!strcmp(name, "grid_blocks_per_sm") && value >= 0) ctx->grid_limit = (int) std::min<int64_t>(value, 64);
-  else if (!strcmp(name, "record_runs")) ctx->record_runs = value != 0;
+  else if (!strcmp(name, "record_runs") && value >= 0 && value <= 2) ctx->record_runs = (int) value;
+  else if (!strcmp(name, "runs_from_wave") && value >= 0) ctx->runs_from_wave = (int) std::min<int64_t>(value, 1 << 20);
   else return GDP_ERR_PARAM;
   return GDP_OK;
 }
@@ -1625,7 +1640,8 @@ gdp_ctx_get_param (gdp_ctx *ctx, const char *name, int64_t *value) {
   else if (!strcmp(name, "first_wave_pairs")) *value = ctx->first_wave;
   else if (!strcmp(name, "wave_priority")) *value = ctx->wave_prio;
   else if (!strcmp(name, "grid_blocks_per_sm")) *value = ctx->grid_limit;
-  else if (!strcmp(name, "record_runs")) *value = ctx->record_runs ? 1 : 0;
+  else if (!strcmp(name, "record_runs")) *value = ctx->record_runs;
+  else if (!strcmp(name, "runs_from_wave")) *value = ctx->runs_from_wave;
   else if (!strcmp(name, "last_d2h_bytes")) *value = ctx->last_d2h;
   else return GDP_ERR_PARAM;
   return GDP_OK;
@@ -1762,7 +1778,13 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   /* runs only pay where the host holds the genome characters: not for a
      wave whose every pair has its window written on the device */
   sl.runs = false;
-  if (ctx->record_runs)
+  /* record_runs 1: every wave; 2: the waves from runs_from_wave on.  The
+     last waves' records cross PCIe after the device has finished, so they
+     set the batch's end: as runs they leave at once and the host rebuilds
+     them while the earlier waves' plain records are still crossing; the
+     first waves stay plain, so that rebuilding does not take the cores
+     from the planner of the waves that follow */
+  if (ctx->record_runs == 1 || (ctx->record_runs == 2 && wave_index >= ctx->runs_from_wave))
     for (int64_t i = first; i < first + count && !sl.runs; i++) sl.runs = !(pairs[i].flags & GDP_FLAG_GWINDOW);
   if (sl.runs) {
     rc = encode_runs(ctx, sl, ctx->arena.as<char>());
@@ -1830,30 +1852,36 @@ slot_finish (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, const char *arena,
   CK(ctx, cudaEventRecord(sl.out_done, ctx->d2h));
   sl.rec_base = *base;
   *base += total;
-  if (expand) {
-    /* the records of each pair from its stream, on the copy-out side's
-       threads; the results (with batch-wide record offsets) are on the host
-       once the copies above are done */
-    GDP_TRACE_BEGIN(t1);
-    CK(ctx, cudaEventSynchronize(sl.out_done));
-    const gdp_pair_t *wp = pairs + sl.first;
-    const gdp_result_t *wr = results + sl.first;
-    const uint8_t *enc = sl.h_enc.as<uint8_t>();
-    const int64_t *off = sl.h_encoff.as<int64_t>();
-    const int64_t n = sl.count;
-    const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, n / 4096));
-    std::atomic<int> bad{0};
-    parallel_chunks(ctx->xpool, n, nt, [&](int64_t lo, int64_t hi, int) {
-      for (int64_t i = lo; i < hi; i++) {
-        const int nr = wr[i].nrecs;
-        if (nr <= 0) continue;
-        if (!rec_decode(run_seqs(wp[i], arena), enc + off[i], off[i + 1] - off[i], recs + wr[i].rec_offset, nr))
-          bad.store(1);
-      }
-    });
-    GDP_TRACE_END(t1, "expand");
-    if (bad.load()) return set_err(ctx, "record runs: a stream did not rebuild its records", cudaErrorUnknown);
-  }
+  sl.expand = expand;
+  return GDP_OK;
+}
+
+/* Rebuilds a wave's records from its runs into recs, on the copy-out
+   side's host threads, once its copies out are done. */
+static int
+slot_expand (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, const char *arena, const gdp_result_t *results,
+             gdp_rec_t *recs) {
+  if (!sl.expand) return GDP_OK;
+  sl.expand = false;
+  GDP_TRACE_BEGIN(t1);
+  CK(ctx, cudaEventSynchronize(sl.out_done));
+  const gdp_pair_t *wp = pairs + sl.first;
+  const gdp_result_t *wr = results + sl.first;
+  const uint8_t *enc = sl.h_enc.as<uint8_t>();
+  const int64_t *off = sl.h_encoff.as<int64_t>();
+  const int64_t n = sl.count;
+  const int nt = (int) std::max<int64_t>(1, std::min<int64_t>(ctx->plan_threads, n / 4096));
+  std::atomic<int> bad{0};
+  parallel_chunks(ctx->xpool, n, nt, [&](int64_t lo, int64_t hi, int) {
+    for (int64_t i = lo; i < hi; i++) {
+      const int nr = wr[i].nrecs;
+      if (nr <= 0) continue;
+      if (!rec_decode(run_seqs(wp[i], arena), enc + off[i], off[i + 1] - off[i], recs + wr[i].rec_offset, nr))
+        bad.store(1);
+    }
+  });
+  GDP_TRACE_END(t1, "expand");
+  if (bad.load()) return set_err(ctx, "record runs: a stream did not rebuild its records", cudaErrorUnknown);
   return GDP_OK;
 }
 
@@ -1959,17 +1987,43 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   std::mutex m;
   std::condition_variable cv;
   std::deque<int> launched;          /* slots launched, not yet handed out, oldest first */
-  bool all_launched = false;
+  std::deque<int> to_expand;         /* slots handed out whose runs wait to be rebuilt */
+  bool all_launched = false, outs_done = false, have_expander = false;
   int out_rc = GDP_OK;
+  /* A wave whose records travel as runs is rebuilt on the host after its
+     copies; an expander thread does that, so the copy-out thread queues
+     the next waves' copies meanwhile.  The slot stays busy until then. */
+  auto expand_one = [&](int k) {
+    Slot &o = ctx->slot[k];
+    {
+      std::lock_guard<std::mutex> g(m);
+      if (out_rc != GDP_OK) o.expand = false;
+    }
+    const int r = slot_expand(ctx, o, pairs, arena, results, recs);
+    std::lock_guard<std::mutex> g(m);
+    if (r != GDP_OK) out_rc = r;
+    o.busy = false;
+    cv.notify_all();
+  };
   auto hand_out = [&](int k) {
     Slot &o = ctx->slot[k];
     const int r = out_rc == GDP_OK ? slot_finish(ctx, o, pairs, arena, results, recs, max_recs, &base, &overflow)
                                    : out_rc;
-    std::lock_guard<std::mutex> g(m);
-    if (r != GDP_OK) out_rc = r;
-    o.busy = false;
-    launched.pop_front();
-    cv.notify_all();
+    bool inline_expand = false;
+    {
+      std::lock_guard<std::mutex> g(m);
+      if (r != GDP_OK) out_rc = r;
+      launched.pop_front();
+      if (o.expand && r == GDP_OK) {
+        if (have_expander) to_expand.push_back(k);
+        else inline_expand = true;
+      } else {
+        o.expand = false;
+        o.busy = false;
+      }
+      cv.notify_all();
+    }
+    if (inline_expand) expand_one(k);
   };
   auto copy_out_loop = [&] {
     cudaSetDevice(ctx->device);
@@ -1984,13 +2038,35 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
       hand_out(k);
     }
   };
+  auto expand_loop = [&] {
+    cudaSetDevice(ctx->device);
+    for (;;) {
+      int k;
+      {
+        std::unique_lock<std::mutex> g(m);
+        cv.wait(g, [&] { return !to_expand.empty() || outs_done; });
+        if (to_expand.empty()) return;
+        k = to_expand.front();
+        to_expand.pop_front();
+      }
+      expand_one(k);
+    }
+  };
   /* a batch of one wave hands out on this thread (and so does any batch
      when no thread can be started) */
-  std::thread copy_out;
+  std::thread copy_out, expander;
   if (n > wave_cap) {
     try {
       copy_out = std::thread(copy_out_loop);
     } catch (...) {
+    }
+    if (copy_out.joinable() && ctx->record_runs) {
+      try {
+        expander = std::thread(expand_loop);
+        std::lock_guard<std::mutex> g(m);
+        have_expander = true;
+      } catch (...) {
+      }
     }
   }
   int cur = 0, wave_index = 0;
@@ -2028,6 +2104,12 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   cv.notify_all();
   if (copy_out.joinable()) copy_out.join();
   else copy_out_loop();
+  {
+    std::lock_guard<std::mutex> g(m);
+    outs_done = true;
+  }
+  cv.notify_all();
+  if (expander.joinable()) expander.join();
   if (rc == GDP_OK) rc = out_rc;
   GDP_TRACE_BEGIN(tdrain);
   cudaError_t e = cudaStreamSynchronize(ctx->d2h);

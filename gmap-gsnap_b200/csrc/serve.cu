@@ -328,7 +328,8 @@ gdp_server_create (int device, int mode, int nworkers, int64_t dir_budget_bytes,
     }
     s->ctx.push_back(c);
   }
-  s->short_workers = nworkers >= 2 ? std::min((nworkers + 1) / 2, nworkers - 1) : 0;
+  /* short requests are most of a read mix: three workers in four take them */
+  s->short_workers = nworkers >= 2 ? std::min(std::max(1, (3 * nworkers) / 4), nworkers - 1) : 0;
   for (int w = 0; w < nworkers; w++) s->workers.emplace_back(&gdp_server::worker, s, w);
   *out = s;
   return GDP_OK;

@@ -289,10 +289,14 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *                    traceback grids (0: no limit); the serving loop's long
  *                    batches keep to part of each SM, so that short batches
  *                    find block slots free
- *   "record_runs"    1 (default): gdp_align_batch's records leave the device
- *                    as runs -- one byte for most records, which follow from
- *                    the one before and the pair's sequences -- and are
- *                    rebuilt byte for byte on the host; 0: as 12-byte records
+ *   "record_runs"    how gdp_align_batch's records leave the device: 0
+ *                    (default) as 12-byte records; 1 as runs -- one byte
+ *                    for most records, which follow from the one before and
+ *                    the pair's sequences -- rebuilt byte for byte on host
+ *                    threads (a sixteenth of the PCIe bytes, for hosts
+ *                    whose PCIe is the bottleneck); 2 the waves from
+ *                    "runs_from_wave" (default 5) on as runs, the earlier
+ *                    ones plain
  * gdp_ctx_get_param also reads "last_d2h_bytes": the bytes the last
  * gdp_align_batch copied from the device to the host.
  * gdp_autotune times plan executions of a sample batch (device-resident
@@ -400,7 +404,8 @@ int gdp_fill16_noalloc(int device, int mode, const gdp_pair_t *d_pairs, int64_t 
  * Each class has its own arrival-
  * order queue, and a batch holds requests of one class only, so a short
  * request never waits for a long one in its batch.  With two or more
- * workers, the first `short_workers` (default: half, rounded up) take short
+ * workers, the first `short_workers` (default: three in four, at least one
+ * and at most all but one) take short
  * batches only; the others take long batches and, when no long request is
  * admissible, short ones.  Short batches compute on the highest stream
  * priority, long batches on the lowest.  A worker takes every admissible
@@ -577,6 +582,59 @@ int gdp_end_setup(gdp_ctx *ctx, int user_open, int user_extend, int user_dynprog
 int gdp_end_gap_batch(gdp_ctx *ctx, const gdp_end_gap_t *gaps, int64_t ngaps, const char *arena,
                       int64_t arena_bytes, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
                       int64_t *nrecs_used);
+
+/*
+ * Dynprog_cdna_gap (src/dynprog_cdna.c:786-1290) for a batch of gaps: the
+ * gap GMAP's stage 3 solves where the read holds more than the genome
+ * between two aligned blocks (src/stage3.c:9313).  The query stretch left
+ * of the gap (rlengthL bases from roffsetL) and the one right of it
+ * (rlengthR bases back from rev_roffsetR) are each aligned against the
+ * genome stretch between the blocks (glength bases from goffset), the left
+ * one forwards and the right one backwards, and the best bridge between the
+ * two is chosen (bridge_cdna_gap_{8,16}_ud).  Per gap, as the reference
+ * does:
+ *   - glength <= 1: no pairs, dynprogindex unchanged; glength or either
+ *     rlength above the Dynprog_T maxima: no pairs, dynprogindex advanced;
+ *   - mismatch type by defect_rate (HIGHQ / MEDQ / LOWQ), open -10 and
+ *     extend -7 (CDNA_OPEN_* / CDNA_EXTEND_*);
+ *   - Dynprog_compute_bands(extraband_paired, wide) for each side; 8-bit
+ *     fills when glength < use8p_size or (rlengthL < use8p_size and
+ *     rlengthR <= use8p_size), else 16-bit;
+ *   - the upper and lower fill of each side (the right side reversed, with
+ *     the tie rule reversed), the bridge search over their scores, the right
+ *     traceback, then a cDNA insertion (queryjump == genomejump == 9: the
+ *     skipped query bases, then the skipped genome bases with '~') or a gap
+ *     holder (incomplete), then the left traceback;
+ *   - a List of the gap holder alone is returned as no pairs.
+ * The query bytes from roffsetL through rev_roffsetR lie contiguously in
+ * the arena: rseq / rseq_uc are the arena offsets of query position
+ * roffsetL.  results[i]: status, tb_score (both tracebacks' score, the
+ * reference's finalscore output), score (the bridge's best score), the
+ * counts, precision, nrecs records at rec_offset in `recs` (the returned
+ * List, head first; its gap holder has comp '\0', querypos = -1 -
+ * queryjump and genomepos = genomejump), and end_found = 1 when the gap
+ * was left incomplete (the reference's *incompletep).  A gap whose bridge
+ * finds no candidate has no defined reference result and gets
+ * GDP_ERR_BAND.  The caller advances its dynprogindex as the reference
+ * does.  Calls on one context must not overlap.
+ */
+typedef struct gdp_cdna_gap {
+  int64_t rseq;            /* rsequenceL (&queryseq_ptr[roffsetL]) */
+  int64_t rseq_uc;         /* rsequence_ucL */
+  int32_t rlengthL, rlengthR, glength;
+  int32_t roffsetL, rev_roffsetR, goffset;
+  uint32_t chroffset, chrhigh;
+  int8_t watsonp, genestrand, jump_late_p, pad8;
+  int32_t extraband_paired;
+  int32_t max_rlength, max_glength;   /* dynprogL / dynprogR maxima (GMAP sizes both alike) */
+  int32_t dynprogindex;
+  int32_t pad32;
+  double defect_rate;
+} gdp_cdna_gap_t;
+
+int gdp_cdna_gap_batch(gdp_ctx *ctx, const gdp_cdna_gap_t *gaps, int64_t ngaps, const char *arena,
+                       int64_t arena_bytes, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                       int64_t *nrecs_used);
 
 /*
  * Stage-3 batching adapter.  GMAP's stage 3 calls Dynprog_single_gap once

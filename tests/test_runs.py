@@ -103,16 +103,18 @@ def test_align_batch_records_same_with_and_without_runs(gdplib):
     try:
         ctx.set_genome(blocks, altb, g.size)
         out = {}
-        for runs in (1, 0):
+        for runs in (1, 2, 0):
             ctx.set_param("record_runs", runs)
             ra, reca = ctx.align(pairs, arena)
             rb, recb = ctx.align(short, sarena)
             out[runs] = (ra, reca, rb, recb, ctx.get_param("last_d2h_bytes"))
     finally:
         ctx.close()
-    on, off = out[1], out[0]
-    assert np.array_equal(on[0], off[0]) and on[1].tobytes() == off[1].tobytes()
-    assert np.array_equal(on[2], off[2]) and on[3].tobytes() == off[3].tobytes()
-    assert on[3].size > 1_000_000
+    off = out[0]
+    for mode in (1, 2):
+        on = out[mode]
+        assert np.array_equal(on[0], off[0]) and on[1].tobytes() == off[1].tobytes(), mode
+        assert np.array_equal(on[2], off[2]) and on[3].tobytes() == off[3].tobytes(), mode
+    assert off[3].size > 1_000_000
     # the short batch (the last call) copied far fewer bytes with runs
-    assert on[4] < 0.35 * off[4]
+    assert out[1][4] < 0.35 * off[4]

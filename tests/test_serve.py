@@ -207,12 +207,13 @@ def test_size_classes_batch_apart(gdplib, genome):
     longest = np.maximum(pool["rlength"], pool["glength"])
     assert np.array_equal(cls, (longest > 512).astype(np.int8))
     assert 50 < int((cls == 1).sum()) < 550
+    srv.drive(pool, arena, 3000, rate=1e6, seed=4)     # warm-up: the workers' buffers reach working size
     lat, elapsed, res = srv.drive(pool, arena, 3000, rate=5000.0, seed=5, want_results=True)
     assert srv.set_classes(512, 1) == 3        # not after requests were submitted
     st = srv.stats()
     srv.close()
-    assert st["class_pairs"][0] + st["class_pairs"][1] == st["pairs"] == 3000
-    assert st["class_pairs"][1] == int((cls[np.arange(3000) % pool.size] == 1).sum())
+    assert st["class_pairs"][0] + st["class_pairs"][1] == st["pairs"] == 6000
+    assert st["class_pairs"][1] == 2 * int((cls[np.arange(3000) % pool.size] == 1).sum())
     assert min(st["class_batches"]) > 0 and sum(st["class_batches"]) == st["batches"]
     ctx = gdp.Context(gdplib)
     ctx.set_genome(blocks, None, GENOME_LEN)
