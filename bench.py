@@ -600,6 +600,109 @@ def end_gap_batch(lib, ctx, seed, ngaps=200000, cpu_gaps=50000):
                                "same_results": bool(same)}
     return out
 
+
+def stage3_cdna_gaps(genome, seed, ngaps, max_rlength, max_glength):
+    """cDNA gaps as stage 3 sends them to Dynprog_cdna_gap (src/stage3.c:
+    9313): a genome gap of 20..150 nt (log-uniform) between two aligned
+    blocks, a query gap 10..60 nt longer (an insertion of unrelated bases at
+    a random place, 1 % substitutions elsewhere), both query stretches
+    glength + 10 long (extramaterial_paired), extraband_paired 6, plus
+    strand, HIGHQ, both tie rules."""
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    gaps = np.zeros(ngaps, dtype=gdp.CDNA_GAP_DTYPE)
+    gl = np.exp(rng.uniform(np.log(20), np.log(151), ngaps)).astype(np.int64)
+    ins = rng.integers(10, 61, ngaps)
+    goff = rng.integers(1000, genome.size - 1000, ngaps)
+    chunks, off = [], 0
+    for i in range(ngaps):
+        g, k = int(gl[i]), int(ins[i])
+        rl = g + 10
+        seg = genome[goff[i]:goff[i] + g].copy()
+        s = int(rng.integers(0, g + 1))
+        mid = np.concatenate([seg[:s], rng.choice(acgt, size=k), seg[s:]])
+        sub = rng.random(mid.size) < 0.01
+        mid[sub] = rng.choice(acgt, size=int(sub.sum()))
+        q = np.concatenate([rng.choice(acgt, size=rl + 4), mid, rng.choice(acgt, size=rl + 4)])
+        q[q == ord("N")] = ord("A")
+        gaps["rseq"][i] = gaps["rseq_uc"][i] = off + rl + 4
+        gaps["rlengthL"][i] = gaps["rlengthR"][i] = rl
+        gaps["glength"][i] = g
+        gaps["roffsetL"][i] = 100
+        gaps["rev_roffsetR"][i] = 100 + mid.size - 1
+        gaps["goffset"][i] = goff[i]
+        chunks.append(q)
+        off += q.size
+    gaps["chroffset"], gaps["chrhigh"] = 0, genome.size
+    gaps["watsonp"] = 1
+    gaps["jump_late_p"] = rng.random(ngaps) < 0.5
+    gaps["extraband_paired"] = 6
+    gaps["max_rlength"], gaps["max_glength"] = max_rlength, max_glength
+    gaps["dynprogindex"] = 1
+    return gaps, np.concatenate(chunks)
+
+
+def cdna_gap_batch(lib, ctx, seed, ngaps=20000, cpu_gaps=5000):
+    """Dynprog_cdna_gap over a batch of stage-3 cDNA gaps, end to end through
+    gdp_cdna_gap_batch (host gaps and sequences in, host records out),
+    against the reference's own Dynprog_cdna_gap on the host (all host
+    threads over a bounded prefix of the same gaps; its results are checked
+    against the device's on that prefix, untimed)."""
+    import torch
+    genome, blocks = gdp.make_genome(lib, 780, 1 << 24)
+    ctx.set_genome(blocks, None, genome.size)
+    gaps, arena = stage3_cdna_gaps(genome, seed, ngaps, 500, 2000)
+    res, recs = ctx.cdna_gaps(gaps, arena)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+
+    def pinned(arr):
+        t = torch.empty(max(arr.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        a = t.numpy()[:arr.nbytes].view(arr.dtype).reshape(arr.shape)
+        a[...] = arr
+        return t, a
+
+    keep = [pinned(gaps), pinned(arena), pinned(np.zeros(ngaps, dtype=gdp.RESULT_DTYPE)),
+            pinned(np.zeros(max(recs.size, 1), dtype=gdp.REC_DTYPE))]
+    h_gaps, h_arena, h_res, h_recs = (k[1] for k in keep)
+    used = ctypes.c_int64(0)
+    times = []
+    for _ in range(4):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rc = lib.gdp_cdna_gap_batch(ctx.h, gdp._ptr(h_gaps), ngaps, gdp._ptr(h_arena), h_arena.size,
+                                    gdp._ptr(h_res), gdp._ptr(h_recs), h_recs.size, ctypes.byref(used))
+        b.record(stream)
+        b.synchronize()
+        assert rc == 0 and used.value == recs.size, ctx.error()
+        times.append(a.elapsed_time(b))
+    ms = statistics.median(times[1:])
+    assert np.array_equal(h_res, res) and np.array_equal(h_recs[:recs.size], recs)
+    out = {"gaps": ngaps, "incomplete": int(res["end_found"].sum()), "filled_8bit": int((res["precision"] == 8).sum()),
+           "records": int(recs.size), "ms": round(ms, 3), "gaps_per_s": round(ngaps / (ms * 1e-3), 1),
+           "bad_status": int((res["status"] != 0).sum()),
+           "h2d_bytes": int(gaps.nbytes + arena.nbytes), "d2h_bytes": int(res.nbytes + recs.nbytes),
+           "timing": "host gaps and sequences to host records (gdp_cdna_gap_batch, pinned host "
+                     "buffers), median of 3 after one warm-up, CUDA events on the context stream"}
+    import oracle
+    if cpu_gaps > 0 and oracle.reference_available():
+        ref = oracle.reference()
+        ref.init(0)
+        ref.set_genome(blocks, None, genome.size)
+        rc_ = oracle.ReferenceCdnaGap(ref, 200, 40)
+        sample = gaps[:cpu_gaps]
+        threads = os.cpu_count() or 1
+        secs, _ = rc_.bench(sample, arena, threads, 200, 40)
+        st, off, rrecs = rc_.run(sample, arena)
+        same = (np.array_equal(st[:, 0], res["tb_score"][:cpu_gaps]) and
+                np.array_equal(st[:, 5], res["nrecs"][:cpu_gaps]) and
+                np.array_equal(rrecs, recs[:int(res["nrecs"][:cpu_gaps].sum())]))
+        out["cpu_baseline"] = {"value": round(cpu_gaps / secs, 1), "unit": "gaps/s", "cores": threads,
+                               "kind": "reference",
+                               "sample": f"the first {cpu_gaps} gaps, Dynprog_cdna_gap of oracle/_ref, "
+                                         f"{secs:.2f} s on {threads} threads",
+                               "same_results": bool(same)}
+    return out
+
 def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000,
                   workers=4):
     """The serving loop under Poisson load: single-pair requests of the
@@ -1039,6 +1142,7 @@ def run_gdp(args):
         extra["endpoint_search"] = endpoint_search(lib, ctx, args.seed + 9)
         extra["single_gap"] = single_gap_batch(lib, ctx, args.seed + 10)
         extra["end_gap"] = end_gap_batch(lib, ctx, args.seed + 11)
+        extra["cdna_gap"] = cdna_gap_batch(lib, ctx, args.seed + 12)
     if rank == 0 and world == 1 and not args.no_serving:
         extra["serving"] = serving_sweep(lib, local, args.seed + 8,
                                          [1e3, 1e4, 5e4, 1e5, 2e5, 3e5, 5e5, 1e6])

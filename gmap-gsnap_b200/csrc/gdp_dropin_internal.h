@@ -41,16 +41,27 @@ struct gdpi_single_cfg {
   bool user_p = false;   /* user_dynprog_p */
   int end_open = 0, end_extend = 0;
   bool end_user_p = false;   /* Dynprog_end_setup's user_dynprog_p */
-  static constexpr int NBUF = 16;
+  static constexpr int NBUF = 24;
   void *dbuf[NBUF] = {};
   size_t dcap[NBUF] = {};
   void *hbuf[NBUF] = {};
   size_t hcap[NBUF] = {};
   gdp_plan *plan = nullptr;
+  gdp_plan *dump_plan = nullptr;   /* plans whose fills also dump their scores (cdna_gap.cu) */
 };
 /* Plans pairs[0..n) into *plan (created on first use; its host and device
    buffers only grow) and uploads the plan on the context stream. */
 int gdpi_plan_reuse(gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t n);
+/* As gdpi_plan_reuse, and the plan's fills also write the score of every
+   swept cell, in the direction words' block-column layout (the score of
+   lane l of the word-column at word offset w is at w * 8 + l); after
+   gdp_plan_execute, gdpi_plan_scores and gdpi_plan_meta (each pair's word
+   offsets, dir16 / dir8) point at them on the device until the plan's next
+   use.  The plan must not be used for pairs that need no scores: its fills
+   keep dumping. */
+int gdpi_plan_reuse_dump(gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t n);
+const int16_t *gdpi_plan_scores(const gdp_plan *plan);
+const gdp_meta_t *gdpi_plan_meta(const gdp_plan *plan);
 void gdpi_single_release(gdpi_single_cfg *c);
 struct gdpi_view {
   int device;

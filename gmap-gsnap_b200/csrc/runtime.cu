@@ -2376,6 +2376,27 @@ gdpi_plan_reuse (gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t
   return rc;
 }
 
+int
+gdpi_plan_reuse_dump (gdp_ctx *ctx, gdp_plan **plan, const gdp_pair_t *pairs, int64_t n) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (*plan == nullptr) *plan = new gdp_plan();
+  gdp_plan *pl = *plan;
+  int rc = plan_build(ctx, pairs, n, -1, pl->h);
+  if (rc == GDP_OK) rc = plan_upload(ctx, pl->h, pl->d, true, ctx->stream);
+  return rc;
+}
+
+const int16_t *
+gdpi_plan_scores (const gdp_plan *plan) {
+  return plan->d.hdump.as<int16_t>();
+}
+
+const gdp_meta_t *
+gdpi_plan_meta (const gdp_plan *plan) {
+  return plan->d.meta.as<gdp_meta_t>();
+}
+
 void
 gdpi_single_release (gdpi_single_cfg *c) {
   for (int k = 0; k < gdpi_single_cfg::NBUF; k++) {
@@ -2385,7 +2406,8 @@ gdpi_single_release (gdpi_single_cfg *c) {
     c->dcap[k] = c->hcap[k] = 0;
   }
   if (c->plan) gdp_plan_destroy(c->plan);
-  c->plan = nullptr;
+  if (c->dump_plan) gdp_plan_destroy(c->dump_plan);
+  c->plan = c->dump_plan = nullptr;
 }
 
 int

@@ -80,6 +80,18 @@ END_GAP_DTYPE = np.dtype([
 assert END_GAP_DTYPE.itemsize == 72
 QUERYEND_GAP, QUERYEND_INDELS, QUERYEND_NOGAPS, BEST_LOCAL = 0, 1, 2, 3
 
+# struct gdp_cdna_gap, 80 bytes: the arguments of Dynprog_cdna_gap
+CDNA_GAP_DTYPE = np.dtype([
+    ("rseq", "<i8"), ("rseq_uc", "<i8"),
+    ("rlengthL", "<i4"), ("rlengthR", "<i4"), ("glength", "<i4"),
+    ("roffsetL", "<i4"), ("rev_roffsetR", "<i4"), ("goffset", "<i4"),
+    ("chroffset", "<u4"), ("chrhigh", "<u4"),
+    ("watsonp", "i1"), ("genestrand", "i1"), ("jump_late_p", "i1"), ("pad8", "i1"),
+    ("extraband_paired", "<i4"), ("max_rlength", "<i4"), ("max_glength", "<i4"), ("dynprogindex", "<i4"),
+    ("pad32", "<i4"), ("defect_rate", "<f8"),
+])
+assert CDNA_GAP_DTYPE.itemsize == 80
+
 WL_FIXED, WL_SHORT, WL_CDNA, WL_MIX, WL_LONG = 1, 2, 3, 4, 5
 
 
@@ -155,6 +167,7 @@ def load(path=LIB_PATH):
     lib.gdp_runs_encode.argtypes = [vp, vp, vp, i32, vp]
     lib.gdp_runs_encode.restype = i64
     lib.gdp_runs_decode.argtypes = [vp, vp, vp, i64, vp, i32]
+    lib.gdp_cdna_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
     lib.gdp_end_setup.argtypes = [vp, i32, i32, i32]
     lib.gdp_end_gap_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
     lib.gdp_gap_queue_create.argtypes = [i32, i32, i64, i64, vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
@@ -469,6 +482,22 @@ class Context:
                                         _ptr(recs), max_recs, ctypes.byref(used))
         if rc != 0:
             raise RuntimeError(f"gdp_end_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
+        return results, recs[:used.value]
+
+    def cdna_gaps(self, gaps, arena, max_recs=None):
+        """Dynprog_cdna_gap over a batch: (results, records); results'
+        end_found is the reference's incompletep."""
+        n = gaps.size
+        results = np.zeros(n, dtype=RESULT_DTYPE)
+        if max_recs is None:
+            max_recs = int((np.maximum(gaps["rlengthL"], 0).astype(np.int64) + np.maximum(gaps["rlengthR"], 0)
+                            + 2 * np.maximum(gaps["glength"], 0) + 24).sum())
+        recs = np.zeros(max(max_recs, 1), dtype=REC_DTYPE)
+        used = ctypes.c_int64(0)
+        rc = self.lib.gdp_cdna_gap_batch(self.h, _ptr(gaps), n, _ptr(arena), arena.size, _ptr(results),
+                                         _ptr(recs), max_recs, ctypes.byref(used))
+        if rc != 0:
+            raise RuntimeError(f"gdp_cdna_gap_batch: {STATUS.get(rc, rc)} {self.error()}")
         return results, recs[:used.value]
 
     def fill_dump(self, pairs, arena, scores=True):

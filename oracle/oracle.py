@@ -336,6 +336,48 @@ class ReferenceEndGap:
         return stats, off, recs[:used]
 
 
+class ReferenceCdnaGap:
+    """The reference's own Dynprog_cdna_gap (oracle/ref_cdna.c) over a batch
+    of gaps, in a reference library (shares its genome and tables)."""
+
+    def __init__(self, ref, maxlookback, extraquerygap):
+        lib = ref.lib
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        lib.ref_cdna_init.argtypes = [i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        lib.ref_cdna_gap_batch.argtypes = [vp, i32, vp, vp, vp, i64, vp]
+        lib.ref_cdna_gap_batch.restype = i64
+        mr, mg = ctypes.c_int(0), ctypes.c_int(0)
+        lib.ref_cdna_init(maxlookback, extraquerygap, ctypes.byref(mr), ctypes.byref(mg))
+        self.lib = lib
+        self.max_rlength, self.max_glength = mr.value, mg.value
+
+    def bench(self, gaps, arena, nthreads, maxlookback, extraquerygap):
+        """Wall seconds and a checksum of Dynprog_cdna_gap over every gap once
+        on nthreads threads, each with its own Dynprog_T pair and Pairpool_T."""
+        lib = self.lib
+        lib.ref_cdna_gap_bench.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+        lib.ref_cdna_gap_bench.restype = ctypes.c_double
+        cs = ctypes.c_int64(0)
+        secs = lib.ref_cdna_gap_bench(_ptr(gaps), gaps.size, _ptr(arena), nthreads, maxlookback, extraquerygap,
+                                      ctypes.byref(cs))
+        return secs, cs.value
+
+    def run(self, gaps, arena):
+        """Per gap: stats (traceback_score, incompletep, 0, 0, 0, npairs, list
+        is NULL, dynprogindex after), record offsets, and the records (the
+        returned List, head first)."""
+        n = gaps.size
+        stats = np.zeros((n, 8), np.int32)
+        off = np.zeros(n, np.int64)
+        cap = int((np.maximum(gaps["rlengthL"], 0).astype(np.int64) + np.maximum(gaps["rlengthR"], 0)
+                   + 2 * np.maximum(gaps["glength"], 0) + 24).sum()) + 1
+        recs = np.zeros(cap, dtype=_rec_dtype())
+        used = self.lib.ref_cdna_gap_batch(_ptr(gaps), n, _ptr(arena), _ptr(stats), _ptr(recs), cap, _ptr(off))
+        assert used <= cap
+        return stats, off, recs[:used]
+
+
 def _segment_end(g, galt, chroffset, chrhigh, goffset, glength, watsonp, end):
     """The genome segment of an end gap, stored forward: end 3 is
     Dynprog_end3_gap's gsequence (Genome_get_segment_right from chroffset +

@@ -11,6 +11,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <time.h>
 
 #include "dynprog.h"
 #include "dynprog_cdna.h"
@@ -89,4 +91,78 @@ ref_cdna_gap_batch (const gdp_cdna_gap_t *gaps, int n, const char *arena, int32_
     used += k;
   }
   return used;
+}
+
+/* ------------------------------------------------------------------ */
+/* CPU baseline: Dynprog_cdna_gap over a batch, one pthread per core    */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  const gdp_cdna_gap_t *gaps;
+  const char *arena;
+  int n, tid, nthreads, maxlookback, extraquerygap;
+  int64_t checksum;
+} cdnajob_t;
+
+static void *
+cdna_worker (void *arg) {
+  cdnajob_t *j = (cdnajob_t *) arg;
+  /* each thread owns its Dynprog_T pair and Pairpool_T, as each GMAP
+     worker thread does */
+  Dynprog_T dl = Dynprog_new(j->maxlookback, j->extraquerygap, 0, 0, 0, /*doublep*/true);
+  Dynprog_T dr = Dynprog_new(j->maxlookback, j->extraquerygap, 0, 0, 0, /*doublep*/true);
+  Pairpool_T pool = Pairpool_new();
+  int64_t sum = 0;
+  int i;
+  for (i = j->tid; i < j->n; i += j->nthreads) {
+    const gdp_cdna_gap_t *g = &j->gaps[i];
+    int dpi = g->dynprogindex, score = 0;
+    bool incomplete = false;
+    List_T pairs;
+    char *rs = (char *) j->arena + g->rseq, *ru = (char *) j->arena + g->rseq_uc;
+    const int to_r = g->rev_roffsetR - g->roffsetL;
+    Pairpool_reset(pool);
+    pairs = Dynprog_cdna_gap(&dpi, &score, &incomplete, dl, dr, rs, ru, rs + to_r, ru + to_r, g->rlengthL,
+                             g->rlengthR, g->glength, g->roffsetL, g->rev_roffsetR, g->goffset,
+                             (Univcoord_T) g->chroffset, (Univcoord_T) g->chrhigh, g->watsonp != 0, g->genestrand,
+                             g->jump_late_p != 0, ref_genome_main(), ref_genome_alt(), pool, g->extraband_paired,
+                             g->defect_rate);
+    sum += score + List_length(pairs);
+  }
+  Pairpool_free(&pool);
+  Dynprog_free(&dr);
+  Dynprog_free(&dl);
+  j->checksum = sum;
+  return NULL;
+}
+
+/* Dynprog_cdna_gap for every gap once, on nthreads threads (static
+   round-robin); returns wall seconds and a checksum of the traceback
+   scores and list lengths. */
+double
+ref_cdna_gap_bench (const gdp_cdna_gap_t *gaps, int n, const char *arena, int nthreads, int maxlookback,
+                    int extraquerygap, int64_t *checksum) {
+  pthread_t *th;
+  cdnajob_t *jobs;
+  struct timespec t0, t1;
+  int64_t sum = 0;
+  int t;
+  if (nthreads < 1) nthreads = 1;
+  th = (pthread_t *) calloc(nthreads, sizeof(pthread_t));
+  jobs = (cdnajob_t *) calloc(nthreads, sizeof(cdnajob_t));
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (t = 0; t < nthreads; t++) {
+    jobs[t].gaps = gaps; jobs[t].arena = arena; jobs[t].n = n; jobs[t].tid = t; jobs[t].nthreads = nthreads;
+    jobs[t].maxlookback = maxlookback; jobs[t].extraquerygap = extraquerygap;
+    pthread_create(&th[t], NULL, cdna_worker, &jobs[t]);
+  }
+  for (t = 0; t < nthreads; t++) {
+    pthread_join(th[t], NULL);
+    sum += jobs[t].checksum;
+  }
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  free(th);
+  free(jobs);
+  if (checksum) *checksum = sum;
+  return (double) (t1.tv_sec - t0.tv_sec) + 1e-9 * (double) (t1.tv_nsec - t0.tv_nsec);
 }
