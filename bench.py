@@ -1184,6 +1184,11 @@ def run_gdp(args):
                          "achieved": round(achieved_ops / 1e12, 3), "peak": round(int_peak / 1e12, 3),
                          "unit": "Tops/s (int32 lane-ops)", "frac": round(achieved_ops / int_peak, 4),
                          "peak_source": "measured int32 issue probe (gdp_measure_int_peak)",
+                         # the packed fill computes two 16-bit lanes per 32-bit
+                         # instruction, so its lane-op ceiling is twice the
+                         # int32 rate; the fraction against that ceiling
+                         "frac_of_packed_16x2_peak": (round(achieved_ops / (2 * int_peak), 4)
+                                                      if top_name.startswith("fill_packed") else None),
                          "ops_per_cell": OPS_PER_CELL, "ms_per_step": round(avg_launch_ms, 3),
                          "kernel_times": "a profiled pass of the same K steps right after the timed region "
                                          "(CUDA events around every launch, on the launching stream)",
