@@ -703,11 +703,15 @@ def cdna_gap_batch(lib, ctx, seed, ngaps=20000, cpu_gaps=5000):
                                "same_results": bool(same)}
     return out
 
-def serving_sweep(lib, device, seed, rates, seconds_per_rate=1.0, max_requests=400_000, pool_size=20_000,
+def serving_sweep(lib, device, seed, rates, seconds_per_rate=2.0, max_requests=400_000, pool_size=20_000,
                   workers=4):
     """The serving loop under Poisson load: single-pair requests of the
     mixed distribution, genome windows extracted on the device from a
-    resident 100 Mbp genome, admission by a 40 GB direction budget."""
+    resident 100 Mbp genome, admission by a 40 GB direction budget.  Each
+    rate runs for `seconds_per_rate` of arrivals (at most max_requests
+    requests); the sustained rate is the requests over the time from the
+    first arrival to the last completion, so the last requests' latency
+    (about 0.1 s for long reads) weighs less in a longer window."""
     genome, blocks = gdp.make_genome(lib, 4242, 100_000_000)
     pool, arena = gdp.make_resident_pairs(lib, gdp.WL_MIX, seed, genome, pool_size)
     cells = gdp.band_cells(pool)
@@ -1153,13 +1157,13 @@ def run_gdp(args):
     # DRAM bytes of the dominant kernel per launch: one ncu capture of the same
     # kernel on 300,000 pairs of this workload (its first launch, the 150,000
     # jump-early pairs: dram__bytes_read.sum + dram__bytes_write.sum =
-    # 357.99 + 832.93 MB over 902,385,535 in-band cells), scaled to this
+    # 359.54 + 829.68 MB over 902,385,535 in-band cells), scaled to this
     # step's launches by their in-band cells; the kernel's bytes grow with the
     # cells (directions and carries per swept cell)
     traffic, traffic_src = None, None
     if name == "short" and top_name.startswith("fill_packed<W16,full"):
-        traffic = int(round((357.993728e6 + 832.926208e6) / 902385535 * top_cells))
-        traffic_src = ("ncu capture of this kernel on 300,000 pairs (1,190.9 MB for 902,385,535 in-band cells), "
+        traffic = int(round((359.537920e6 + 829.679616e6) / 902385535 * top_cells))
+        traffic_src = ("ncu capture of this kernel on 300,000 pairs (1,189.2 MB for 902,385,535 in-band cells), "
                        "scaled by in-band cells to one step's launches")
     if rank == 0:
         line = {

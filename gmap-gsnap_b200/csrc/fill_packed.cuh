@@ -42,7 +42,9 @@
  * Bodies.  A steady column (every lane inside the band) needs no lane
  * masks; the general body handles the band edges with per-word masks built
  * from the lane index; the half body skips lanes 0-7 once the top band lane
- * is 8 or more (they never feed an in-band cell again).  Every body is one
+ * is 8 or more (they never feed an in-band cell again); the bottom-half
+ * body skips lanes 8-15 while the bottom band lane is 7 or less, where that
+ * is exact (below).  Every body is one
  * run of straight-line code over the eight words (edges are masks, not
  * branches), so the compiler interleaves the words' independent steps:
  * per-word skip branches, tried and measured, split the column into basic
@@ -164,39 +166,67 @@ pblock_start (PBlock &B, const PairView &v, const gdp_tables_t *tab, int xlo) {
 }
 
 /* Column class scores of words K0..7: max(score(ka), score(kb)) per lane. */
-template <int K0>
+template <int K0, int K1>
 __device__ __forceinline__ void
 pcol_scores (const PBlock &B, int ka, int kb, uint32_t ps[8]) {
   using namespace gdp_pk;
   if (ka < 4) {
     const uint32_t s = sel_class(ka);
 #pragma unroll
-    for (int k = K0; k < 8; k++) ps[k] = prmt(B.plo[2 * k], B.plo[2 * k + 1], s);
+    for (int k = K0; k < K1; k++) ps[k] = prmt(B.plo[2 * k], B.plo[2 * k + 1], s);
   } else {
 #pragma unroll
-    for (int k = K0; k < 8; k++) ps[k] = prmt(B.phi4[k >> 1], B.phi4[k >> 1], sel_n(k));
+    for (int k = K0; k < K1; k++) ps[k] = prmt(B.phi4[k >> 1], B.phi4[k >> 1], sel_n(k));
   }
   if (kb != ka) {
     if (kb < 4) {
       const uint32_t s = sel_class(kb);
 #pragma unroll
-      for (int k = K0; k < 8; k++) ps[k] = max2(ps[k], prmt(B.plo[2 * k], B.plo[2 * k + 1], s));
+      for (int k = K0; k < K1; k++) ps[k] = max2(ps[k], prmt(B.plo[2 * k], B.plo[2 * k + 1], s));
     } else {
 #pragma unroll
-      for (int k = K0; k < 8; k++) ps[k] = max2(ps[k], prmt(B.phi4[k >> 1], B.phi4[k >> 1], sel_n(k)));
+      for (int k = K0; k < K1; k++) ps[k] = max2(ps[k], prmt(B.phi4[k >> 1], B.phi4[k >> 1], sel_n(k)));
     }
   }
 }
 
 /*
- * One swept column y of a full-band block, lanes 2 K0 .. 15.  GEN = false:
- * a steady column (no band edge inside the block: the top band lane is
- * above lane 0 and the bottom one below lane 15, y >= 1, a full block).
- * GEN = true: any column, with the band edges of block_column: the bottom
- * cell (H from the diagonal only, DIAG directions, :6926-6945), the top
- * cell (F chain restart, :6962-6974), F only on the lanes between them,
- * column 0 (pairscores_col0, :6668-6678).  K0 = 4 (the half body): lanes
- * 0-7 lie above the band for good and are skipped (GEN, top lane >= 8).
+ * One swept column y of a full-band block, lanes 2 K0 .. 2 K1 - 1.
+ * GEN = false: a steady column (no band edge inside the block: the top
+ * band lane is above lane 0 and the bottom one below lane 15, y >= 1, a
+ * full block).  GEN = true: any column, with the band edges of
+ * block_column: the bottom cell (H from the diagonal only, DIAG
+ * directions, :6926-6945), the top cell (F chain restart, :6962-6974), F
+ * only on the lanes between them, column 0 (pairscores_col0, :6668-6678).
+ * K0 = 4 (the half body): lanes 0-7 lie above the band for good and are
+ * skipped (GEN, top lane >= 8).  K1 = 4 (the bottom-half body): lanes
+ * 8-15 lie below the band and are skipped (GEN, bottom lane <= 7, not the
+ * last column); they keep the block's start values until a general column
+ * takes them up again.  Bodies specialised further by band edge (top edge
+ * only, bottom edge only) left out the masks of the other edge but made
+ * the kernel 17 % slower: six bodies overflow the instruction cache.
+ *
+ * Why skipping lanes below the band is exact where pair_fill_packed uses
+ * it.  The reference computes them, and their values enter the band only
+ * as the E of a lane that has just become the bottom cell: the bottom cell
+ * ignores its E (H from the diagonal and F, Egap DIAG), and the next column
+ * takes max(E, H_bottom + open).  A below-band value is a score of the
+ * block's start values (H = NEG_INFINITY - open) plus at most 15 table
+ * entries, so it is at most NEG - open + 15 mx, in the reference and here
+ * alike.  Every in-band H off column 0 is at least the score of the path
+ * from the corner along the main diagonal and then straight along a row
+ * or a column (E and F only add to H), that is at least
+ * mn min(r, c) + open + extend |r - c| with mn the most negative table
+ * entry; a bottom cell has |r - c| = lband.  Where that bound plus open
+ * lies above NEG - open + 15 mx (the pair's test in pair_fill_packed) and
+ * the block's sweep starts right of column 0 (whose cells are
+ * NEG_INFINITY), max(E, H_bottom + open) is H_bottom + open whichever
+ * below-band values E came from, and so are its tie-rule direction bits:
+ * every in-band score and direction is the reference's.  Only the
+ * direction bits and the carries of the skipped below-band cells differ,
+ * and nothing reads them (a traceback stops at the bottom cell's DIAG
+ * Egap; the next block reads carries from its own sweep's first column
+ * on, where lane 15 is in the band).
  *
  *   diag    H[y-1][xlo-1] + OFF (or the row-0 value);
  *   Hc, Fc  H[y][xlo-1] and the F carry of the block above, + OFF.
@@ -204,12 +234,13 @@ pcol_scores (const PBlock &B, int ka, int kb, uint32_t ps[8]) {
  * Returns the carry for the block below: the last lane's H and its F, packed.
  * With `track`, the in-band scores of the column go into vmax.
  */
-template <bool LATE, bool GEN, int K0>
+template <bool LATE, bool GEN, int K0, int K1 = 8>
 __device__ __forceinline__ uint32_t
 pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int kb, uint32_t *dcol,
-      int16_t *hd, uint32_t &vmax, bool track) {
+      int16_t *hd, uint32_t &vmax, bool track, const uint32_t *s_pre) {
   using namespace gdp_pk;
   static_assert(K0 == 0 || GEN, "the half body handles band edges");
+  static_assert(K1 == 8 || (GEN && K0 == 0), "the bottom-half body handles band edges");
   const uint32_t open2 = bc(v.open), ext2 = bc(v.ext), oe2 = bc(v.oe), neg2 = bc(NEG);
   const int xlo = B.xlo, last = B.last;
   const int rel = y - xlo;
@@ -223,7 +254,7 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
   const bool cut_lo = GEN && t >= 1;
 
   uint32_t ps[8];
-  pcol_scores<K0>(B, ka, kb, ps);
+  pcol_scores<K0, K1>(B, ka, kb, ps);
 
   /* E and H steps (:6862-6913); accE / accN collect the Egap / HORIZ bits
      (jump late: their negations) */
@@ -231,7 +262,7 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
   uint32_t prev = (K0 == 0) ? ((uint32_t) diag << 16) : B.H[K0 - 1];
   const uint32_t negbt2 = bc(-bt);
 #pragma unroll
-  for (int k = K0; k < 8; k++) {
+  for (int k = K0; k < K1; k++) {
     const uint32_t Hold = B.H[k], Eold = B.E[k];
     const uint32_t T1 = addmax(Hold, open2, neg2);
     const uint32_t m = max2(Eold, T1);
@@ -270,7 +301,7 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
   const uint32_t negt2 = bc(-t), fhi2 = bc(fhi);
   uint32_t Flast = 0;
 #pragma unroll
-  for (int k = K0; k < 8; k++) {
+  for (int k = K0; k < K1; k++) {
     const uint32_t Hpre = B.H[k];
     uint32_t Hoe = add2(Hpre, oe2);
     if (cut_lo) Hoe = lowwhere(Hoe, negmask(add2(lanes2(k), negt2)));    /* lanes above the top cell */
@@ -292,13 +323,15 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
   }
 
   /* the direction words (W = 16 layout of gdp_internal.h) */
-  const uint32_t comp = lanes_acc(2 * K0, 15);                 /* lanes computed */
-  const uint32_t frange = lanes_acc(max(s, 2 * K0), fhi);      /* lanes with an F step */
+  const uint32_t comp = lanes_acc(2 * K0, 2 * K1 - 1);         /* lanes computed */
+  /* lanes with an F step: s_pre[i] = lanes_acc(0, i - 1), so lanes lo..hi
+     are s_pre[hi + 1] & ~s_pre[lo] (0 <= lo <= 16, -1 <= hi <= 15) */
+  const uint32_t frange = s_pre[fhi + 1] & ~s_pre[max(s, 2 * K0)];
   uint32_t nb = LATE ? (accN ^ comp) : accN;
   uint32_t vb = LATE ? (accV ^ (comp << 8)) : accV;
   uint32_t eb = LATE ? (accE ^ comp) : accE;
   uint32_t fj = accFj;
-  if (LATE) fj ^= (0xffu & ~((1u << K0) - 1u)) * 0x10001u;
+  if (LATE) fj ^= (((1u << K1) - 1u) & ~((1u << K0) - 1u)) * 0x10001u;
   const uint32_t odd = fj & 0xffu;                              /* lanes 2k+1 */
   const uint32_t even = ((fj >> 16) << 1) & 0xfeu;              /* lanes 2k+2 */
   uint32_t fb = (even | (odd << 16)) & ~1u;
@@ -306,12 +339,12 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
   fb |= (s == 0) ? pF0 : 0u;
   nb = (nb & comp) | (vb & (frange << 8));
   eb = (eb & comp) | ((fb & frange) << 8);
-  if (hasbot) eb &= ~lanes_acc(bt, bt);
+  if (hasbot) eb &= ~(s_pre[bt + 1] & ~s_pre[bt]);
   *reinterpret_cast<uint2 *>(dcol) = make_uint2(prmt(nb, eb, 0x5410u), prmt(nb, eb, 0x7632u));
 
   if (track) {
 #pragma unroll
-    for (int k = K0; k < 8; k++) {
+    for (int k = K0; k < K1; k++) {
       uint32_t h = B.H[k];
       if (cut_lo) h = lowwhere(h, negmask(add2(lanes2(k), negt2)));
       if (cut_hi) h = lowwhere(h, negmask(add2(fhi2, neglanes2(k))));
@@ -338,7 +371,7 @@ pcol (PBlock &B, const PairView &v, int y, int diag, int Hc, int Fc, int ka, int
 template <bool LATE, int MODE>
 __device__ __forceinline__ void
 pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v, const int8_t *s_nt2int,
-                  int64_t slot) {
+                  const uint32_t *s_pre, int64_t slot) {
   using namespace gdp_pk;
   static_assert(MODE == 0 || MODE == 1, "plain fills and the 16-bit pass of rerun pairs");
   uint32_t *dir = P.dirs + mp->dir16;
@@ -346,10 +379,17 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
   const int64_t scs = P.nslots;
   int final_score = -32768;
   uint32_t vmax = LOW2;
+  /* the pair's bound for skipping lanes below the band (pcol): every
+     bottom cell, at least mn min(r, c) + open + extend lband, plus open
+     lies above NEG_INFINITY - open + 15 mx; no dump asked for */
+  const bool skip_ok = P.hdump == nullptr &&
+                       P.tab_mn * min(v.g.X, v.g.Y) + 3 * v.open + v.ext * v.lband - 15 * P.tab_mx > -32768 + 64;
   for (int xlo = 0; xlo <= v.g.X; xlo += 16) {
     PBlock B;
     pblock_start<LATE>(B, v, P.tab, xlo);
     if (B.y1 < B.y0) continue;
+    /* ... and the block's sweep starts right of column 0 */
+    const bool skip_bot = skip_ok && B.y0 >= 1;
     int bot_prev = NEG;   /* H[y-1][xlo-1] from the block above */
     if (xlo > 0 && B.y0 > 0) bot_prev = lo16(sc[(int64_t) (B.y0 - 1) * scs]);
     int ka, kb;
@@ -376,11 +416,13 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
       const int t = y - xlo - v.uband;
       uint32_t out;
       if (y >= ys0 && y <= ys1)
-        out = pcol<LATE, false, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+        out = pcol<LATE, false, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track, s_pre);
       else if (y >= 1 && t >= 8 && y != v.g.Y)
-        out = pcol<LATE, true, 4>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+        out = pcol<LATE, true, 4>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track, s_pre);
+      else if (skip_bot && y - xlo + v.lband <= 7 && y != v.g.Y)
+        out = pcol<LATE, true, 0, 4>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, nullptr, vmax, track, s_pre);
       else
-        out = pcol<LATE, true, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track);
+        out = pcol<LATE, true, 0>(B, v, y, diag, lo16(above), hi16(above), ka, kb, dcol, hd, vmax, track, s_pre);
       sc[(int64_t) y * scs] = out;
       if (y == v.g.Y) {
         const int L = v.g.X - xlo;
@@ -420,7 +462,9 @@ template <bool LATE, int MODE>
 __global__ void __launch_bounds__(128, GDP_PACKED_MINB)
 fill_packed_kernel (FillParams P) {
   __shared__ int8_t s_nt2int[128];
+  __shared__ uint32_t s_pre[17];   /* lanes_acc(0, i - 1): the lane-range masks of pcol */
   for (int i = threadIdx.x; i < 128; i += blockDim.x) s_nt2int[i] = P.tab->nt2int[i];
+  if (threadIdx.x < 17) s_pre[threadIdx.x] = gdp_pk::lanes_acc(0, (int) threadIdx.x - 1);
   __syncthreads();
   const int64_t slot = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
   const int n = *P.count;
@@ -433,7 +477,7 @@ fill_packed_kernel (FillParams P) {
     pair_view<16, GDP_FULL>(p, P.arena, v);
     v.reach_from = (int) ((P.reach_from4 >> (8 * (v.mt & 3))) & 255u);
     v.endmode = 0;
-    pair_fill_packed<LATE, MODE>(P, pi, P.meta + pi, v, s_nt2int, slot);
+    pair_fill_packed<LATE, MODE>(P, pi, P.meta + pi, v, s_nt2int, s_pre, slot);
   }
 }
 

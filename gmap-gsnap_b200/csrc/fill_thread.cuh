@@ -84,6 +84,10 @@ struct FillParams {
      per-register fill_thread_kernel skips them and takes the others (every
      pair when this is below 0). */
   int packed_len;
+  /* the smallest (at most 0) and the largest (at least 0) entry of the
+     substitution tables over every mismatch type (fill_packed_kernel's
+     bound for skipping lanes below the band) */
+  int tab_mn, tab_mx;
 };
 
 /* Lanes lo..hi (0 <= lo <= hi <= 31) as a bit mask. */

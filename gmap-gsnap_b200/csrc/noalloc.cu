@@ -36,6 +36,7 @@
  * cleared by it.
  */
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <mutex>
 
 #include "gdp_internal.h"
@@ -68,6 +69,7 @@ static gdp_tables_t *g_tables_dev[GDP_NOALLOC_MAX_DEVICES];
 static int g_tables_mode[GDP_NOALLOC_MAX_DEVICES];
 static bool g_ready[GDP_NOALLOC_MAX_DEVICES];
 static int g_packed_len[GDP_NOALLOC_MAX_DEVICES];
+static int g_tab_mn[GDP_NOALLOC_MAX_DEVICES], g_tab_mx[GDP_NOALLOC_MAX_DEVICES];
 static gdp_tables_t g_host_tables;   /* host staging for the one-time upload */
 
 /*
@@ -164,6 +166,13 @@ noalloc_setup (int device, int mode, unsigned char **scratch, gdp_tables_t **tab
        caller's non-blocking stream would not wait for it */
     if (cudaDeviceSynchronize() != cudaSuccess) return GDP_ERR_CUDA;
     g_packed_len[device] = gdp_packed_len_of(&g_host_tables);
+    g_tab_mn[device] = g_tab_mx[device] = 0;
+    for (int mt = 0; mt < 4; mt++)
+      for (int a = 0; a < 128; a++)
+        for (int b = 0; b < 128; b++) {
+          g_tab_mn[device] = std::min(g_tab_mn[device], (int) g_host_tables.pd[mt][a][b]);
+          g_tab_mx[device] = std::max(g_tab_mx[device], (int) g_host_tables.pd[mt][a][b]);
+        }
     g_scratch_dev[device] = (unsigned char *) ps;
     g_tables_dev[device] = (gdp_tables_t *) pt;
     g_tables_mode[device] = mode;
@@ -213,6 +222,8 @@ noalloc_run (int device, int mode, const gdp_pair_t *d_pairs, int64_t npairs, co
   P.reach_from4 = 0;
   P.lower_slack4 = 0;
   P.packed_len = g_packed_len[device];
+  P.tab_mn = g_tab_mn[device];
+  P.tab_mx = g_tab_mx[device];
   for (int late = 1; late >= 0; late--) {
     P.list = late ? list_late : list_early;
     P.count = counts + (late ? 0 : 1);

@@ -223,10 +223,12 @@ struct PlanDev {
   DevBuf total;        /* int64 record total of the plan */
   DevBuf cub_tmp;
   DevBuf sel_tmp;      /* temporary storage of the 8-bit pass selection */
+  DevBuf sel_tmp_late; /* the same for the jump-late chain */
   void release () {
     lists.release(); work.release(); counts.release(); work_counts.release(); status.release();
     meta0.release(); meta.release(); rec_off.release(); dirs.release(); hdump.release();
     slots.release(); nrec_scan.release(); total.release(); cub_tmp.release(); sel_tmp.release();
+    sel_tmp_late.release();
   }
 };
 
@@ -273,7 +275,7 @@ struct Slot {
      streams) and the slot's own scratch, so consecutive waves overlap on
      the device (one wave's tail beside the next wave's start) */
   cudaStream_t cs = nullptr;
-  DevBuf scratch, scratch8;
+  DevBuf scratch, scratch8, scratch_late;
   HostBuf total;           /* pinned int64: records of the wave */
   /* the record-run transport (rec_runs.h): the wave's encoded records, each
      pair's stream offset, and their pinned host copies */
@@ -296,19 +298,22 @@ struct gdp_ctx {
   int nsm = 148;
   cudaStream_t stream = nullptr;        /* compute */
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  /* the one-warp/one-CTA-per-pair fill kinds run beside the thread kinds */
-  cudaStream_t side[2] = {nullptr, nullptr};
+  /* the one-warp/one-CTA-per-pair fill kinds run beside the thread kinds on
+     side[0] and side[1]; side[2] takes the jump-late thread kinds and their
+     8-bit passes, a chain of its own beside the jump-early one */
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
   /* the side streams of the wave streams, each at its wave stream's
      priority: a wave's lane-group, CTA and early 8-bit kinds run beside its
      thread kinds with the same priority, and waves on different streams do
      not queue behind one another's side kernels */
-  cudaStream_t wave_side[GDP_MAX_WAVE_STREAMS][2] = {};
-  cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+  cudaStream_t wave_side[GDP_MAX_WAVE_STREAMS][3] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
   int reach_from[4] = {0, 0, 0, 0};   /* FillParams::reach_from of h_tab */
   int lower_slack[4] = {0, 0, 0, 0};  /* FillParams::lower_slack4 of h_tab */
   int packed_len = -1;                 /* FillParams::packed_len of h_tab */
+  int tab_mn = 0, tab_mx = 0;          /* FillParams::tab_mn / tab_mx of h_tab */
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
@@ -322,7 +327,7 @@ struct gdp_ctx {
   bool check_groups = false; /* the 8-bit pass of rerun pairs on lane groups (false: one thread per pair) ... */
   int check_min_x = 1 << 30; /* ... or only for pairs with at least this many rows (lower: columns) */
   gdpi_single_cfg single;   /* Dynprog_single_setup's user penalties */
-  DevBuf arena, scratch, scratch8;
+  DevBuf arena, scratch, scratch8, scratch_late;
   Slot slot[NSLOTS];
   WorkPool pool;            /* the planner's host threads */
   WorkPool xpool;           /* the copy-out side's host threads (record-run expansion) */
@@ -431,6 +436,13 @@ update_reach (gdp_ctx *ctx) {
     ctx->lower_slack[mt] = std::min(slack, 255);
   }
   ctx->packed_len = gdp_packed_len_of(ctx->h_tab);
+  ctx->tab_mn = ctx->tab_mx = 0;
+  for (int mt = 0; mt < 4; mt++)
+    for (int a = 0; a < 128; a++)
+      for (int b = 0; b < 128; b++) {
+        ctx->tab_mn = std::min(ctx->tab_mn, (int) ctx->h_tab->pd[mt][a][b]);
+        ctx->tab_mx = std::max(ctx->tab_mx, (int) ctx->h_tab->pd[mt][a][b]);
+      }
   const char *pe = getenv("GDP_PACKED");   /* 0: every pair on the one-lane-per-register fill */
   if (pe && atoi(pe) == 0) ctx->packed_len = -1;
 }
@@ -465,6 +477,7 @@ slot_release (Slot &sl) {
   sl.cs = nullptr;
   sl.scratch.release();
   sl.scratch8.release();
+  sl.scratch_late.release();
 }
 
 extern "C" void
@@ -481,7 +494,7 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
       cudaStreamSynchronize(ctx->wave_stream[k]);
       cudaStreamDestroy(ctx->wave_stream[k]);
     }
-  ctx->arena.release(); ctx->scratch.release(); ctx->scratch8.release();
+  ctx->arena.release(); ctx->scratch.release(); ctx->scratch8.release(); ctx->scratch_late.release();
   gdpi_single_release(&ctx->single);
   if (ctx->d_tab) cudaFree(ctx->d_tab);
   if (ctx->d_genome) cudaFree(ctx->d_genome);
@@ -489,12 +502,12 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 3; k++) {
     if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
   for (int w = 0; w < GDP_MAX_WAVE_STREAMS; w++)
-    for (int k = 0; k < 2; k++)
+    for (int k = 0; k < 3; k++)
       if (ctx->wave_side[w][k]) cudaStreamDestroy(ctx->wave_side[w][k]);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   free(ctx->h_tab);
@@ -515,9 +528,11 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
       cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&ctx->side[1], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side[2], cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->join_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->join_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&ctx->join_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->join_ev[2], cudaEventDisableTiming) != cudaSuccess) {
     gdp_ctx_destroy(ctx);
     return GDP_ERR_CUDA;
   }
@@ -530,7 +545,8 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   for (int k = 0; k < ctx->nwave; k++) {
     if (cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->wave_side[k][0], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->wave_side[k][1], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
+        cudaStreamCreateWithPriority(&ctx->wave_side[k][1], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->wave_side[k][2], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
       gdp_ctx_destroy(ctx);
       return GDP_ERR_CUDA;
     }
@@ -1299,13 +1315,14 @@ launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_
 static int
 plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
           gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t stream = nullptr, DevBuf *scratch_buf = nullptr,
-          DevBuf *scratch8_buf = nullptr) {
+          DevBuf *scratch8_buf = nullptr, DevBuf *scratch_late_buf = nullptr) {
   cudaStream_t s = stream ? stream : ctx->stream;
   cudaStream_t *side_s = ctx->side;
   for (int w = 0; w < ctx->nwave; w++)
     if (s == ctx->wave_stream[w]) side_s = ctx->wave_side[w];
   DevBuf &scratch = scratch_buf ? *scratch_buf : ctx->scratch;
   DevBuf &scratch8 = scratch8_buf ? *scratch8_buf : ctx->scratch8;   /* the early 8-bit kinds' own */
+  DevBuf &scratch_late = scratch_late_buf ? *scratch_late_buf : ctx->scratch_late;   /* the jump-late chain's */
   const int64_t n = ph.n;
   if (n == 0) return GDP_OK;
   cudaEvent_t ev0 = nullptr;
@@ -1327,10 +1344,11 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
-  size_t need = 0, need8 = 0;
+  size_t need = 0, need8 = 0, need_late = 0;
   for (int k = 0; k < NTHREADKINDS; k++) {
     if (!ph.counts[k]) continue;
-    need = std::max(need, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
+    size_t &nd = ((k >> 1) & 1) ? need_late : need;
+    nd = std::max(nd, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
   for (int k = FIRST_EARLY8; k < NKINDS; k++) {
     if (!ph.counts[k]) continue;
@@ -1338,11 +1356,21 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   }
   CK(ctx, scratch.ensure(std::max<size_t>(need, 64)));
   if (need8 > 0) CK(ctx, scratch8.ensure(need8));
+  if (need_late > 0) CK(ctx, scratch_late.ensure(need_late));
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs.
      The one-warp / one-CTA-per-pair kinds (no scratch) go first, on the
      two side streams, so that they run beside the one-thread-per-pair
-     kinds, which share the scratch and stay in order on the main stream. */
-  bool forked = false;
+     kinds.  Those form two chains: the jump-early kinds share the scratch
+     and stay in order on the main stream, the jump-late kinds have a
+     scratch of their own and stay in order on the third side stream.  A
+     pair's 8-bit pass waits only for its own 16-bit pass, so each chain's
+     8-bit pass (few pairs, a few blocks per SM) runs beside the other
+     chain's 16-bit pass instead of after it.  With per-launch timing on,
+     both chains stay on the main stream, so that each kernel's events
+     time it alone; so they do under a grid footprint cap (grid_limit),
+     which bounds the blocks per SM of one launch at a time. */
+  const bool two_chains = !ctx->profiling && ctx->grid_limit == 0;
+  bool forked = false, forked_late = false;
   int side = 0;
   CK(ctx, cudaEventRecord(ctx->fork_ev, s));
   for (int round = 0; round < 2; round++) {
@@ -1362,6 +1390,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       const int w32 = thread ? (k >> 2) / 3 : 0, pass = thread ? (k & 1) : 0;
       const bool second = (w32 == 1 && pass == 1) || warp8;
       if ((round == 0) == second || !ph.counts[k]) continue;
+      /* the jump-late chain: thread kinds and lane-group 8-bit passes of
+         jump-late pairs */
+      const bool late_chain = (thread && ((k >> 1) & 1)) || (warp8 && (((k - FIRST_WARP8) / 3) & 1));
+      if (late_chain && !forked_late && two_chains) {
+        CK(ctx, cudaStreamWaitEvent(side_s[2], ctx->fork_ev, 0));
+        forked_late = true;
+      }
+      cudaStream_t ks = (late_chain && two_chains) ? side_s[2] : s;
       const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], grid_cap(ctx, 8)))
                      : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
                      : warp8 ? warp_grid(ctx, ph.counts[k], WARP8_K[(k - FIRST_WARP8) % 3])
@@ -1375,15 +1411,16 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
            pass; the selection keeps the planner's order, so a warp's pairs
            share band width and lband as in the other passes */
         const NeedsPass8 need{pd.meta.as<gdp_meta_t>()};
+        DevBuf &sel_tmp = late_chain ? pd.sel_tmp_late : pd.sel_tmp;
         size_t tmp = 0;
         CK(ctx, cub::DeviceSelect::If(nullptr, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
-                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, s));
-        CK(ctx, pd.sel_tmp.ensure(std::max<size_t>(tmp, 16)));
+                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, ks));
+        CK(ctx, sel_tmp.ensure(std::max<size_t>(tmp, 16)));
         cudaEvent_t evc = nullptr;
-        prof_begin(ctx, &evc, s);
-        CK(ctx, cub::DeviceSelect::If(pd.sel_tmp.p, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
-                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, s));
-        prof_end(ctx, PROF_RERUN, evc, s);
+        prof_begin(ctx, &evc, ks);
+        CK(ctx, cub::DeviceSelect::If(sel_tmp.p, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
+                                      pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, ks));
+        prof_end(ctx, PROF_RERUN, evc, ks);
         ctx->launches++;
         P.list = pd.work.as<int32_t>() + ph.start[k];
         P.count = pd.work_counts.as<int32_t>() + k;
@@ -1392,18 +1429,19 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.hdump = pd.hdump.as<int16_t>();
       P.meta = pd.meta.as<gdp_meta_t>();
       P.res = d_res;
-      P.scratch = early8 ? scratch8.as<int2>() : scratch.as<int2>();
+      P.scratch = early8 ? scratch8.as<int2>() : (late_chain ? scratch_late.as<int2>() : scratch.as<int2>());
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
       P.reach_from4 = 0;
       P.lower_slack4 = 0;
       P.packed_len = ctx->packed_len;
+      P.tab_mn = ctx->tab_mn;
+      P.tab_mx = ctx->tab_mx;
       for (int q = 0; q < 4; q++) {
         P.reach_from4 |= (uint32_t) std::min(ctx->reach_from[q], 255) << (8 * q);
         P.lower_slack4 |= (uint32_t) ctx->lower_slack[q] << (8 * q);
       }
-      cudaStream_t ks = s;
       if (warp || cta || early8) {
         if (!forked) {
           for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(side_s[q], ctx->fork_ev, 0));
@@ -1430,6 +1468,10 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       ctx->launches += nlaunch;
       CK(ctx, cudaGetLastError());
     }
+  }
+  if (forked_late) {
+    CK(ctx, cudaEventRecord(ctx->join_ev[2], side_s[2]));
+    CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[2], 0));
   }
   /* the 8-bit outcome of rerun pairs, after both of their passes */
   for (int k = 0; k < NKINDS; k++) {
@@ -1764,7 +1806,7 @@ slot_launch (gdp_ctx *ctx, Slot &sl, const gdp_pair_t *pairs, int64_t first, int
   if (arena_ready) CK(ctx, cudaStreamWaitEvent(sl.cs, arena_ready, 0));
   GDP_TEV(sl.cs, "comp_begin %lld", first);
   rc = plan_run(ctx, sl.h, sl.d, sl.pairs.as<gdp_pair_t>(), ctx->arena.as<char>(), sl.results.as<gdp_result_t>(),
-                sl.d.slots.as<gdp_rec_t>(), sl.cs, &sl.scratch, &sl.scratch8);
+                sl.d.slots.as<gdp_rec_t>(), sl.cs, &sl.scratch, &sl.scratch8, &sl.scratch_late);
   if (rc != GDP_OK) return rc;
   /* the count reaches the host through a mapped pinned word written by the
      compaction kernel, not a copy on the compute stream (a copy engine busy

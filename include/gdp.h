@@ -346,6 +346,9 @@ void *gdp_ctx_stream(gdp_ctx *ctx);
  * result initialisation, integer-rate probe, rerun-list compaction, record
  * compaction and window extraction; unused ids have an empty name), its
  * name, total device milliseconds and launch count since the last reset.
+ * While enabled, a plan's kernels run one after another on the context's
+ * stream (without it, the jump-late fills run beside the jump-early ones
+ * on a side stream), so that each launch's events time it alone.
  */
 int gdp_profile_enable(gdp_ctx *ctx, int on);
 int gdp_profile_read(gdp_ctx *ctx, int id, char *name, int name_cap, double *ms, int64_t *launches);
