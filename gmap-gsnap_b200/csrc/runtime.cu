@@ -2179,6 +2179,79 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
   return rc;
 }
 
+/*
+ * One batch over several contexts (one per GPU, or several on one GPU).
+ * Pairs are independent, so the batch splits into contiguous shards of
+ * about equal band cells, one per context, each run by gdp_align_batch
+ * from its own host thread; no data crosses between devices.  A shard
+ * gets only its own part of the arena: its pairs' offsets are rebased to
+ * the shard's first sequence byte (rounded down to 256, which keeps every
+ * sequence's alignment).  Shard k's records start at the record slots
+ * (rlength + glength + 2 per traceback pair) of the pairs before it, and
+ * its results' rec_offset count from recs.
+ */
+extern "C" int
+gdp_align_batch_multi (gdp_ctx *const *ctxs, int nctx, const gdp_pair_t *pairs, int64_t n, const char *arena,
+                       int64_t arena_bytes, gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                       int64_t *nrecs_used) {
+  if (nrecs_used) *nrecs_used = 0;
+  if (ctxs == nullptr || nctx < 1 || n < 0 || (n > 0 && (pairs == nullptr || results == nullptr))) return GDP_ERR_PARAM;
+  for (int k = 0; k < nctx; k++)
+    if (ctxs[k] == nullptr) return GDP_ERR_PARAM;
+  if (n == 0) return GDP_OK;
+  std::vector<int64_t> work(n + 1, 0), slots(n + 1, 0);
+  for (int64_t i = 0; i < n; i++) {
+    const gdp_pair_t &p = pairs[i];
+    const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
+    const int64_t band = std::max(p.lband, 0) + std::max(p.uband, 0) + 1;
+    work[i + 1] = work[i] + 1 + (p.variant == GDP_LOWER ? gl : rl) * std::min<int64_t>(band, rl + gl + 1);
+    slots[i + 1] = slots[i] + ((p.flags & GDP_FLAG_TRACEBACK) ? rl + gl + 2 : 0);
+  }
+  if (slots[n] > 0 && (recs == nullptr || max_recs < slots[n])) return GDP_ERR_RECS;
+  std::vector<int64_t> first(nctx + 1, n);
+  first[0] = 0;
+  for (int k = 1; k < nctx; k++) {
+    const int64_t target = work[n] / nctx * k;
+    first[k] = std::max(first[k - 1], (int64_t) (std::lower_bound(work.begin(), work.end(), target) - work.begin()));
+    first[k] = std::min(first[k], n);
+  }
+  std::vector<int> rc(nctx, GDP_OK);
+  std::vector<int64_t> used(nctx, 0);
+  auto run = [&](int k) {
+    const int64_t lo = first[k], hi = first[k + 1], m = hi - lo;
+    if (m <= 0) return;
+    int64_t alo = (int64_t) 1 << 62, ahi = 0;
+    for (int64_t i = lo; i < hi; i++) {
+      const gdp_pair_t &p = pairs[i];
+      const int64_t rl = std::max(p.rlength, 0), gl = std::max(p.glength, 0);
+      alo = std::min(alo, std::min(std::min(p.rseq, p.rseq_uc), std::min(p.gseq, p.gseq_alt)));
+      ahi = std::max(ahi, std::max(std::max(p.rseq + rl, p.rseq_uc + rl), std::max(p.gseq + gl, p.gseq_alt + gl)));
+    }
+    alo = std::min(std::max<int64_t>(alo, 0), arena_bytes) & ~(int64_t) 255;
+    ahi = std::min(std::max(ahi, alo), arena_bytes);
+    /* offsets out of the arena stay out of the shard's arena, so they fail
+       validation as they would in one batch */
+    std::vector<gdp_pair_t> sp(pairs + lo, pairs + hi);
+    for (gdp_pair_t &p : sp) {
+      p.rseq -= alo; p.rseq_uc -= alo; p.gseq -= alo; p.gseq_alt -= alo;
+    }
+    rc[k] = gdp_align_batch(ctxs[k], sp.data(), m, arena + alo, ahi - alo, results + lo,
+                            slots[n] > 0 ? recs + slots[lo] : nullptr, slots[hi] - slots[lo], &used[k]);
+    for (int64_t i = lo; i < hi; i++) results[i].rec_offset += slots[lo];
+  };
+  std::vector<std::thread> th;
+  for (int k = 1; k < nctx; k++) th.emplace_back(run, k);
+  run(0);
+  for (auto &t : th) t.join();
+  int64_t end = 0;
+  for (int k = 0; k < nctx; k++) {
+    if (rc[k] != GDP_OK) return rc[k];
+    if (first[k + 1] > first[k] && used[k] > 0) end = slots[first[k]] + used[k];
+  }
+  if (nrecs_used) *nrecs_used = end;
+  return GDP_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* Parity/debug: dense dump of the compare domain                      */
 /* ------------------------------------------------------------------ */

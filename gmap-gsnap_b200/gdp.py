@@ -110,6 +110,8 @@ def load(path=LIB_PATH):
     lib.gdp_ctx_destroy.argtypes = [vp]
     lib.gdp_set_genome.argtypes = [vp, vp, vp, ctypes.c_uint64]
     lib.gdp_align_batch.argtypes = [vp, vp, i64, vp, i64, vp, vp, i64, ctypes.POINTER(i64)]
+    lib.gdp_align_batch_multi.argtypes = [ctypes.POINTER(vp), i32, vp, i64, vp, i64, vp, vp, i64,
+                                          ctypes.POINTER(i64)]
     lib.gdp_plan_create.argtypes = [vp, vp, i64, ctypes.POINTER(vp)]
     lib.gdp_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
     lib.gdp_plan_total_recs.argtypes = [vp]
@@ -520,6 +522,24 @@ class Context:
         if rc != 0:
             raise RuntimeError(f"gdp_fill_dump: {STATUS.get(rc, rc)} {self.error()}")
         return offs, H, dN, dE, dF, results
+
+
+def align_multi(lib, contexts, pairs, arena, max_recs=None):
+    """One batch over several contexts (gdp_align_batch_multi): (results,
+    recs), pair i's records at results[i]["rec_offset"] in recs."""
+    n = pairs.size
+    results = np.zeros(n, dtype=RESULT_DTYPE)
+    if max_recs is None:
+        max_recs = int((pairs["rlength"].astype(np.int64) + pairs["glength"] + 2).sum())
+    recs = np.zeros(max(max_recs, 1), dtype=REC_DTYPE)
+    hs = (ctypes.c_void_p * len(contexts))(*[c.h.value if isinstance(c.h, ctypes.c_void_p) else c.h
+                                             for c in contexts])
+    used = ctypes.c_int64(0)
+    rc = lib.gdp_align_batch_multi(hs, len(contexts), _ptr(pairs), n, _ptr(arena), arena.size, _ptr(results),
+                                   _ptr(recs), max_recs, ctypes.byref(used))
+    if rc != 0:
+        raise RuntimeError(f"gdp_align_batch_multi: {STATUS.get(rc, rc)}")
+    return results, recs[:used.value]
 
 
 class Server:

@@ -240,6 +240,28 @@ int gdp_align_batch(gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t npairs,
                     int64_t *nrecs_used);
 
 /*
+ * gdp_align_batch over several contexts, typically one per GPU (contexts
+ * on one GPU also work).  The pairs split into contiguous shards of about
+ * equal band cells, one per context, each aligned by gdp_align_batch from
+ * its own host thread: pairs are independent, so no data crosses between
+ * devices, and each shard copies only its own part of the arena.  Every
+ * context needs the genome set.  Results come back in pair order.  Shard
+ * k's records start at the record slots of the pairs before it (a
+ * traceback pair has rlength + glength + 2 slots), so records are in pair
+ * order with gaps between shards: read pair i's records at
+ * results[i].rec_offset (counted from recs), results[i].nrecs of them.
+ * `max_recs` must hold the slots of every traceback pair (else
+ * GDP_ERR_RECS before any work); *nrecs_used is the end of the last
+ * shard's records.  Returns the first failing shard's status.  The
+ * reference has no counterpart (it aligns one pair per call, on the
+ * calling thread).
+ */
+int gdp_align_batch_multi(gdp_ctx *const *ctxs, int nctx, const gdp_pair_t *pairs, int64_t npairs,
+                          const char *arena, int64_t arena_bytes,
+                          gdp_result_t *results, gdp_rec_t *recs, int64_t max_recs,
+                          int64_t *nrecs_used);
+
+/*
  * Plans for device-resident batches.  gdp_plan_create inspects the pairs
  * (host copy) once: it validates them, bins them by fill kind and work,
  * and lays out the device direction storage and the traceback record
