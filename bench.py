@@ -33,6 +33,7 @@ import statistics
 import subprocess
 import sys
 import threading
+import time
 
 import numpy as np
 
@@ -749,6 +750,74 @@ def serving_sweep(lib, device, seed, rates, seconds_per_rate=2.0, max_requests=4
             "peak_admitted_dir_gb": round(st["peak_reserved_bytes"] / 2**30, 3)}
 
 
+def per_pair_concurrent(lib, pairs, arena, blocks, genome_len, sample, res0, params, nthreads=8):
+    """The per-pair GPU path as a multi-threaded caller uses it (GMAP's
+    worker threads each calling the reference-signature entry points): the
+    sample split over `nthreads` host threads, each with its own context
+    (own streams, the routing parameters `params`) executing one one-pair
+    plan per pair back to back, all threads at once.  Wall clock from a
+    device-wide synchronize before the first launch to one after the last."""
+    import torch
+    d_pairs = torch.from_numpy(pairs.view(np.uint8)).cuda()
+    d_arena = torch.from_numpy(arena).cuda()
+    d_res = torch.empty(pairs.size * gdp.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    slices = np.array_split(sample, nthreads)
+    ctxs, plans, offs, tot = [], [], [], 0
+    for sl in slices:
+        c = gdp.Context(lib, device=torch.cuda.current_device())
+        c.set_genome(blocks, None, genome_len)
+        for k, v in params.items():
+            lib.gdp_ctx_set_param(c.h, k.encode(), int(v))
+        pl_c, off_c = [], []
+        for i in sl:
+            pl = ctypes.c_void_p()
+            assert lib.gdp_plan_create(c.h, gdp._ptr(pairs[i:i + 1]), 1, ctypes.byref(pl)) == 0, c.error()
+            pl_c.append(pl)
+            off_c.append(tot)
+            tot += max(int(lib.gdp_plan_total_recs(pl)), 1)
+        ctxs.append(c)
+        plans.append(pl_c)
+        offs.append(off_c)
+    d_recs = torch.empty(tot * gdp.REC_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    pb, ab, rb, cb = d_pairs.data_ptr(), d_arena.data_ptr(), d_res.data_ptr(), d_recs.data_ptr()
+
+    def run(t):
+        c = ctxs[t]
+        for j, i in enumerate(slices[t]):
+            lib.gdp_plan_execute(c.h, plans[t][j], ctypes.c_void_p(pb + int(i) * gdp.PAIR_DTYPE.itemsize),
+                                 ctypes.c_void_p(ab), ctypes.c_void_p(rb + int(i) * gdp.RESULT_DTYPE.itemsize),
+                                 ctypes.c_void_p(cb + offs[t][j] * gdp.REC_DTYPE.itemsize))
+        lib.gdp_sync(c.h)
+
+    def all_threads():
+        th = [threading.Thread(target=run, args=(t,)) for t in range(nthreads)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+
+    all_threads()                      # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    all_threads()
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    one = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=gdp.RESULT_DTYPE)
+    for t in range(nthreads):
+        for pl in plans[t]:
+            lib.gdp_plan_destroy(pl)
+        ctxs[t].close()
+    same = all(np.array_equal(one[k][sample], res0[k][sample])
+               for k in ("status", "score", "precision", "tb_score", "nmatches", "nmismatches", "nopens",
+                         "nindels", "nrecs"))
+    pcells = float(gdp.band_cells(pairs[sample]).sum())
+    return {"gcups": round(pcells / (wall_ms * 1e-3) / 1e9, 3), "pairs": int(sample.size),
+            "threads": nthreads, "alignments_per_s": round(sample.size / (wall_ms * 1e-3), 1),
+            "sample": f"the same {sample.size} pairs, one plan per pair, {nthreads} host threads each with its "
+                      f"own context, concurrently; wall clock between device-wide synchronizes",
+            "results_identical_to_batch": bool(same)}
+
+
 def measure_config(lib, ctx, label, name, npairs, seed, chunk, cpu_seconds, genome=None, tune_pairs=0,
                    per_pair=0, cpu_max_pairs=None):
     """One workload at its stated size on the device, chunk by chunk (each
@@ -894,6 +963,11 @@ def measure_config(lib, ctx, label, name, npairs, seed, chunk, cpu_seconds, geno
                                      f"per pair, back to back on one stream",
                            "results_identical_to_batch": bool(same)}
         out["batched_vs_per_pair"] = round(out["device"]["gcups"] / per, 2)
+        routing = {k: ctx.get_param(k) for k in ("warp_min_x", "warp_max_sweep", "group_slack", "tb_warp",
+                                                  "check_groups", "check_min_x")}
+        conc = per_pair_concurrent(lib, pairs, arena, blocks, genome.size, sample, res0, routing)
+        out["per_pair_concurrent"] = conc
+        out["batched_vs_per_pair_concurrent"] = round(out["device"]["gcups"] / conc["gcups"], 2)
     if cpu_seconds > 0:
         out["cpu_baseline"] = cpu_leg(pairs, arena, blocks, genome.size, cpu_seconds, res=res0, recs=recs0,
                                       max_pairs=cpu_max_pairs)

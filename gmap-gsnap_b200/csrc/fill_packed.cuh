@@ -396,16 +396,27 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
     column_classes<GDP_FULL>(v, s_nt2int, B.y0, ka, kb);
     uint32_t above = pk(NEG, NEG);
     if (xlo > 0) above = sc[(int64_t) B.y0 * scs];
+    /* column y + 1's genome characters and carry, loaded one column before
+       they are classified / used (two columns ahead of their use) */
+    int ra = 'N', rb = 'N';
+    uint32_t above1 = pk(NEG, NEG);
+    if (B.y0 + 1 <= B.y1) {
+      ra = seqch(v.sseq, v.slen, B.y0 + 1, v.revp);
+      rb = seqch(v.salt, v.slen, B.y0 + 1, v.revp);
+      if (xlo > 0) above1 = sc[(int64_t) (B.y0 + 1) * scs];
+    }
     uint32_t *dcol = dir;
     /* the block's steady columns: no band edge inside the block */
     const int ys0 = max(xlo + 16 - v.lband, 1), ys1 = (B.last == 15) ? xlo + v.uband - 1 : -1;
     for (int y = B.y0; y <= B.y1; y++) {
-      /* prefetch column y + 1 */
-      int ka2 = 0, kb2 = 0;
-      uint32_t above2 = pk(NEG, NEG);
-      if (y < B.y1) {
-        column_classes<GDP_FULL>(v, s_nt2int, y + 1, ka2, kb2);
-        if (xlo > 0) above2 = sc[(int64_t) (y + 1) * scs];
+      /* column y + 1 from the characters loaded last column, and the
+         loads for column y + 2 */
+      const int ka2 = s_nt2int[ra], kb2 = s_nt2int[rb];
+      const uint32_t above2 = above1;
+      if (y + 2 <= B.y1) {
+        ra = seqch(v.sseq, v.slen, y + 2, v.revp);
+        rb = seqch(v.salt, v.slen, y + 2, v.revp);
+        if (xlo > 0) above1 = sc[(int64_t) (y + 2) * scs];
       }
       int diag;
       if (y == 0) diag = (xlo == 0) ? OFF : NEG;   /* the corner scores 0 */

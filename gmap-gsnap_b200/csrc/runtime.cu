@@ -317,8 +317,8 @@ struct gdp_ctx {
   uint32_t *d_genome = nullptr, *d_genomealt = nullptr;
   uint64_t genome_len = 0;
   int64_t budget = 0;
-  int64_t wave = 262144;
-  int64_t first_wave = 0;   /* pairs of the first wave (0: wave / 16, at least 16,384) */
+  int64_t wave = 131072;
+  int64_t first_wave = 0;   /* pairs of the first wave (0: wave / 2, at least 16,384) */
   int warp_min_x = 512;     /* pairs with at least this many lanes (rows; lower: columns) ... */
   int warp_max_sweep = 496; /* ... and at most this sweep width per block go one warp per pair */
   bool tb_warp = true;      /* tracebacks with one warp per pair (false: one thread per pair) */
@@ -1344,10 +1344,14 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
+  /* the jump-late chain runs beside the jump-early one (below) unless
+     per-launch timing is on or a grid footprint cap is set; only then does
+     it need a scratch of its own */
+  const bool two_chains = !ctx->profiling && ctx->grid_limit == 0;
   size_t need = 0, need8 = 0, need_late = 0;
   for (int k = 0; k < NTHREADKINDS; k++) {
     if (!ph.counts[k]) continue;
-    size_t &nd = ((k >> 1) & 1) ? need_late : need;
+    size_t &nd = (((k >> 1) & 1) && two_chains) ? need_late : need;
     nd = std::max(nd, (size_t) (ph.maxY[k] + 1) * (size_t) fill_grid(ctx, ph.counts[k]) * 128 * sizeof(int2));
   }
   for (int k = FIRST_EARLY8; k < NKINDS; k++) {
@@ -1369,7 +1373,6 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
      both chains stay on the main stream, so that each kernel's events
      time it alone; so they do under a grid footprint cap (grid_limit),
      which bounds the blocks per SM of one launch at a time. */
-  const bool two_chains = !ctx->profiling && ctx->grid_limit == 0;
   bool forked = false, forked_late = false;
   int side = 0;
   CK(ctx, cudaEventRecord(ctx->fork_ev, s));
@@ -1411,7 +1414,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
            pass; the selection keeps the planner's order, so a warp's pairs
            share band width and lband as in the other passes */
         const NeedsPass8 need{pd.meta.as<gdp_meta_t>()};
-        DevBuf &sel_tmp = late_chain ? pd.sel_tmp_late : pd.sel_tmp;
+        DevBuf &sel_tmp = (late_chain && two_chains) ? pd.sel_tmp_late : pd.sel_tmp;
         size_t tmp = 0;
         CK(ctx, cub::DeviceSelect::If(nullptr, tmp, P.list, pd.work.as<int32_t>() + ph.start[k],
                                       pd.work_counts.as<int32_t>() + k, (int) ph.counts[k], need, ks));
@@ -1429,7 +1432,8 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       P.hdump = pd.hdump.as<int16_t>();
       P.meta = pd.meta.as<gdp_meta_t>();
       P.res = d_res;
-      P.scratch = early8 ? scratch8.as<int2>() : (late_chain ? scratch_late.as<int2>() : scratch.as<int2>());
+      P.scratch = early8 ? scratch8.as<int2>()
+                         : ((late_chain && two_chains) ? scratch_late.as<int2>() : scratch.as<int2>());
       P.nslots = (int64_t) grid * 128;
       P.scratch_rows = ph.maxY[k] + 1;
       P.tab = ctx->d_tab;
@@ -1963,10 +1967,10 @@ gdp_align_batch (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, const char *a
     }
     return GDP_OK;
   };
-  /* Short first waves get the pipeline going: the first holds 1/8 of a
+  /* A short first wave gets the pipeline going: the first holds half a
      wave and each next one twice the one before, up to a full wave, so the
      copies out start early and never wait long for the next wave. */
-  int64_t wave_cap = std::min(wave, ctx->first_wave > 0 ? ctx->first_wave : std::max<int64_t>(16384, wave / 16));
+  int64_t wave_cap = std::min(wave, ctx->first_wave > 0 ? ctx->first_wave : std::max<int64_t>(16384, wave / 2));
   /* A wave also ends before its direction words would pass the context's
      budget (an upper bound per pair: every block sweeps at most
      W + lband + uband columns).  One pass finds the count and the end of the

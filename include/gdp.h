@@ -301,7 +301,7 @@ int gdp_plan_use_graph(gdp_plan *plan, int on);
  *   "check_min_x"    ... pairs with at least this many lanes, whose 8-bit
  *                    pass goes to lane groups all the same
  *   "wave_pairs"     pairs per wave of gdp_align_batch
- *   "first_wave_pairs" pairs of its first wave (0: wave_pairs / 16, at least
+ *   "first_wave_pairs" pairs of its first wave (0: wave_pairs / 2, at least
  *                    16,384); each next wave holds twice the one before,
  *                    up to wave_pairs
  *   "wave_priority"  stream priority of a batch's first wave, 0 the highest
