@@ -390,6 +390,9 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
     if (B.y1 < B.y0) continue;
     /* ... and the block's sweep starts right of column 0 */
     const bool skip_bot = skip_ok && B.y0 >= 1;
+    /* a 16-bit pass that has already seen an in-band score at the limit
+       has decided the rerun: no further tracking */
+    const bool need_track = MODE == 1 && max(lo16(vmax), hi16(vmax)) < v.lim + OFF;
     int bot_prev = NEG;   /* H[y-1][xlo-1] from the block above */
     if (xlo > 0 && B.y0 > 0) bot_prev = lo16(sc[(int64_t) (B.y0 - 1) * scs]);
     int ka, kb;
@@ -423,7 +426,7 @@ pair_fill_packed (const FillParams &P, int pi, gdp_meta_t *mp, const PairView &v
       else diag = (xlo == 0) ? NEG : bot_prev;
       bot_prev = lo16(above);
       int16_t *hd = (P.hdump != nullptr) ? P.hdump + (dcol - P.dirs) * 8 : nullptr;
-      const bool track = MODE == 1 && y >= 1 && y >= v.reach_from && xlo + B.last >= v.reach_from;
+      const bool track = need_track && y >= 1 && y >= v.reach_from && xlo + B.last >= v.reach_from;
       const int t = y - xlo - v.uband;
       uint32_t out;
       if (y >= ys0 && y <= ys1)

@@ -61,8 +61,9 @@ struct DevBuf {
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
-    /* grow geometrically: a buffer that keeps growing is reallocated rarely */
-    size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
+    /* a quarter of headroom (device buffers can be a large part of HBM, so
+       no doubling) */
+    size_t grow = want + want / 4 + 4096;
     cudaError_t e = cudaMalloc(&p, grow);
     if (e == cudaSuccess) bytes = grow;
     return e;
@@ -76,11 +77,12 @@ struct HostBuf {   /* pinned host memory */
   size_t bytes = 0;
   cudaError_t ensure (size_t want) {
     if (want <= bytes) return cudaSuccess;
+    /* grow geometrically, so that a buffer that keeps growing is
+       reallocated rarely: freeing pinned memory waits for the device */
+    const size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    /* grow geometrically: a buffer that keeps growing is reallocated rarely */
-    size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     cudaError_t e = cudaHostAlloc(&p, grow, cudaHostAllocMapped);
     if (e == cudaSuccess) bytes = grow;
     return e;

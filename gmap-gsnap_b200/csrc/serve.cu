@@ -53,10 +53,12 @@ struct Pinned {
   size_t bytes = 0;
   bool ensure (size_t want) {
     if (want <= bytes) return true;
+    /* geometric growth: freeing pinned memory waits for the device, which
+       a worker should do rarely while other workers' batches run */
+    const size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    const size_t grow = std::max(want + want / 4, 2 * bytes) + 4096;
     if (cudaHostAlloc(&p, grow, cudaHostAllocDefault) != cudaSuccess) return false;
     bytes = grow;
     return true;
