@@ -291,6 +291,9 @@ struct Slot {
 };
 
 #define GDP_MAX_WAVE_STREAMS 6
+/* side streams of a compute stream for the lane-group / CTA / early 8-bit
+   kinds (one more takes the jump-late chain) */
+#define GDP_NSIDE 6
 struct gdp_ctx {
   int device = 0;
   cudaStream_t wave_stream[GDP_MAX_WAVE_STREAMS] = {};   /* gdp_align_batch's compute, highest priority first */
@@ -300,16 +303,17 @@ struct gdp_ctx {
   int nsm = 148;
   cudaStream_t stream = nullptr;        /* compute */
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  /* the one-warp/one-CTA-per-pair fill kinds run beside the thread kinds on
-     side[0] and side[1]; side[2] takes the jump-late thread kinds and their
-     8-bit passes, a chain of its own beside the jump-early one */
-  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  /* side[0] takes the early 8-bit kinds, side[1 .. GDP_NSIDE-1] the
+     one-warp/one-CTA-per-pair fill kinds (each kind beside the others and
+     beside the thread kinds), side[GDP_NSIDE] the jump-late thread kinds and
+     their 8-bit passes, a chain of its own beside the jump-early one */
+  cudaStream_t side[GDP_NSIDE + 1] = {};
   /* the side streams of the wave streams, each at its wave stream's
      priority: a wave's lane-group, CTA and early 8-bit kinds run beside its
      thread kinds with the same priority, and waves on different streams do
      not queue behind one another's side kernels */
-  cudaStream_t wave_side[GDP_MAX_WAVE_STREAMS][3] = {};
-  cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t wave_side[GDP_MAX_WAVE_STREAMS][GDP_NSIDE + 1] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[GDP_NSIDE + 1] = {};
   gdp_tables_t *h_tab = nullptr;
   gdp_tables_t *d_tab = nullptr;
   int reach_from[4] = {0, 0, 0, 0};   /* FillParams::reach_from of h_tab */
@@ -504,12 +508,12 @@ gdp_ctx_destroy (gdp_ctx *ctx) {
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
-  for (int k = 0; k < 3; k++) {
+  for (int k = 0; k <= GDP_NSIDE; k++) {
     if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
   for (int w = 0; w < GDP_MAX_WAVE_STREAMS; w++)
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k <= GDP_NSIDE; k++)
       if (ctx->wave_side[w][k]) cudaStreamDestroy(ctx->wave_side[w][k]);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   free(ctx->h_tab);
@@ -525,16 +529,14 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   ctx->budget = budget > 0 ? budget : (int64_t) 40 << 30;
   if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return GDP_ERR_CUDA; }
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->side[1], cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->side[2], cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->join_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->join_ev[1], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->join_ev[2], cudaEventDisableTiming) != cudaSuccess) {
+  bool ok = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+  for (int k = 0; ok && k <= GDP_NSIDE; k++)
+    ok = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
     gdp_ctx_destroy(ctx);
     return GDP_ERR_CUDA;
   }
@@ -545,10 +547,10 @@ gdp_ctx_create (gdp_ctx **out, int device, int mode, int64_t budget) {
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
   ctx->nwave = std::max(1, std::min(GDP_MAX_WAVE_STREAMS, least - greatest + 1));
   for (int k = 0; k < ctx->nwave; k++) {
-    if (cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->wave_side[k][0], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->wave_side[k][1], cudaStreamNonBlocking, greatest + k) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->wave_side[k][2], cudaStreamNonBlocking, greatest + k) != cudaSuccess) {
+    ok = cudaStreamCreateWithPriority(&ctx->wave_stream[k], cudaStreamNonBlocking, greatest + k) == cudaSuccess;
+    for (int q = 0; ok && q <= GDP_NSIDE; q++)
+      ok = cudaStreamCreateWithPriority(&ctx->wave_side[k][q], cudaStreamNonBlocking, greatest + k) == cudaSuccess;
+    if (!ok) {
       gdp_ctx_destroy(ctx);
       return GDP_ERR_CUDA;
     }
@@ -1364,9 +1366,9 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   if (need8 > 0) CK(ctx, scratch8.ensure(need8));
   if (need_late > 0) CK(ctx, scratch_late.ensure(need_late));
   /* 16-bit and plain passes first, then the 8-bit passes of rerun pairs.
-     The one-warp / one-CTA-per-pair kinds (no scratch) go first, on the
-     two side streams, so that they run beside the one-thread-per-pair
-     kinds.  Those form two chains: the jump-early kinds share the scratch
+     The one-warp / one-CTA-per-pair kinds (no scratch) go first, on side
+     streams, so that they run beside the one-thread-per-pair kinds and
+     beside one another.  Those form two chains: the jump-early kinds share the scratch
      and stay in order on the main stream, the jump-late kinds have a
      scratch of their own and stay in order on the third side stream.  A
      pair's 8-bit pass waits only for its own 16-bit pass, so each chain's
@@ -1380,7 +1382,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
   CK(ctx, cudaEventRecord(ctx->fork_ev, s));
   for (int round = 0; round < 2; round++) {
     if (round == 1 && forked) {
-      for (int q = 0; q < 2; q++) {
+      for (int q = 0; q < GDP_NSIDE; q++) {
         CK(ctx, cudaEventRecord(ctx->join_ev[q], side_s[q]));
         CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
       }
@@ -1399,10 +1401,10 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
          jump-late pairs */
       const bool late_chain = (thread && ((k >> 1) & 1)) || (warp8 && (((k - FIRST_WARP8) / 3) & 1));
       if (late_chain && !forked_late && two_chains) {
-        CK(ctx, cudaStreamWaitEvent(side_s[2], ctx->fork_ev, 0));
+        CK(ctx, cudaStreamWaitEvent(side_s[GDP_NSIDE], ctx->fork_ev, 0));
         forked_late = true;
       }
-      cudaStream_t ks = (late_chain && two_chains) ? side_s[2] : s;
+      cudaStream_t ks = (late_chain && two_chains) ? side_s[GDP_NSIDE] : s;
       const int grid = cta ? (int) std::max<int64_t>(1, std::min<int64_t>(ph.counts[k], grid_cap(ctx, 8)))
                      : warp ? warp_grid(ctx, ph.counts[k], WARP_K[(k - NTHREADKINDS) % 3])
                      : warp8 ? warp_grid(ctx, ph.counts[k], WARP8_K[(k - FIRST_WARP8) % 3])
@@ -1450,7 +1452,7 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       }
       if (warp || cta || early8) {
         if (!forked) {
-          for (int q = 0; q < 2; q++) CK(ctx, cudaStreamWaitEvent(side_s[q], ctx->fork_ev, 0));
+          for (int q = 0; q < GDP_NSIDE; q++) CK(ctx, cudaStreamWaitEvent(side_s[q], ctx->fork_ev, 0));
           forked = true;
         }
         if (early8) {
@@ -1458,8 +1460,13 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
              one side stream */
           ks = side_s[0];
         } else {
-          ks = side_s[side];
-          side ^= 1;
+          /* each lane-group / CTA kind on a side stream of its own (round
+             robin): a few long pairs leave most of the GPU idle, and their
+             kinds, one after another, took the sum of their latencies.
+             Under a grid footprint cap two side streams, as the cap
+             assumes. */
+          ks = side_s[1 + side % (ctx->grid_limit > 0 ? 2 : GDP_NSIDE - 1)];
+          side++;
         }
       }
       cudaEvent_t ev = nullptr;
@@ -1476,8 +1483,8 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
     }
   }
   if (forked_late) {
-    CK(ctx, cudaEventRecord(ctx->join_ev[2], side_s[2]));
-    CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[2], 0));
+    CK(ctx, cudaEventRecord(ctx->join_ev[GDP_NSIDE], side_s[GDP_NSIDE]));
+    CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[GDP_NSIDE], 0));
   }
   /* the 8-bit outcome of rerun pairs, after both of their passes */
   for (int k = 0; k < NKINDS; k++) {
