@@ -5,7 +5,8 @@ collective on the data path (weak scaling): each rank aligns its own shard
 and the only collectives are the max of the ranks' times and the sums of
 their cell and pair counts.  These tests run that plumbing with world_size
 2 on the gloo backend: the shards of one batch are disjoint, cover it and
-carry balanced work, and the bench's reductions give the max and the sums.
+carry balanced work, the bench's reductions give the max and the sums, and
+outputs aligned rank by rank and gathered equal the whole batch's.
 """
 import os
 import socket
@@ -68,6 +69,56 @@ def test_two_gloo_ranks_shard_and_reduce(tmp_path):
         tmax, tsum, total = np.load(tmp_path / f"rank{r}.npy")
         assert tmax == 3.0                                  # max over ranks of (rank + 1) * 1.5
         assert tsum == total == cells.sum()
+
+
+def _align_rank_main(rank, world, port, out_dir):
+    """One rank aligns its own shard (the oracle's C restatement standing
+    in for the device) and the shards' outputs are gathered on rank 0."""
+    sys.path.insert(0, os.path.join(ROOT, "gmap-gsnap_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import datetime
+    import hashlib
+    import torch.distributed as dist
+    import gdp
+    import oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    lib = gdp.load_workload()
+    genome, blocks = gdp.make_genome(lib, 778, 1 << 20)
+    pairs, arena = gdp.make_pairs(lib, gdp.WL_FIXED, 6, genome, 120)
+    ref = oracle.restatement()
+    ref.init(0)
+    ref.set_genome(blocks, None, genome.size)
+    out = {}
+    for i in gdp.shard_indices(pairs, world, rank).tolist():
+        o = ref.align(pairs, i, arena, want_matrix=False)
+        out[i] = (int(o["score"]), [int(v) for v in o["stats"]], hashlib.sha1(o["recs"].tobytes()).hexdigest())
+    gathered = [None] * world
+    dist.all_gather_object(gathered, out)
+    if rank == 0:
+        merged = {}
+        for g in gathered:
+            assert not set(g) & set(merged)                 # every pair aligned by one rank only
+            merged.update(g)
+        whole = {}
+        for i in range(pairs.size):                         # the same batch in one process
+            o = ref.align(pairs, i, arena, want_matrix=False)
+            whole[i] = (int(o["score"]), [int(v) for v in o["stats"]], hashlib.sha1(o["recs"].tobytes()).hexdigest())
+        np.save(os.path.join(out_dir, "same.npy"), np.array([merged == whole, len(merged)], dtype=np.int64))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_align_their_shards(tmp_path):
+    """The sharded data path: each rank aligns only its shard and the
+    gathered outputs equal the whole batch aligned in one process."""
+    import torch.multiprocessing as mp
+    world, port = 2, _free_port()
+    mp.start_processes(_align_rank_main, args=(world, port, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    same, n = np.load(tmp_path / "same.npy")
+    assert n == 120 and same == 1
 
 
 def test_shards_are_deterministic_and_balanced():
