@@ -200,7 +200,9 @@ struct PlanHost {
   int64_t nlists = 0;
   HostBuf lists, meta, status, rec_off;
   int64_t start[NKINDS + 2] = {0};
-  int32_t counts[NKINDS + 1] = {0};
+  /* entries of each kind's list, then of the traceback list (jump-late
+     pairs first), then its jump-late and its jump-early part */
+  int32_t counts[NKINDS + 3] = {0};
   int maxY[NKINDS] = {0};
   int maxMin[NKINDS] = {0};   /* per kind: the largest min(rlength, glength) */
   int64_t dir_words = 0, total_recs = 0;
@@ -1036,7 +1038,15 @@ plan_build (gdp_ctx *ctx, const gdp_pair_t *pairs, int64_t n, int64_t arena_byte
   }
   ph.start[NKINDS] = pos;
   ph.counts[NKINDS] = (int32_t) ntb;
-  if (ntb > 0) memcpy(lists + pos, tbl, ntb * sizeof(int32_t));
+  /* the traceback list: jump-late pairs first (each part in pair order), so
+     that each fill chain can trace its own pairs back */
+  int64_t nlate = 0;
+  for (int64_t t = 0; t < ntb; t++)
+    if (pairs[tbl[t]].flags & GDP_FLAG_JUMP_LATE) lists[pos + nlate++] = tbl[t];
+  for (int64_t t = 0, e2 = nlate; t < ntb; t++)
+    if (!(pairs[tbl[t]].flags & GDP_FLAG_JUMP_LATE)) lists[pos + e2++] = tbl[t];
+  ph.counts[NKINDS + 1] = (int32_t) nlate;
+  ph.counts[NKINDS + 2] = (int32_t) (ntb - nlate);
   pos += ntb;
   ph.start[NKINDS + 1] = pos;
   ph.nlists = pos;
@@ -1053,7 +1063,7 @@ plan_upload (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, bool hdump, cudaStre
   const size_t nl = (size_t) std::max<int64_t>(ph.nlists, 1);
   CK(ctx, pd.lists.ensure(nl * sizeof(int32_t)));
   CK(ctx, pd.work.ensure(nl * sizeof(int32_t)));
-  CK(ctx, pd.counts.ensure((NKINDS + 1) * sizeof(int32_t)));
+  CK(ctx, pd.counts.ensure((NKINDS + 3) * sizeof(int32_t)));
   CK(ctx, pd.work_counts.ensure(NKINDS * sizeof(int32_t)));
   CK(ctx, pd.status.ensure(n * sizeof(int32_t)));
   CK(ctx, pd.meta0.ensure(n * sizeof(gdp_meta_t)));
@@ -1064,7 +1074,7 @@ plan_upload (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, bool hdump, cudaStre
   if (hdump) CK(ctx, pd.hdump.ensure(std::max<int64_t>(ph.dir_words, 4) * 8 * sizeof(int16_t)));
   if (ph.nlists > 0)
     CK(ctx, cudaMemcpyAsync(pd.lists.p, ph.lists.p, ph.nlists * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  CK(ctx, cudaMemcpyAsync(pd.counts.p, ph.counts, (NKINDS + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(pd.counts.p, ph.counts, (NKINDS + 3) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   if (ph.n > 0) {
     CK(ctx, cudaMemcpyAsync(pd.status.p, ph.status.p, ph.n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     CK(ctx, cudaMemcpyAsync(pd.meta0.p, ph.meta.p, ph.n * sizeof(gdp_meta_t), cudaMemcpyHostToDevice, s));
@@ -1286,14 +1296,17 @@ launch_warp_kind (int k, FillParams P, int grid, cudaStream_t s) {
   else { if (late) launch_warp<GDP_LOWER, true>(kg, P, grid, s); else launch_warp<GDP_LOWER, false>(kg, P, grid, s); }
 }
 
-/* The traceback launch over the plan's traceback list on stream ks. */
+/* The traceback launch over the plan's traceback list on stream ks: part 0
+   the whole list, 1 its jump-late pairs, 2 its jump-early pairs. */
 static int
 launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pairs, const char *d_arena,
-                  gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t ks) {
+                  gdp_result_t *d_res, gdp_rec_t *d_slots, cudaStream_t ks, int part = 0) {
+  const int64_t count = ph.counts[NKINDS + part];
+  if (count <= 0) return GDP_OK;
   TbParams T;
   T.pairs = d_pairs; T.arena = d_arena;
-  T.list = pd.lists.as<int32_t>() + ph.start[NKINDS];
-  T.count = pd.counts.as<int32_t>() + NKINDS;
+  T.list = pd.lists.as<int32_t>() + ph.start[NKINDS] + (part == 2 ? ph.counts[NKINDS + 1] : 0);
+  T.count = pd.counts.as<int32_t>() + NKINDS + part;
   T.dirs = pd.dirs.as<uint32_t>(); T.meta = pd.meta.as<gdp_meta_t>(); T.res = d_res; T.recs = d_slots;
   T.rec_off = pd.rec_off.as<int64_t>();
   T.genome = ctx->d_genome; T.genomealt = ctx->d_genomealt;
@@ -1303,10 +1316,10 @@ launch_traceback (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_
   cudaEvent_t ev = nullptr;
   prof_begin(ctx, &ev, ks);
   if (ctx->tb_warp) {
-    const int g = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[NKINDS] + 3) / 4, grid_cap(ctx, 16)));
+    const int g = (int) std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, grid_cap(ctx, 16)));
     traceback_warp_kernel<<<g, 128, 0, ks>>>(T);
   } else {
-    traceback_kernel<<<fill_grid(ctx, ph.counts[NKINDS]), 128, 0, ks>>>(T);
+    traceback_kernel<<<fill_grid(ctx, count), 128, 0, ks>>>(T);
   }
   prof_end(ctx, PROF_TB, ev, ks);
   ctx->launches++;
@@ -1482,23 +1495,38 @@ plan_run (gdp_ctx *ctx, const PlanHost &ph, PlanDev &pd, const gdp_pair_t *d_pai
       CK(ctx, cudaGetLastError());
     }
   }
-  if (forked_late) {
-    CK(ctx, cudaEventRecord(ctx->join_ev[GDP_NSIDE], side_s[GDP_NSIDE]));
-    CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[GDP_NSIDE], 0));
-  }
-  /* the 8-bit outcome of rerun pairs, after both of their passes */
+  /* The 8-bit outcome of rerun pairs, after both of their passes, then
+     the tracebacks.  With the two chains, the jump-late pairs' outcomes and
+     tracebacks run on the jump-late chain's stream once it and the side
+     kinds are done, beside the jump-early chain's tail (its 8-bit pass
+     holds few pairs and leaves most of the GPU idle); the jump-early ones
+     follow on the plan's stream. */
+  cudaStream_t late_s = forked_late ? side_s[GDP_NSIDE] : s;
+  if (forked_late && forked)
+    for (int q = 0; q < GDP_NSIDE; q++) CK(ctx, cudaStreamWaitEvent(late_s, ctx->join_ev[q], 0));
   for (int k = 0; k < NKINDS; k++) {
     const bool check8 = (k < NTHREADKINDS && (k >> 2) / 3 == 1 && (k & 1)) || (k >= FIRST_WARP8 && k < FIRST_CTA) ||
                         k >= FIRST_EARLY8;
     if (!check8 || !ph.counts[k]) continue;
+    const int late = (k < NTHREADKINDS) ? ((k >> 1) & 1)
+                   : (k < FIRST_CTA) ? (((k - FIRST_WARP8) / 3) & 1) : ((k - FIRST_EARLY8) & 1);
+    cudaStream_t as = late ? late_s : s;
     const int ag = (int) std::max<int64_t>(1, std::min<int64_t>((ph.counts[k] + 255) / 256, (int64_t) ctx->nsm * 8));
-    apply_rerun8_kernel<<<ag, 256, 0, s>>>(pd.lists.as<int32_t>() + ph.start[k], pd.counts.as<int32_t>() + k,
-                                           pd.meta.as<gdp_meta_t>(), d_res);
+    apply_rerun8_kernel<<<ag, 256, 0, as>>>(pd.lists.as<int32_t>() + ph.start[k], pd.counts.as<int32_t>() + k,
+                                            pd.meta.as<gdp_meta_t>(), d_res);
     ctx->launches++;
     CK(ctx, cudaGetLastError());
   }
-  if (ph.counts[NKINDS] > 0) return launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, s);
-  return GDP_OK;
+  int rc = GDP_OK;
+  if (forked_late) {
+    rc = launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, late_s, 1);
+    if (rc == GDP_OK) rc = launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, s, 2);
+    CK(ctx, cudaEventRecord(ctx->join_ev[GDP_NSIDE], late_s));
+    CK(ctx, cudaStreamWaitEvent(s, ctx->join_ev[GDP_NSIDE], 0));
+  } else {
+    rc = launch_traceback(ctx, ph, pd, d_pairs, d_arena, d_res, d_slots, s, 0);
+  }
+  return rc;
 }
 
 /* Dense records after plan_run: scan of nrecs, gather into `out`, total in
