@@ -2280,9 +2280,19 @@ gdp_align_batch_multi (gdp_ctx *const *ctxs, int nctx, const gdp_pair_t *pairs, 
                             slots[n] > 0 ? recs + slots[lo] : nullptr, slots[hi] - slots[lo], &used[k]);
     for (int64_t i = lo; i < hi; i++) results[i].rec_offset += slots[lo];
   };
+  /* shard k > 0 on a thread of its own; a shard whose thread cannot be
+     started runs on this thread after shard 0 */
   std::vector<std::thread> th;
-  for (int k = 1; k < nctx; k++) th.emplace_back(run, k);
+  std::vector<int> inline_shards;
+  for (int k = 1; k < nctx; k++) {
+    try {
+      th.emplace_back(run, k);
+    } catch (...) {
+      inline_shards.push_back(k);
+    }
+  }
   run(0);
+  for (int k : inline_shards) run(k);
   for (auto &t : th) t.join();
   int64_t end = 0;
   for (int k = 0; k < nctx; k++) {
