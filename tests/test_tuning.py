@@ -6,6 +6,8 @@
   one thread, a lane group or a CTA; the traceback mapping) from timings of
   a sample; the results of a batch aligned with the tuned parameters are
   identical to those with the defaults.
+* The plan's stream layouts (concurrent chains, one stream, footprint cap)
+  give identical results.
 """
 import ctypes
 
@@ -87,6 +89,34 @@ def test_autotuned_routing_gives_identical_results(gdplib):
     assert (ref["status"] == 0).all()
     assert _same(got, ref) and got_recs.tobytes() == ref_recs.tobytes()
     assert _same(thr, ref) and thr_recs.tobytes() == ref_recs.tobytes()
+
+
+def test_stream_layouts_give_identical_results(gdplib):
+    """The concurrent layout of a plan (jump-late chain and lane-group kinds
+    on side streams, each chain tracing its own pairs back), the one-stream
+    layout of per-launch timing, and the layout under a grid footprint cap
+    (two side streams, one chain) give the same results and records."""
+    genome, blocks = gdp.make_genome(gdplib, 81, 1 << 22)
+    a, arena_a = gdp.make_pairs(gdplib, gdp.WL_MIX, 82, genome, 800)
+    b, arena_b = gdp.make_pairs(gdplib, gdp.WL_SHORT, 83, genome, 2000)
+    b = b.copy()
+    for f in ("rseq", "rseq_uc", "gseq", "gseq_alt"):
+        b[f] += arena_a.size
+    pairs, arena = np.concatenate([a, b]), np.concatenate([arena_a, arena_b])
+    ctx = gdp.Context(gdplib)
+    ctx.set_genome(blocks, None, genome.size)
+    ref, ref_recs = ctx.align(pairs, arena)
+    ctx.profile(True)
+    prof, prof_recs = ctx.align(pairs, arena)
+    ctx.profile(False)
+    ctx.set_param("grid_blocks_per_sm", 2)
+    cap, cap_recs = ctx.align(pairs, arena)
+    ctx.close()
+    assert (ref["status"] == 0).all()
+    late = (pairs["flags"] & gdp.FLAG_JUMP_LATE) != 0
+    assert late.any() and (~late).any()
+    assert _same(prof, ref) and prof_recs.tobytes() == ref_recs.tobytes()
+    assert _same(cap, ref) and cap_recs.tobytes() == ref_recs.tobytes()
 
 
 def test_direction_budget_splits_waves(gdplib):
